@@ -1,0 +1,231 @@
+"""Reference-named entry points over the CUDA library.
+
+Each function has the name, argument meaning and return values of the MATLAB
+function of toby-sanders/GBM3D it replaces, and calls libgbm3d.so through its
+C ABI.  Arrays follow MATLAB's column-major layout (numpy order='F'):
+
+  U, out          = GBM3D(I, sigma, opts)                     source/GBM3D.m:1
+  S, Volume       = matchBlocksCPU(I, sigma, opts)            source/matchBlocksCPU.m:1
+  U, W            = denoiseAndAggregateGPU(Volume, S, tau, Psi, Psi2, opts)
+                                                              source/denoiseAndAggregateGPU.m:1
+  S, V1, V2       = matchBlocksWie(I, In, sigma, opts)        source/matchBlocksWie.m:1
+  U, W            = denoiseAndAggregateWieFast(V1, V2, S, sigma, opts)
+                                                              source/denoiseAndAggregateWieFast.m:1
+  U, W            = denoiseAndAggregateWie(V1, V2, S, sigma, opts)
+                                                              source/denoiseAndAggregateWie.m:1
+
+S is returned as a MatchSet: a uint32 array of shape (K, M, N) whose column
+S[:, i, j] is the reference's cell S{i+1, j+1}, plus the per-cell counts.
+Errors raise GBM3DError with the library's message, as the MATLAB code raises
+error(); nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import options as _opt
+from ._lib import Context, GBM3DError, context, gbm3d_filters, gbm3d_opts, lib
+
+
+class MatchSet(np.ndarray):
+    """uint32 (K, M, N) match indices; ``.count`` is numel(S{i,j}) per cell."""
+
+    count: np.ndarray | None = None
+
+    def cell(self, i: int, j: int) -> np.ndarray:
+        """The MATLAB cell S{i+1, j+1} (trailing unused entries removed)."""
+        k = self.shape[0] if self.count is None else int(self.count[i, j])
+        return np.asarray(self[:k, i, j])
+
+
+def _as_set(S, count=None) -> MatchSet:
+    out = np.asfortranarray(S, dtype=np.uint32).view(MatchSet)
+    out.count = count
+    return out
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def c_opts(opts: dict) -> gbm3d_opts:
+    o = _opt.checkBM3Dopts(opts)
+    c = gbm3d_opts()
+    c.numMax, c.numMin = int(o["numMax"]), int(o["numMin"])
+    c.blockSize, c.blockSizeWie, c.matchSize = int(o["blockSize"]), int(o["blockSizeWie"]), int(o["matchSize"])
+    c.refStride = 0 if int(o["refStride"]) == int(o["blockSize"]) else int(o["refStride"])
+    c.levels, c.cycleSpin, c.tauMode = int(o["levels"]), int(o["cycleSpin"]), int(o["tauMode"])
+    c.Wiener = 1 if o["Wiener"] else 0
+    ft = o.get("filtType", "ht")
+    if ft not in ("ht", "median"):
+        raise GBM3DError(1, "unrecognized filtering")  # denoiseAndAggregateGPU.m:54
+    c.filtType = 0 if ft == "ht" else 1
+    ms, mw = list(o["matchSpins"]), list(o["matchSpinsWie"])
+    if len(ms) > 8 or len(mw) > 8:
+        raise GBM3DError(1, "at most 8 match spins per step")
+    c.nMatchSpins = len(ms)
+    for i, s in enumerate(ms):
+        c.matchSpins[i] = int(s)
+    c.nMatchSpinsWie = len(mw)
+    for i, s in enumerate(mw):
+        c.matchSpinsWie[i] = int(s)
+    c.staleWeights = 1 if o.get("staleWeights", True) else 0
+    return c
+
+
+def c_filters(fac: dict) -> gbm3d_filters:
+    f = gbm3d_filters()
+    f.len_xy = len(fac["a_lo_xy"])
+    f.len_z = len(fac["a_lo_z"])
+    for k in ("a_lo_xy", "a_hi_xy", "s_lo_xy", "s_hi_xy", "a_lo_z", "a_hi_z", "s_lo_z", "s_hi_z"):
+        v = np.asarray(fac[k], dtype=np.float64)
+        if v.size > 16:
+            raise GBM3DError(5, "filters longer than 16 taps are not supported")
+        getattr(f, k)[: v.size] = list(v)
+    return f
+
+
+def _sigma_scalar(sigma) -> float:
+    """matchBlocksCPU.m:21 — a coloured-noise sigma matrix becomes mean(sqrt(sigma))."""
+    s = np.asarray(sigma, dtype=np.float64)
+    if s.ndim >= 1 and s.shape[0] > 1:
+        return float(np.mean(np.sqrt(s)))
+    return float(s.reshape(-1)[0])
+
+
+def matchBlocksCPU(I, sigma, opts: dict, ctx: Context | None = None):
+    """[S, Volume] = matchBlocksCPU(I, sigma, opts)."""
+    ctx = ctx or context()
+    o = _opt.checkBM3Dopts(opts)
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n = I.shape
+    d, K = int(o["blockSize"]), int(o["numMax"])
+    M, N = m // d, n // d
+    S = np.zeros((K, M, N), dtype=np.uint32, order="F")
+    cnt = np.zeros((M, N), dtype=np.int32, order="F")
+    V = np.zeros((m, n, K), dtype=np.float32, order="F")
+    co = c_opts(o)
+    ctx.check(lib().gbm3d_matchBlocksCPU(ctx.h, _p(I), m, n, _sigma_scalar(sigma), C.byref(co),
+                                         _p(S), _p(cnt), _p(V)))
+    return _as_set(S, cnt), V
+
+
+def denoiseAndAggregateGPU(Volume, S, tau, Psi, Psi2, opts: dict, ctx: Context | None = None):
+    """[U, W] = denoiseAndAggregateGPU(Volume, S, tau, Psi, Psi2, opts).
+
+    Psi/Psi2 may be the reference's 4D banks (factorised into separable 1D
+    filters) or None for the default bior1.5 x Haar bank.
+    """
+    ctx = ctx or context()
+    o = _opt.checkBM3Dopts(opts)
+    if o.get("filtType", "ht") not in ("ht", "median"):
+        raise GBM3DError(1, "unrecognized filtering")
+    fac = _opt.bior_factors() if Psi is None else _opt.factors_from_bank(Psi, Psi2)
+    Volume = np.asfortranarray(Volume, dtype=np.float32)
+    K, M, N = S.shape
+    cnt = getattr(S, "count", None)
+    Sa = np.asfortranarray(S, dtype=np.uint32)
+    d = int(o["blockSize"])
+    if Volume.shape != (M * d, N * d, K):
+        raise GBM3DError(1, f"Volume shape {Volume.shape} does not match S ({M * d}, {N * d}, {K})")
+    tau = np.asfortranarray(tau, dtype=np.float64)
+    if tau.shape != (int(o["levels"]), 7):
+        raise GBM3DError(1, "tau must be levels x 7")
+    U = np.zeros((M * d, N * d), order="F")
+    W = np.zeros_like(U)
+    co, cf = c_opts(o), c_filters(fac)
+    cp = None
+    if cnt is not None:
+        cnt = np.asfortranarray(cnt, dtype=np.int32)
+        cp = _p(cnt)
+    ctx.check(lib().gbm3d_denoiseAndAggregateGPU(ctx.h, _p(Volume), _p(Sa), cp, M, N, _p(tau), C.byref(cf),
+                                                 C.byref(co), _p(U), _p(W)))
+    return U, W
+
+
+def matchBlocksWie(I, In, sigma, opts: dict, ctx: Context | None = None):
+    """[S, V1, V2] = matchBlocksWie(I, In, sigma, opts)."""
+    ctx = ctx or context()
+    o = _opt.checkBM3Dopts(opts)
+    I = np.asfortranarray(I, dtype=np.float64)
+    In = np.asfortranarray(In, dtype=np.float64)
+    if I.shape != In.shape:
+        raise GBM3DError(1, "I and In must have the same size")
+    m, n = I.shape
+    d, K = int(o["blockSizeWie"]), int(o["numMax"])
+    M, N = m // d, n // d
+    S = np.zeros((K, M, N), dtype=np.uint32, order="F")
+    V1 = np.zeros((d, d, K, M, N), dtype=np.float32, order="F")
+    V2 = np.zeros_like(V1)
+    co = c_opts(o)
+    ctx.check(lib().gbm3d_matchBlocksWie(ctx.h, _p(I), _p(In), m, n, _sigma_scalar(sigma), C.byref(co),
+                                         _p(S), _p(V1), _p(V2)))
+    return _as_set(S), V1, V2
+
+
+def _wiener(V1, V2, S, sigma, opts, ctx, variant):
+    ctx = ctx or context()
+    o = _opt.checkBM3Dopts(opts)
+    V1 = np.asfortranarray(V1, dtype=np.float32)
+    V2 = np.asfortranarray(V2, dtype=np.float32)
+    d, _, K, M, N = V1.shape
+    if V2.shape != V1.shape or S.shape != (K, M, N):
+        raise GBM3DError(1, "V1, V2 and S sizes disagree")
+    o = dict(o, blockSizeWie=d, numMax=K, numMin=min(int(o["numMin"]), K))
+    Sa = np.asfortranarray(S, dtype=np.uint32)
+    sg = np.asfortranarray(np.atleast_1d(np.asarray(sigma, dtype=np.float64)))
+    U = np.zeros((M * d, N * d), order="F")
+    W = np.zeros_like(U)
+    co = c_opts(o)
+    if variant == 0:
+        is_mat = 1 if sg.size > 1 else 0
+        if is_mat and sg.shape != (d, d):
+            raise GBM3DError(1, "sigma must be a scalar or a d x d matrix")
+        ctx.check(lib().gbm3d_denoiseAndAggregateWieFast(ctx.h, _p(V1), _p(V2), _p(Sa), M, N, _p(sg), is_mat,
+                                                         C.byref(co), _p(U), _p(W)))
+    else:
+        if sg.size != 1:
+            raise GBM3DError(5, "denoiseAndAggregateWie takes a scalar sigma")
+        ctx.check(lib().gbm3d_denoiseAndAggregateWie(ctx.h, _p(V1), _p(V2), _p(Sa), M, N, float(sg[0]),
+                                                     C.byref(co), _p(U), _p(W)))
+    return U, W
+
+
+def denoiseAndAggregateWieFast(V1, V2, S, sigma, opts: dict, ctx: Context | None = None):
+    """[U, W] = denoiseAndAggregateWieFast(V1, V2, S, sigma, opts)."""
+    return _wiener(V1, V2, S, sigma, opts, ctx, 0)
+
+
+def denoiseAndAggregateWie(V1, V2, S, sigma, opts: dict, ctx: Context | None = None):
+    """[U, W] = denoiseAndAggregateWie(V1, V2, S, sigma, opts) (legacy variant)."""
+    return _wiener(V1, V2, S, sigma, opts, ctx, 1)
+
+
+def GBM3D(I, sigma, opts: dict | None = None, ctx: Context | None = None):
+    """[U, out] = GBM3D(I, sigma, opts); out['U1'] is the step-1 estimate.
+
+    ``opts`` with a 'profile' field is replaced by that profile (GBM3D.m:16-19).
+    """
+    ctx = ctx or context()
+    o = _opt.resolve_opts(opts)
+    if np.ndim(sigma) != 0 and np.size(sigma) != 1:
+        raise GBM3DError(5, "coloured-noise (matrix) sigma is not supported by GBM3D here")
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n = I.shape
+    U = np.zeros((m, n), order="F")
+    U1 = np.zeros((m, n), order="F")
+    co = c_opts(o)
+    ctx.check(lib().gbm3d_denoise(ctx.h, _p(I), m, n, float(np.asarray(sigma).reshape(-1)[0]), C.byref(co),
+                                  _p(U), _p(U1)))
+    return U, {"U1": U1}
+
+
+def GBM3D_device(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dict | None = None,
+                 U1_ptr: int = 0, ctx: Context | None = None) -> None:
+    """Whole pipeline on device buffers (float64, column-major), asynchronous on the context stream."""
+    ctx = ctx or context()
+    co = c_opts(_opt.resolve_opts(opts))
+    ctx.check(lib().gbm3d_denoise_device(ctx.h, C.c_void_p(I_ptr), m, n, float(sigma), C.byref(co),
+                                         C.c_void_p(U_ptr), C.c_void_p(U1_ptr or 0)))

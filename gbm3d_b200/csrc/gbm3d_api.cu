@@ -1,0 +1,873 @@
+// C ABI of the GBM3D library (include/gbm3d.h) and the device pipeline that
+// restates source/GBM3D.m:15-83.
+//
+// Data stays on the device for the whole two-step pipeline: the image is
+// uploaded once (double), converted to single and mirror-padded on the
+// device, and only U (and optionally U1) come back.  The per-function entry
+// points (matchBlocksCPU, denoiseAndAggregateGPU, matchBlocksWie,
+// denoiseAndAggregateWieFast, denoiseAndAggregateWie) copy their host
+// arguments in and their results out, so a MEX gateway can call them with
+// mxArray data directly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/gbm3d.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace gbm3d;
+
+struct gbm3d_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t st = nullptr;
+  std::string err;
+  std::map<std::string, std::pair<void*, size_t>> bufs;
+  bool timing = false;
+  std::vector<cudaEvent_t> evpool;           // events reused across calls
+  std::vector<std::pair<int, int>> records;  // (stage, index of start event; end = +1)
+  int launches = 0;
+  int* flag = nullptr;  // device status word (non-finite input)
+};
+
+namespace {
+
+struct Fail {
+  int code;
+};
+
+void set_err(gbm3d_ctx* c, const std::string& s) {
+  if (c) c->err = s;
+}
+
+void ck(gbm3d_ctx* c, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    set_err(c, std::string(what) + ": " + cudaGetErrorString(e));
+    throw Fail{e == cudaErrorMemoryAllocation ? GBM3D_ERR_NOMEM : GBM3D_ERR_CUDA};
+  }
+}
+
+void argfail(gbm3d_ctx* c, const std::string& s, int code = GBM3D_ERR_ARG) {
+  set_err(c, s);
+  throw Fail{code};
+}
+
+template <class T>
+T* buf(gbm3d_ctx* c, const char* name, size_t count) {
+  const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+  auto it = c->bufs.find(name);
+  if (it != c->bufs.end() && it->second.second >= bytes) return reinterpret_cast<T*>(it->second.first);
+  if (it != c->bufs.end()) {
+    cudaFree(it->second.first);
+    c->bufs.erase(it);
+  }
+  void* p = nullptr;
+  ck(c, cudaMalloc(&p, bytes), name);
+  c->bufs[name] = {p, bytes};
+  return reinterpret_cast<T*>(p);
+}
+
+void launched(gbm3d_ctx* c, cudaError_t e, const char* what) {
+  ck(c, e, what);
+  ++c->launches;
+}
+
+// Stage timer: records a start/end event pair on the stream when timing is on.
+// Stages: 0 prepare, 1 step-1 matching, 2 step-1 wavelet, 3 step-1 aggregation,
+// 4 step-2 matching, 5 step-2 Wiener, 6 step-2 aggregation, 7 whole call.
+struct StageTimer {
+  gbm3d_ctx* c;
+  int idx = -1;
+  StageTimer(gbm3d_ctx* cc, int stage) : c(cc) {
+    if (!c->timing) return;
+    idx = (int)c->records.size() * 2;
+    while ((int)c->evpool.size() < idx + 2) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      c->evpool.push_back(e);
+    }
+    c->records.push_back({stage, idx});
+    cudaEventRecord(c->evpool[idx], c->st);
+  }
+  ~StageTimer() {
+    if (idx >= 0) cudaEventRecord(c->evpool[idx + 1], c->st);
+  }
+};
+
+// ---- small host helpers shared with the option layer --------------------------
+
+void sine_window(int d, double lo, double hi, double* w) {
+  std::vector<double> v(d);
+  for (int i = 0; i < d; ++i) {
+    double t = (d == 1) ? hi : (i == d - 1 ? hi : lo + i * (hi - lo) / (d - 1));
+    v[i] = std::sin(M_PI * t);
+  }
+  for (int c = 0; c < d; ++c)
+    for (int r = 0; r < d; ++r) w[r + c * d] = v[r] * v[c];
+}
+
+// dct(eye(d)) and inv() of it (denoiseAndAggregateWieFast.m:33-34)
+void dct_matrices(int d, double* Tm, double* Ti) {
+  for (int k = 0; k < d; ++k)
+    for (int n = 0; n < d; ++n) {
+      double ck = (k == 0) ? std::sqrt(1.0 / d) : std::sqrt(2.0 / d);
+      Tm[k + n * d] = ck * std::cos(M_PI * (2 * n + 1) * k / (2.0 * d));
+    }
+  std::vector<double> a(d * 2 * d);
+  for (int r = 0; r < d; ++r)
+    for (int c = 0; c < 2 * d; ++c) a[r * 2 * d + c] = c < d ? Tm[r + c * d] : (c - d == r ? 1.0 : 0.0);
+  for (int col = 0; col < d; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < d; ++r)
+      if (std::fabs(a[r * 2 * d + col]) > std::fabs(a[piv * 2 * d + col])) piv = r;
+    if (piv != col)
+      for (int c = 0; c < 2 * d; ++c) std::swap(a[col * 2 * d + c], a[piv * 2 * d + c]);
+    double p = a[col * 2 * d + col];
+    for (int c = 0; c < 2 * d; ++c) a[col * 2 * d + c] /= p;
+    for (int r = 0; r < d; ++r) {
+      if (r == col) continue;
+      double f = a[r * 2 * d + col];
+      if (f == 0.0) continue;
+      for (int c = 0; c < 2 * d; ++c) a[r * 2 * d + c] -= f * a[col * 2 * d + c];
+    }
+  }
+  for (int r = 0; r < d; ++r)
+    for (int c = 0; c < d; ++c) Ti[r + c * d] = a[r * 2 * d + d + c];
+}
+
+Taps make_taps(const double* h, int len) {
+  Taps t{};
+  t.n = 0;
+  for (int k = 0; k < len && k < GBM3D_MAX_TAPS; ++k)
+    if (h[k] != 0.0) {
+      t.k[t.n] = k;
+      t.h[t.n] = (float)h[k];
+      ++t.n;
+    }
+  return t;
+}
+
+WaveletBank make_bank(gbm3d_ctx* c, const gbm3d_filters* f) {
+  if (f->len_xy < 1 || f->len_xy > GBM3D_MAX_TAPS || f->len_z < 1 || f->len_z > GBM3D_MAX_TAPS)
+    argfail(c, "filter length out of range");
+  WaveletBank b{};
+  b.xy.a[0] = make_taps(f->a_lo_xy, f->len_xy);
+  b.xy.a[1] = make_taps(f->a_hi_xy, f->len_xy);
+  b.xy.s[0] = make_taps(f->s_lo_xy, f->len_xy);
+  b.xy.s[1] = make_taps(f->s_hi_xy, f->len_xy);
+  b.z.a[0] = make_taps(f->a_lo_z, f->len_z);
+  b.z.a[1] = make_taps(f->a_hi_z, f->len_z);
+  b.z.s[0] = make_taps(f->s_lo_z, f->len_z);
+  b.z.s[1] = make_taps(f->s_hi_z, f->len_z);
+  b.reach_a = b.reach_s = 0;
+  for (int x = 0; x < 2; ++x) {
+    for (int u = 0; u < b.xy.a[x].n; ++u) b.reach_a = std::max(b.reach_a, b.xy.a[x].k[u]);
+    for (int u = 0; u < b.xy.s[x].n; ++u) b.reach_s = std::max(b.reach_s, b.xy.s[x].k[u]);
+    for (int u = 0; u < b.z.a[x].n; ++u)
+      if (b.z.a[x].k[u] > 1) argfail(c, "slot-axis filters longer than 2 taps are not supported", GBM3D_ERR_UNSUPPORTED);
+    for (int u = 0; u < b.z.s[x].n; ++u)
+      if (b.z.s[x].k[u] > 1) argfail(c, "slot-axis filters longer than 2 taps are not supported", GBM3D_ERR_UNSUPPORTED);
+  }
+  return b;
+}
+
+void bior(gbm3d_filters* f) {
+  std::memset(f, 0, sizeof(*f));
+  const double Ca = 0.016572815184060, Cb = 0.121533978016438, Cc = std::sqrt(2.0) / 2;
+  const double lo[10] = {Ca, -Ca, -Cb, Cb, Cc, Cc, Cb, -Cb, -Ca, Ca};
+  const double shi[10] = {-Ca, -Ca, Cb, Cb, -Cc, Cc, -Cb, -Cb, Ca, Ca};
+  f->len_xy = 10;
+  for (int k = 0; k < 10; ++k) {
+    f->a_lo_xy[k] = lo[k];
+    f->s_hi_xy[k] = shi[k];
+  }
+  f->a_hi_xy[4] = -Cc;
+  f->a_hi_xy[5] = Cc;
+  f->s_lo_xy[4] = Cc;
+  f->s_lo_xy[5] = Cc;
+  f->len_z = 2;
+  f->a_lo_z[0] = Cc; f->a_lo_z[1] = Cc; f->a_hi_z[0] = -Cc; f->a_hi_z[1] = Cc;
+  f->s_lo_z[0] = Cc; f->s_lo_z[1] = Cc; f->s_hi_z[0] = -Cc; f->s_hi_z[1] = Cc;
+}
+
+void tau_table(int levels, int mode, double* tau) {
+  for (int j = 0; j < 7; ++j)
+    for (int i = 0; i < levels; ++i) {
+      double base = 3.3 - 0.3 * i, v = 0;
+      switch (mode) {
+        case 1: v = base; break;
+        case 2: v = j < 3 ? base : (j < 6 ? base + 0.5 : base + 1.0); break;
+        case 3: v = j < 3 ? base : (j < 6 ? base + 0.25 : base + 1.5); break;
+        case 4: v = j < 3 ? 2.9 : (j < 6 ? 2.9 + 0.5 : 2.9 + 1.0); break;
+        default: v = 0;
+      }
+      tau[i + levels * j] = v;
+    }
+}
+
+// band code (fy + 2 fx + 4 fz) -> detail column j of tau (getWaveFilters3Dbior.m:39-46)
+const int kDetailJ[8] = {-1, 0, 1, 3, 2, 4, 5, 6};
+
+// ---- glue kernels --------------------------------------------------------------
+
+// double m x n -> mirror-padded single M x N (myMirrorPadImage.m:3-8 then
+// single(), matchBlocksCPU.m:31); flags non-finite input.
+__global__ void k_prep(const double* __restrict__ I, int m, int n, float* __restrict__ out, int Mp, int Np,
+                       int* flag) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= Mp || c >= Np) return;
+  const int sr = r < m ? r : m - 1 - (r - m), sc = c < n ? c : n - 1 - (c - n);
+  const double v = I[sr + (size_t)sc * m];
+  if (!isfinite(v)) atomicOr(flag, 1);
+  out[r + (size_t)c * Mp] = (float)v;
+}
+
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, size_t n) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+
+// acc[p] (+)= (double) v[(r+s) mod Mp, (c+s) mod Np]: circshift(.,[-s,-s]) then
+// the running sum over spins (GBM3D.m:53-57,78-83).
+__global__ void k_accum(const float* __restrict__ v, int Mp, int Np, int s, double* __restrict__ acc, int first) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= Mp || c >= Np) return;
+  const double x = (double)v[pmod(r + s, Mp) + (size_t)pmod(c + s, Np) * Mp];
+  const size_t o = r + (size_t)c * Mp;
+  acc[o] = first ? x : acc[o] + x;
+}
+
+__global__ void k_shift_copy(const float* __restrict__ v, int Mp, int Np, int s, float* __restrict__ out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= Mp || c >= Np) return;
+  out[r + (size_t)c * Mp] = v[pmod(r + s, Mp) + (size_t)pmod(c + s, Np) * Mp];
+}
+
+__global__ void k_add_f(const float* __restrict__ v, double* __restrict__ acc, size_t n) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) acc[i] = acc[i] + (double)v[i];
+}
+
+// out = a ./ b on the padded grid (double), its single copy, and the m x n crop.
+__global__ void k_ratio(const double* __restrict__ a, const double* __restrict__ b, int Mp, int Np,
+                        double* __restrict__ full, float* __restrict__ full_f, double* __restrict__ crop,
+                        int m, int n) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= Mp || c >= Np) return;
+  const size_t o = r + (size_t)c * Mp;
+  const double v = a[o] / b[o];
+  if (full) full[o] = v;
+  if (full_f) full_f[o] = (float)v;
+  if (crop && r < m && c < n) crop[r + (size_t)c * m] = v;
+}
+
+dim3 grid2(int rows, int cols) { return dim3((rows + 255) / 256, cols); }
+
+// ---- validation ------------------------------------------------------------------
+
+void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
+  if (!o) argfail(c, "opts is NULL");
+  if (o->numMax < 1 || o->numMax > 32) argfail(c, "numMax must be in 1..32");
+  if (o->numMin < 1 || o->numMin > o->numMax) argfail(c, "numMin must be in 1..numMax");
+  if (o->matchSize < 2 || (o->matchSize & 1)) argfail(c, "matchSize must be even");
+  if (o->refStride != 0 && o->refStride != o->blockSize)
+    argfail(c, "refStride other than blockSize is not supported yet", GBM3D_ERR_UNSUPPORTED);
+  if (o->filtType != 0) argfail(c, "filtType 'median' is not supported", GBM3D_ERR_UNSUPPORTED);
+}
+
+void check_match(gbm3d_ctx* c, int d, int d2, int K) {
+  if (!match_supported(d, d2))
+    argfail(c, "unsupported (blockSize, matchSize) pair for block matching: (" + std::to_string(d) + "," +
+                   std::to_string(d2) + ")", GBM3D_ERR_UNSUPPORTED);
+  if (d2 * d2 < K) argfail(c, "numMax exceeds the number of candidates");
+}
+
+int pitch4(int rows) { return (rows + 3) & ~3; }
+
+// ---- pipelines ----------------------------------------------------------------------
+
+// Block matching on a single-precision image already on the device.
+void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, int spin, int d, int d2,
+               int K, int numMin, double sigma, uint32_t* S, int32_t* cnt, float* volume, float* V1,
+               float* V2, const char* tag) {
+  const int P = pitch4(m + d2);
+  const std::string t(tag);
+  float* pad = buf<float>(c, (t + ".pad").c_str(), (size_t)P * (n + d2));
+  launched(c, launch_make_pad(img, m, n, d2, spin, pad, P, c->st), "make_pad");
+  float* pad2 = nullptr;
+  if (img2) {
+    pad2 = buf<float>(c, (t + ".pad2").c_str(), (size_t)P * (n + d2));
+    launched(c, launch_make_pad(img2, m, n, d2, spin, pad2, P, c->st), "make_pad");
+  }
+  MatchArgs A{};
+  A.pad = pad;
+  A.pad2 = pad2;
+  A.P = P;
+  A.M = m / d;
+  A.N = n / d;
+  A.K = K;
+  A.numMin = numMin;
+  A.tol = (float)(0.005 * sigma * sigma * d * d);
+  A.tol_branch = numMin != K;
+  A.S = S;
+  A.cnt = cnt;
+  A.volume = volume;
+  A.m = m;
+  A.n = n;
+  A.V1 = V1;
+  A.V2 = V2;
+  launched(c, launch_match(d, d2, A, c->st), "match");
+}
+
+// denoiseAndAggregateGPU on device buffers; U, W are float (M d) x (N d).
+void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cnt, int M, int N, int d,
+            int d2, int K, int levels, int cycleSpin, const double* tau, const WaveletBank& bk, float* U,
+            float* W) {
+  const int m = M * d, n = N * d;
+  const int q = 1 << levels;
+  if (levels < 1 || levels > GBM3D_MAX_LEVELS) argfail(c, "levels out of range");
+  if (m % q || n % q || K % q)
+    argfail(c, "image size and numMax must be divisible by 2^levels for the 3D wavelet");
+  if (cycleSpin < 1) argfail(c, "cycleSpin must be >= 1");
+  std::vector<float*> coef(levels), rec(levels);
+  for (int lv = 0; lv < levels; ++lv) {
+    const size_t insz = (size_t)(m >> lv) * (n >> lv) * (K >> lv);
+    coef[lv] = buf<float>(c, ("ht.coef" + std::to_string(lv)).c_str(), insz);  // 8 bands = input size
+    if (lv > 0) rec[lv] = buf<float>(c, ("ht.rec" + std::to_string(lv)).c_str(), insz);
+  }
+  float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
+  std::vector<LevelBands> th(levels);
+  for (int lv = 0; lv < levels; ++lv) {
+    th[lv].tau[0] = 0.f;
+    for (int code = 1; code < 8; ++code) th[lv].tau[code] = (float)tau[lv + levels * kDetailJ[code]];
+  }
+  {
+  StageTimer tw(c, 2);
+  for (int s = 0; s < cycleSpin; ++s) {
+    for (int lv = 0; lv < levels; ++lv) {
+      const float* in = lv == 0 ? vol : coef[lv - 1];
+      launched(c, launch_wav_analysis(in, m >> lv, n >> lv, K >> lv, lv == 0 ? s : 0, coef[lv], bk, th[lv], c->st),
+               "wav_analysis");
+    }
+    for (int lv = levels - 1; lv >= 0; --lv) {
+      const float* approx = lv == levels - 1 ? coef[lv] : rec[lv + 1];
+      SynthOut o{};
+      if (lv == 0) {
+        o.out = vsum;
+        o.shift = s;
+        o.first = s == 0;
+        o.last = s == cycleSpin - 1;
+        o.cycles = (float)cycleSpin;
+      } else {
+        o.out = rec[lv];
+        o.shift = 0;
+        o.first = 1;
+        o.last = 0;
+        o.cycles = 1.f;
+      }
+      launched(c, launch_wav_synthesis(coef[lv], approx, m >> lv, n >> lv, K >> lv, o, bk, c->st), "wav_synthesis");
+    }
+  }
+  }
+  StageTimer tagg(c, 3);
+  float* wgt = buf<float>(c, "ht.wgt", (size_t)M * N);
+  launched(c, launch_ht_weights(vsum, m, n, M, N, d, K, cnt, wgt, c->st), "ht_weights");
+  AggArgs A{};
+  A.S = S;
+  A.cnt = cnt;
+  A.M = M;
+  A.N = N;
+  A.d = d;
+  A.d2 = d2;
+  A.K = K;
+  A.wiener = 0;
+  A.blocks = vsum;
+  A.gw = wgt;
+  std::vector<double> mk(d * d);
+  sine_window(d, 0.1, 0.9, mk.data());
+  for (int e = 0; e < d * d; ++e) A.win[e] = (float)mk[e];
+  A.m = m;
+  A.n = n;
+  A.U = U;
+  A.W = W;
+  launched(c, launch_aggregate(A, c->st), "aggregate");
+}
+
+void fill_wiener_consts(WienerArgs& A, int d, const double* sigma, int is_matrix, int variant) {
+  std::vector<double> Tm(d * d), Ti(d * d);
+  dct_matrices(d, Tm.data(), Ti.data());
+  for (int e = 0; e < d * d; ++e) {
+    A.T[e] = (float)Tm[e];
+    A.Ti[e] = variant == 0 ? (float)Ti[e] : (float)Tm[(e / d) + (e % d) * d];
+    const double s = is_matrix ? sigma[e] : sigma[0];
+    A.s2[e] = (float)(s * s);
+  }
+  A.clamp_one = variant == 1;
+}
+
+void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float* W) {
+  const int M = A.M, N = A.N, K = A.K;
+  if (!wiener_supported(d, K))
+    argfail(c, "unsupported (blockSizeWie, numMax) pair for the Wiener step", GBM3D_ERR_UNSUPPORTED);
+  A.out = buf<float>(c, "wie.out", (size_t)d * d * K * M * N);
+  A.n2 = buf<float>(c, "wie.n2", (size_t)M * N);
+  {
+    StageTimer t(c, 5);
+    launched(c, launch_wiener(d, A, c->st), "wiener");
+  }
+  StageTimer t(c, 6);
+  AggArgs G{};
+  G.S = A.S;
+  G.cnt = nullptr;
+  G.M = M;
+  G.N = N;
+  G.d = d;
+  G.d2 = d2;
+  G.K = K;
+  G.wiener = 1;
+  G.blocks = A.out;
+  G.gw = A.n2;
+  std::vector<double> wk(d * d);
+  sine_window(d, 0.2, 0.8, wk.data());
+  for (int e = 0; e < d * d; ++e) G.win[e] = (float)wk[e];
+  G.m = M * d;
+  G.n = N * d;
+  G.U = U;
+  G.W = W;
+  launched(c, launch_aggregate(G, c->st), "aggregate");
+}
+
+void to_host_double(gbm3d_ctx* c, const float* dsrc, size_t n, double* host) {
+  double* tmp = buf<double>(c, "io.f64", n);
+  k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>(dsrc, tmp, n);
+  launched(c, cudaGetLastError(), "f32_to_f64");
+  ck(c, cudaMemcpyAsync(host, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, c->st), "D2H");
+}
+
+template <class F>
+int guarded(gbm3d_ctx* c, F&& f) {
+  if (!c) return GBM3D_ERR_ARG;
+  c->err.clear();
+  try {
+    ck(c, cudaSetDevice(c->device), "cudaSetDevice");
+    c->launches = 0;
+    c->records.clear();
+    f();
+    return GBM3D_OK;
+  } catch (const Fail& e) {
+    return e.code;
+  } catch (const std::exception& e) {
+    set_err(c, e.what());
+    return GBM3D_ERR_CUDA;
+  }
+}
+
+void opts_dims(const gbm3d_opts* o, int& d, int& dw, int& d2, int& K) {
+  d = o->blockSize;
+  dw = o->blockSizeWie;
+  d2 = o->matchSize;
+  K = o->numMax;
+}
+
+// The whole GBM3D.m pipeline on device buffers.
+void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const gbm3d_opts* o, double* dU,
+              double* dU1) {
+  check_opts(c, o);
+  int d, dw, d2, K;
+  opts_dims(o, d, dw, d2, K);
+  check_match(c, d, d2, K);
+  if (o->Wiener) check_match(c, dw, d2, K);
+  if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
+  if (!(sigma >= 0) || !std::isfinite(sigma)) argfail(c, "sigma must be a finite non-negative scalar");
+  const int Mp = (m + d - 1) / d * d, Np = (n + d - 1) / d * d;
+  if (Mp - m > m || Np - n > n) argfail(c, "image smaller than the padding it needs");
+  if (Mp < d2 || Np < d2) argfail(c, "image smaller than matchSize");
+  if (o->Wiener && (Mp % dw || Np % dw)) argfail(c, "padded size must be a multiple of blockSizeWie");
+  const int nS = o->nMatchSpins, nW = o->Wiener ? o->nMatchSpinsWie : 0;
+  if (nS < 1 || nS > 8 || nW < 0 || nW > 8 || (o->Wiener && nW < 1)) argfail(c, "match spin count out of range");
+  const size_t px = (size_t)Mp * Np;
+  gbm3d_filters f;
+  bior(&f);
+  const WaveletBank bk = make_bank(c, &f);
+  std::vector<double> tau(o->levels * 7);
+  tau_table(o->levels, o->tauMode, tau.data());
+  for (auto& t : tau) t *= sigma;
+
+  StageTimer tall(c, 7);
+  float* If = buf<float>(c, "p.If", px);
+  {
+    StageTimer t(c, 0);
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    k_prep<<<grid2(Mp, Np), 256, 0, c->st>>>(dI, m, n, If, Mp, Np, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+  }
+
+  // step 1: hard-thresholding estimate over the match spins
+  const int M1 = Mp / d, N1 = Np / d;
+  uint32_t* S1 = buf<uint32_t>(c, "p.S1", (size_t)K * M1 * N1);
+  int32_t* cnt1 = buf<int32_t>(c, "p.cnt1", (size_t)M1 * N1);
+  float* vol = buf<float>(c, "p.vol", px * K);
+  float* Us = buf<float>(c, "p.Us", px);
+  float* Ws = buf<float>(c, "p.Ws", px);
+  double* Ua = buf<double>(c, "p.Ua", px);
+  double* Wa = buf<double>(c, "p.Wa", px);
+  const bool stale = o->Wiener && o->staleWeights && nW < nS;
+  float* Wstale = stale ? buf<float>(c, "p.Wstale", px * (nS - nW)) : nullptr;
+  for (int ii = 0; ii < nS; ++ii) {
+    const int s = o->matchSpins[ii];
+    {
+      StageTimer t(c, 1);
+      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1");
+    }
+    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws);
+    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
+    launched(c, cudaGetLastError(), "accum");
+    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa, ii == 0);
+    launched(c, cudaGetLastError(), "accum");
+    if (stale && ii >= nW) {
+      k_shift_copy<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wstale + (size_t)(ii - nW) * px);
+      launched(c, cudaGetLastError(), "shift_copy");
+    }
+  }
+  double* U1d = buf<double>(c, "p.U1d", px);
+  float* U1f = buf<float>(c, "p.U1f", px);
+  k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua, Wa, Mp, Np, U1d, U1f, dU1, m, n);
+  launched(c, cudaGetLastError(), "ratio");
+  if (!o->Wiener) {
+    k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua, Wa, Mp, Np, nullptr, nullptr, dU, m, n);
+    launched(c, cudaGetLastError(), "ratio");
+    return;
+  }
+
+  // step 2: empirical Wiener estimate over the Wiener match spins
+  const int M2 = Mp / dw, N2 = Np / dw;
+  uint32_t* S2 = buf<uint32_t>(c, "p.S2", (size_t)K * M2 * N2);
+  for (int ii = 0; ii < nW; ++ii) {
+    const int s = o->matchSpinsWie[ii];
+    {
+      StageTimer t(c, 4);
+      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2");
+    }
+    float* padP = buf<float>(c, "m2.pad", 1);  // the pilot search image run_match just built
+    float* padN = buf<float>(c, "m2.padN", (size_t)pitch4(Mp + d2) * (Np + d2));
+    launched(c, launch_make_pad(If, Mp, Np, d2, s, padN, pitch4(Mp + d2), c->st), "make_pad");
+    WienerArgs A{};
+    A.padP = padP;
+    A.padN = padN;
+    A.P = pitch4(Mp + d2);
+    A.d2 = d2;
+    A.S = S2;
+    A.M = M2;
+    A.N = N2;
+    A.K = K;
+    double sg = sigma;
+    fill_wiener_consts(A, dw, &sg, 0, 0);
+    run_wiener_agg(c, A, dw, d2, Us, Ws);
+    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
+    launched(c, cudaGetLastError(), "accum");
+    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa, ii == 0);
+    launched(c, cudaGetLastError(), "accum");
+  }
+  if (stale)
+    for (int ii = nW; ii < nS; ++ii) {
+      k_add_f<<<(unsigned)((px + 255) / 256), 256, 0, c->st>>>(Wstale + (size_t)(ii - nW) * px, Wa, px);
+      launched(c, cudaGetLastError(), "add");
+    }
+  k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua, Wa, Mp, Np, nullptr, nullptr, dU, m, n);
+  launched(c, cudaGetLastError(), "ratio");
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+int gbm3d_version(void) { return 100; }
+
+int gbm3d_ctx_create(int device, gbm3d_ctx** out) {
+  if (!out) return GBM3D_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) return GBM3D_ERR_CUDA;
+  if (device < 0 || device >= n) return GBM3D_ERR_ARG;
+  gbm3d_ctx* c = new gbm3d_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->flag, sizeof(int)) != cudaSuccess) {
+    delete c;
+    return GBM3D_ERR_CUDA;
+  }
+  c->st = c->own;
+  *out = c;
+  return GBM3D_OK;
+}
+
+void gbm3d_ctx_destroy(gbm3d_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->st);
+  for (auto& kv : c->bufs) cudaFree(kv.second.first);
+  for (auto& e : c->evpool) cudaEventDestroy(e);
+  if (c->flag) cudaFree(c->flag);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+int gbm3d_ctx_set_stream(gbm3d_ctx* c, void* s) {
+  if (!c) return GBM3D_ERR_ARG;
+  c->st = s ? (cudaStream_t)s : c->own;
+  return GBM3D_OK;
+}
+
+const char* gbm3d_last_error(const gbm3d_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int gbm3d_ctx_enable_timing(gbm3d_ctx* c, int on) {
+  if (!c) return GBM3D_ERR_ARG;
+  c->timing = on != 0;
+  return GBM3D_OK;
+}
+
+int gbm3d_stage_times(const gbm3d_ctx* c, float* ms, int n) {
+  if (!c || !ms || !c->timing) return 0;
+  float acc[8] = {};
+  for (const auto& r : c->records) {
+    float t = 0.f;
+    if (cudaEventSynchronize(c->evpool[r.second + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&t, c->evpool[r.second], c->evpool[r.second + 1]) != cudaSuccess)
+      return -1;
+    acc[r.first] += t;
+  }
+  int k = 0;
+  for (; k < n && k < 8; ++k) ms[k] = acc[k];
+  return k;
+}
+
+int gbm3d_last_launch_count(const gbm3d_ctx* c) { return c ? c->launches : 0; }
+
+void gbm3d_default_opts(const char* profile, gbm3d_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  std::string p = profile ? profile : "default";
+  o->numMax = 16;
+  o->numMin = 16;
+  o->levels = 3;
+  o->cycleSpin = 2;
+  o->tauMode = 1;
+  o->blockSize = 16;
+  o->blockSizeWie = 8;
+  o->matchSize = 32;
+  o->Wiener = 1;
+  o->filtType = 0;
+  o->staleWeights = 1;
+  auto spins = [](int* dst, int& cnt, std::initializer_list<int> v) {
+    cnt = 0;
+    for (int s : v) dst[cnt++] = s;
+  };
+  if (p == "fast") {
+    spins(o->matchSpins, o->nMatchSpins, {0, 4, 6});
+    spins(o->matchSpinsWie, o->nMatchSpinsWie, {0});
+  } else if (p == "superFast") {
+    spins(o->matchSpins, o->nMatchSpins, {0, 4, 6});
+    spins(o->matchSpinsWie, o->nMatchSpinsWie, {0});
+    o->blockSize = 32;
+    o->Wiener = 0;
+  } else if (p == "accuracy") {
+    spins(o->matchSpins, o->nMatchSpins, {0, 4, 6});
+    spins(o->matchSpinsWie, o->nMatchSpinsWie, {0, 4, 6});
+  } else {
+    spins(o->matchSpins, o->nMatchSpins, {0, 4});
+    spins(o->matchSpinsWie, o->nMatchSpinsWie, {0, 4});
+  }
+}
+
+void gbm3d_get_tau(int levels, int mode, double* tau) {
+  if (tau && levels > 0) tau_table(levels, mode, tau);
+}
+
+void gbm3d_bior_filters(gbm3d_filters* f) {
+  if (f) bior(f);
+}
+
+int gbm3d_matchBlocksCPU(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
+                         uint32_t* S, int32_t* S_count, float* Volume) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    const int d = o->blockSize, d2 = o->matchSize, K = o->numMax;
+    check_match(c, d, d2, K);
+    if (!I || !S) argfail(c, "I and S are required");
+    if (m < d2 || n < d2 || m < d || n < d) argfail(c, "image smaller than matchSize");
+    const int M = m / d, N = n / d;
+    const size_t px = (size_t)m * n;
+    double* dI = buf<double>(c, "io.I", px);
+    ck(c, cudaMemcpyAsync(dI, I, px * sizeof(double), cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    float* If = buf<float>(c, "io.If", px);
+    k_prep<<<grid2(m, n), 256, 0, c->st>>>(dI, m, n, If, m, n, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    int32_t* dc = buf<int32_t>(c, "io.cnt", (size_t)M * N);
+    float* dV = nullptr;
+    if (Volume) {
+      dV = buf<float>(c, "io.V", px * K);
+      ck(c, cudaMemsetAsync(dV, 0, px * K * sizeof(float), c->st), "memset");
+    }
+    run_match(c, If, nullptr, m, n, 0, d, d2, K, o->numMin, sigma, dS, dc, dV, nullptr, nullptr, "m1");
+    ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (S_count) ck(c, cudaMemcpyAsync(S_count, dc, (size_t)M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (Volume) ck(c, cudaMemcpyAsync(Volume, dV, px * K * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+  });
+}
+
+int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* c, const float* Volume, const uint32_t* S, const int32_t* S_count,
+                                 int M, int N, const double* tau, const gbm3d_filters* f, const gbm3d_opts* o,
+                                 double* U, double* W) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    if (!Volume || !S || !tau || !U || !W) argfail(c, "missing argument");
+    const int d = o->blockSize, d2 = o->matchSize, K = o->numMax;
+    if (M < 1 || N < 1) argfail(c, "empty match set");
+    gbm3d_filters fb;
+    if (f) fb = *f; else bior(&fb);
+    const WaveletBank bk = make_bank(c, &fb);
+    const int m = M * d, n = N * d;
+    const size_t px = (size_t)m * n;
+    float* dV = buf<float>(c, "io.V", px * K);
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    int32_t* dc = nullptr;
+    ck(c, cudaMemcpyAsync(dV, Volume, px * K * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemcpyAsync(dS, S, (size_t)K * M * N * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    if (S_count) {
+      dc = buf<int32_t>(c, "io.cnt", (size_t)M * N);
+      ck(c, cudaMemcpyAsync(dc, S_count, (size_t)M * N * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    }
+    float* dU = buf<float>(c, "io.U", px);
+    float* dW = buf<float>(c, "io.W", px);
+    run_ht(c, dV, dS, dc, M, N, d, d2, K, o->levels, o->cycleSpin, tau, bk, dU, dW);
+    to_host_double(c, dU, px, U);
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    to_host_double(c, dW, px, W);
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+  });
+}
+
+int gbm3d_matchBlocksWie(gbm3d_ctx* c, const double* I, const double* In, int m, int n, double sigma,
+                         const gbm3d_opts* o, uint32_t* S, float* V1, float* V2) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    const int d = o->blockSizeWie, d2 = o->matchSize, K = o->numMax;
+    check_match(c, d, d2, K);
+    if (!I || !In || !S) argfail(c, "missing argument");
+    if (m < d2 || n < d2) argfail(c, "image smaller than matchSize");
+    const int M = m / d, N = n / d;
+    const size_t px = (size_t)m * n, gs = (size_t)d * d * K * M * N;
+    double* dI = buf<double>(c, "io.I", px);
+    double* dIn = buf<double>(c, "io.In", px);
+    ck(c, cudaMemcpyAsync(dI, I, px * 8, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemcpyAsync(dIn, In, px * 8, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    float* If = buf<float>(c, "io.If", px);
+    float* Inf = buf<float>(c, "io.Inf", px);
+    k_prep<<<grid2(m, n), 256, 0, c->st>>>(dI, m, n, If, m, n, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+    k_prep<<<grid2(m, n), 256, 0, c->st>>>(dIn, m, n, Inf, m, n, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    float* d1 = V1 ? buf<float>(c, "io.V1", gs) : nullptr;
+    float* d2p = V2 ? buf<float>(c, "io.V2", gs) : nullptr;
+    run_match(c, If, V2 ? Inf : nullptr, m, n, 0, d, d2, K, K, sigma, dS, nullptr, nullptr, d1, d2p, "m2");
+    ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (V1) ck(c, cudaMemcpyAsync(V1, d1, gs * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (V2) ck(c, cudaMemcpyAsync(V2, d2p, gs * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+  });
+}
+
+static int wiener_entry(gbm3d_ctx* c, const float* V1, const float* V2, const uint32_t* S, int M, int N,
+                        const double* sigma, int is_matrix, const gbm3d_opts* o, double* U, double* W,
+                        int variant) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    if (!V1 || !V2 || !S || !sigma || !U || !W) argfail(c, "missing argument");
+    const int d = o->blockSizeWie, d2 = o->matchSize, K = o->numMax;
+    if (M < 1 || N < 1) argfail(c, "empty match set");
+    if (d * d > 256) argfail(c, "blockSizeWie too large", GBM3D_ERR_UNSUPPORTED);
+    const size_t gs = (size_t)d * d * K * M * N, px = (size_t)M * d * N * d;
+    float* d1 = buf<float>(c, "io.V1", gs);
+    float* d2p = buf<float>(c, "io.V2", gs);
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    ck(c, cudaMemcpyAsync(d1, V1, gs * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemcpyAsync(d2p, V2, gs * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemcpyAsync(dS, S, (size_t)K * M * N * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    WienerArgs A{};
+    A.V1 = d1;
+    A.V2 = d2p;
+    A.S = dS;
+    A.M = M;
+    A.N = N;
+    A.K = K;
+    A.d2 = d2;
+    fill_wiener_consts(A, d, sigma, is_matrix, variant);
+    float* dU = buf<float>(c, "io.U", px);
+    float* dW = buf<float>(c, "io.W", px);
+    run_wiener_agg(c, A, d, d2, dU, dW);
+    to_host_double(c, dU, px, U);
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    to_host_double(c, dW, px, W);
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+  });
+}
+
+int gbm3d_denoiseAndAggregateWieFast(gbm3d_ctx* c, const float* V1, const float* V2, const uint32_t* S, int M,
+                                     int N, const double* sigma, int is_matrix, const gbm3d_opts* o, double* U,
+                                     double* W) {
+  return wiener_entry(c, V1, V2, S, M, N, sigma, is_matrix, o, U, W, 0);
+}
+
+int gbm3d_denoiseAndAggregateWie(gbm3d_ctx* c, const float* V1, const float* V2, const uint32_t* S, int M, int N,
+                                 double sigma, const gbm3d_opts* o, double* U, double* W) {
+  return wiener_entry(c, V1, V2, S, M, N, &sigma, 0, o, U, W, 1);
+}
+
+int gbm3d_denoise_device(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
+                         double* U, double* U1) {
+  return guarded(c, [&] {
+    if (!I || !U) argfail(c, "missing argument");
+    pipeline(c, I, m, n, sigma, o, U, U1);
+  });
+}
+
+int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,
+                  double* U1) {
+  return guarded(c, [&] {
+    if (!I || !U) argfail(c, "missing argument");
+    if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
+    const size_t px = (size_t)m * n;
+    double* dI = buf<double>(c, "h.I", px);
+    double* dU = buf<double>(c, "h.U", px);
+    double* dU1 = U1 ? buf<double>(c, "h.U1", px) : nullptr;
+    ck(c, cudaMemcpyAsync(dI, I, px * 8, cudaMemcpyHostToDevice, c->st), "H2D");
+    pipeline(c, dI, m, n, sigma, o, dU, dU1);
+    ck(c, cudaMemcpyAsync(U, dU, px * 8, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (U1) ck(c, cudaMemcpyAsync(U1, dU1, px * 8, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+  });
+}
+
+}  // extern "C"

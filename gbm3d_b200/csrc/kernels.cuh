@@ -1,0 +1,95 @@
+// Launch interfaces of the GBM3D kernels (host side of each .cu file).
+#pragma once
+#include "common.cuh"
+
+namespace gbm3d {
+
+// ---- block matching (match.cu) ----------------------------------------------
+struct MatchArgs {
+  const float* pad;   // padded search image of the matched image, pitch P
+  const float* pad2;  // padded search image gathered into V2 (may be null)
+  int P;              // column pitch of pad/pad2 in floats
+  int M, N, K;        // reference grid and group size
+  int numMin;         // tolerance branch: minimum group size
+  float tol;          // tolerance on ssd/||xR||^2
+  int tol_branch;     // numMin != numMax
+  uint32_t* S;        // K x M x N
+  int32_t* cnt;       // M x N (may be null)
+  float* volume;      // m x n x K gather (may be null)
+  int m, n;           // image size for the volume gather
+  float* V1;          // d x d x K x M x N gathers (may be null)
+  float* V2;
+};
+bool match_supported(int d, int d2);
+size_t match_smem_bytes(int d, int d2);
+cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st);
+cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
+                            cudaStream_t st);
+
+// ---- step 1: global 3D wavelet hard thresholding (wavelet.cu) ----------------
+struct WaveletBank {
+  AxisBank xy, z;
+  int reach_a;  // largest analysis tap index on the spatial axes
+  int reach_s;  // largest synthesis tap index on the spatial axes
+};
+struct LevelBands {
+  float tau[8];  // hard threshold per band code (code 0 unused)
+};
+// Analysis of one level + hard threshold.  in: Ly x Lx x Lz, read at
+// ((y-shift) mod Ly, (x-shift) mod Lx, (z-shift) mod Lz).  out: 8 bands, band
+// code fy + 2 fx + 4 fz, each (Ly/2)(Lx/2)(Lz/2) floats.
+cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
+                                const WaveletBank& bk, const LevelBands& th, cudaStream_t st);
+// Synthesis of one level: bands (codes 1..7) + approx -> out (Oy x Ox x Oz).
+// mode 0: out[p] = v; with shift_out, the value for p lands at p - shift_out.
+// Level-1 cycle-spin accumulation: first (store) / middle (add) / last
+// (add, divide by cycle count, clamp at 0).
+struct SynthOut {
+  float* out;
+  int shift;
+  int first, last;
+  float cycles;
+};
+cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy, int Ox, int Oz,
+                                 const SynthOut& o, const WaveletBank& bk, cudaStream_t st);
+// Aggregation weight 1/(TV(group)+eps) per group of the image-shaped Vavg.
+cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int d, int K,
+                              const int32_t* cnt, float* wgt, cudaStream_t st);
+
+// ---- step 2: empirical Wiener (wiener.cu) --------------------------------------
+struct WienerArgs {
+  // group sources: either gathered from padded images through S, or read from
+  // V1/V2 arrays (d x d x K x M x N)
+  const float* padP;  // pilot search image (pitch P) or null
+  const float* padN;  // noisy search image
+  int P, d2;
+  const float* V1;
+  const float* V2;
+  const uint32_t* S;
+  int M, N, K;
+  float s2[256];      // sigma^2 per DCT coefficient (d x d), single precision
+  float T[256];       // DCT-II matrix (d x d, column-major)
+  float Ti[256];      // inverse used by the inverse transform
+  int clamp_one;      // legacy variant: clamp to [0,1]
+  float* out;         // filtered groups, d x d x K x M x N
+  float* n2;          // ||filt||^2 per group (sqrt then square, single)
+};
+bool wiener_supported(int d, int K);
+cudaError_t launch_wiener(int d, const WienerArgs& A, cudaStream_t st);
+
+// ---- owner-ordered aggregation (aggregate.cu) ------------------------------------
+struct AggArgs {
+  const uint32_t* S;
+  const int32_t* cnt;   // may be null (every group holds K)
+  int M, N, d, d2, K;
+  int wiener;           // 0: step-1 weights (scalar x mask); 1: step-2 (window / n2)
+  const float* blocks;  // step 1: image-shaped Vavg (m x n x K); step 2: d x d x K per group
+  const float* gw;      // step 1: weight per group; step 2: n2 per group
+  float win[1024];      // step 1: mask; step 2: Wiener window (d x d)
+  int m, n;             // output size (m = M*d, n = N*d)
+  float* U;             // m x n
+  float* W;
+};
+cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st);
+
+}  // namespace gbm3d

@@ -1,0 +1,236 @@
+// Block matching — the search of matchBlocksCPU.m:21-116 and matchBlocksWie.m:21-92.
+//
+// One warp per reference block.  The block's search window (d+d2-1)^2 of the
+// padded image sits in shared memory; lane a owns the d2 candidates with row
+// offset a (one per column offset b) and streams the window rows a+r past its
+// d2 accumulators, so every shared-memory read of a warp touches 32
+// consecutive words.  The reference block itself is read from the window
+// (it is the candidate at offset (d2/2, d2/2)) by warp-uniform broadcasts.
+//
+// Distances are exact FP32 sums of squared differences, row-major over the
+// block: t = x - y; acc = fmaf(t, t, acc).  The K best candidates are the K
+// smallest (distance, column-major window index) pairs — the stable order of
+// MATLAB's mink — found by a bitwise radix search for the K-th smallest
+// distance with warp reductions, then an index-ordered pick among ties.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace gbm3d {
+
+// Ipad of the reference for a circularly shifted image: rows (m+d2), cols
+// (n+d2), column pitch P floats.  spin is the circshift applied to the image.
+__global__ void k_make_pad(const float* __restrict__ img, int m, int n, int h, int spin,
+                           float* __restrict__ pad, int P, int R, int Q) {
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  const int x = blockIdx.y;
+  if (y >= R || x >= Q) return;
+  const int sr = pmod(pad_index(y, m, h) - spin, m);
+  const int sc = pmod(pad_index(x, n, h) - spin, n);
+  pad[y + (size_t)x * P] = img[sr + (size_t)sc * m];
+}
+
+template <int D, int D2>
+__global__ void __launch_bounds__(128) k_match(MatchArgs A) {
+  constexpr int WD = D + D2 - 1;  // window rows/cols that candidates touch
+  constexpr int H = D2 / 2;
+  extern __shared__ float smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* win = smem + warp * (WD * WD);
+  uint32_t* lst = reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 96;  // keys, idx, S
+  const int g = blockIdx.x * 4 + warp;
+  if (g >= A.M * A.N) return;  // warp-uniform
+  const int i = g % A.M, j = g / A.M;
+
+  // ---- stage the search window (column-major, stride WD) --------------------
+  const float* src = A.pad + (size_t)i * D + (size_t)j * D * A.P;
+  for (int c = 0; c < WD; ++c)
+    for (int r = lane; r < WD; r += 32) win[r + c * WD] = src[r + (size_t)c * A.P];
+  __syncwarp();
+
+  // ---- exact SSD for the lane's candidates (a = lane, b = 0..D2-1) ----------
+  float acc[D2];
+#pragma unroll
+  for (int b = 0; b < D2; ++b) acc[b] = 0.f;
+  const int a = lane < D2 ? lane : 0;
+#pragma unroll 1
+  for (int r = 0; r < D; ++r) {
+    float xr[D];
+#pragma unroll
+    for (int c = 0; c < D; ++c) xr[c] = win[(H + r) + (H + c) * WD];
+    const float* wrow = win + (a + r);
+#pragma unroll
+    for (int xw = 0; xw < WD; ++xw) {
+      const float w = wrow[xw * WD];
+#pragma unroll
+      for (int b = 0; b < D2; ++b) {
+        const int c = xw - b;
+        if (c >= 0 && c < D) {
+          const float t = xr[c] - w;
+          acc[b] = fmaf(t, t, acc[b]);
+        }
+      }
+    }
+  }
+
+  // ---- selection -------------------------------------------------------------
+  const unsigned FULL = 0xffffffffu;
+  uint32_t key[D2];
+#pragma unroll
+  for (int b = 0; b < D2; ++b) key[b] = lane < D2 ? __float_as_uint(acc[b]) : 0xffffffffu;
+  const int K = A.K;
+  uint32_t selmask = 0;
+  int count = K;
+  bool index_order = false;  // tolerance branch with numMin <= #found <= numMax
+  int want = K;
+  if (A.tol_branch) {
+    // matchBlocksCPU.m:89-99: D = ssd/||xR||^2 compared with tol.
+    float nR = 0.f;
+    for (int c = 0; c < D; ++c)
+      for (int r = 0; r < D; ++r) {
+        const float xv = win[(H + r) + (H + c) * WD];
+        nR = fmaf(xv, xv, nR);
+      }
+    int nf = 0;
+#pragma unroll
+    for (int b = 0; b < D2; ++b)
+      if (lane < D2 && __uint_as_float(key[b]) / nR < A.tol) { selmask |= 1u << b; ++nf; }
+    const int found = __reduce_add_sync(FULL, nf);
+    if (found > K) { want = K; selmask = 0; }
+    else if (found < A.numMin) { want = A.numMin; selmask = 0; }
+    else { index_order = true; count = found; }
+    if (!index_order) count = want;
+  }
+  if (!index_order) {
+    // radix search for v* = the want-th smallest key (keys are >= +0 floats)
+    uint32_t p = 0;
+#pragma unroll 1
+    for (int bit = 30; bit >= 0; --bit) {
+      const uint32_t t = p | ((1u << bit) - 1u);
+      int c = 0;
+#pragma unroll
+      for (int b = 0; b < D2; ++b) c += key[b] <= t ? 1 : 0;
+      if (__reduce_add_sync(FULL, c) < want) p |= 1u << bit;
+    }
+    int lt = 0;
+#pragma unroll
+    for (int b = 0; b < D2; ++b)
+      if (key[b] < p) { selmask |= 1u << b; ++lt; }
+    const int need = want - __reduce_add_sync(FULL, lt);
+    // ties at v*: lowest column-major index first (b major, a = lane minor)
+    int taken = 0;
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int b = 0; b < D2; ++b) {
+      const unsigned eq = __ballot_sync(FULL, key[b] == p);
+      if (taken < need && eq) {
+        const bool mine = (eq >> lane) & 1u;
+        if (mine && taken + __popc(eq & below) < need) selmask |= 1u << b;
+        taken += __popc(eq);
+      }
+    }
+  }
+
+  // ---- order the selection and write S ---------------------------------------
+  uint32_t* lkey = lst;
+  uint32_t* lidx = lst + 32;
+  uint32_t* lS = lst + 64;
+  int mine = __popc(selmask);
+  int pos = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(FULL, pos, o);
+    if (lane >= o) pos += v;
+  }
+  pos -= mine;
+#pragma unroll
+  for (int b = 0; b < D2; ++b)
+    if ((selmask >> b) & 1u) {
+      lkey[pos] = key[b];
+      lidx[pos] = (uint32_t)(a + b * D2);
+      ++pos;
+    }
+  __syncwarp();
+  const uint32_t ref_idx = (uint32_t)(H + H * D2 + 1);  // matchBlocksCPU.m:103
+  if (lane < count) {
+    const uint32_t kv = lkey[lane], ix = lidx[lane];
+    int rank = 0;
+    for (int t = 0; t < count; ++t) {
+      const uint32_t k2 = lkey[t], i2 = lidx[t];
+      if (index_order) rank += i2 < ix ? 1 : 0;
+      else rank += (k2 < kv || (k2 == kv && i2 < ix)) ? 1 : 0;
+    }
+    lS[rank] = rank == 0 ? ref_idx : ix + 1;
+  }
+  __syncwarp();
+  uint32_t* Sg = A.S + (size_t)g * K;
+  if (lane < K) Sg[lane] = lane < count ? lS[lane] : 0u;
+  if (lane == 0 && A.cnt) A.cnt[g] = count;
+
+  // ---- optional gathers: Volume (matchBlocksCPU.m:107-114), V1/V2 (matchBlocksWie.m:85-89)
+  if (A.volume) {
+    const size_t mn = (size_t)A.m * A.n;
+    for (int k = 0; k < K; ++k) {
+      int aa = H, bb = H;
+      if (k < count) { const int e = (int)lS[k] - 1; aa = e % D2; bb = e / D2; }
+      for (int c = 0; c < D; ++c)
+        for (int r = lane; r < D; r += 32)
+          A.volume[(size_t)(i * D + r) + (size_t)A.m * (j * D + c) + mn * k] = win[(aa + r) + (bb + c) * WD];
+    }
+  }
+  if (A.V1 || A.V2) {
+    const float* src2 = A.pad2 + (size_t)i * D + (size_t)j * D * A.P;
+    for (int k = 0; k < K; ++k) {
+      const int e = (int)lS[k] - 1, aa = e % D2, bb = e / D2;
+      float* o1 = A.V1 ? A.V1 + (size_t)D * D * (k + (size_t)K * g) : nullptr;
+      float* o2 = A.V2 ? A.V2 + (size_t)D * D * (k + (size_t)K * g) : nullptr;
+      for (int t = lane; t < D * D; t += 32) {
+        const int r = t % D, c = t / D;
+        if (o1) o1[t] = win[(aa + r) + (bb + c) * WD];
+        if (o2) o2[t] = src2[(aa + r) + (size_t)(bb + c) * A.P];
+      }
+    }
+  }
+}
+
+size_t match_smem_bytes(int d, int d2) {
+  const int wd = d + d2 - 1;
+  return (size_t)4 * wd * wd * sizeof(float) + 4 * 96 * sizeof(uint32_t);
+}
+
+template <int D, int D2>
+static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
+  const size_t sm = match_smem_bytes(D, D2);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_match<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int G = A.M * A.N;
+  k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(A);
+  return cudaGetLastError();
+}
+
+bool match_supported(int d, int d2) {
+  return (d == 8 || d == 16 || d == 32) && (d2 == 16 || d2 == 24 || d2 == 32);
+}
+
+cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st) {
+#define GBM3D_MATCH_CASE(DD, DD2) \
+  if (d == DD && d2 == DD2) return launch_match_t<DD, DD2>(A, st);
+  GBM3D_MATCH_CASE(8, 16) GBM3D_MATCH_CASE(8, 24) GBM3D_MATCH_CASE(8, 32)
+  GBM3D_MATCH_CASE(16, 16) GBM3D_MATCH_CASE(16, 24) GBM3D_MATCH_CASE(16, 32)
+  GBM3D_MATCH_CASE(32, 16) GBM3D_MATCH_CASE(32, 24) GBM3D_MATCH_CASE(32, 32)
+#undef GBM3D_MATCH_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
+                            cudaStream_t st) {
+  const int R = m + d2, Q = n + d2;
+  dim3 grid((R + 255) / 256, Q);
+  k_make_pad<<<grid, 256, 0, st>>>(img, m, n, d2 / 2, spin, pad, P, R, Q);
+  return cudaGetLastError();
+}
+
+}  // namespace gbm3d

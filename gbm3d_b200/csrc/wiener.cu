@@ -1,0 +1,236 @@
+// Step 2: empirical Wiener collaborative filter, one warp per group.
+//
+// Restates denoiseAndAggregateWieFast.m:23-81 with myWavDec1D.m:10-26 and
+// myWavRec1D.m:6-26 (and the legacy denoiseAndAggregateWie.m:16-90 when
+// clamp_one is set and Ti is the transposed DCT).  Per group (d x d x K):
+//   gather pilot (V1) and noisy (V2) blocks through S, or read them from
+//   V1/V2 arrays;
+//   page-wise DCT  Y = T X T'           (pagemtimes, serial fmaf chains)
+//   circular Haar along the slots, 3 levels (2 when K < 16);
+//   filt = |Y1|^2 / (|Y1|^2 + sigma^2), filt(1,1,15:end) = 1;
+//   Y2 .* filt, inverse Haar, X = Ti (Y Ti'), clamp max(.,0) (and min(.,1));
+//   n2 = norm(filt)^2 with the fixed 32-way reduction order, sqrt then square.
+// The filtered groups and n2 feed the owner-ordered aggregation kernel.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace gbm3d {
+
+// Circular Haar of K slots, LV = 3 levels (2 when K < 16), in registers.
+// Detail of level lv at q: fmaf(cc, u[2q-1 mod L], -cc*u[2q]); approximation
+// fmaf(cc, u[2q-1 mod L], cc*u[2q]).  Output layout: level-1 details,
+// level-2 details, ..., approximation (myWavDec1D.m:14-25).
+template <int K>
+__device__ __forceinline__ void haar_dec(float* v, float cc) {
+  constexpr int LV = K < 16 ? 2 : 3;
+  float out[K];
+  float U[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) U[q] = v[q];
+#pragma unroll
+  for (int lv = 0; lv < LV; ++lv) {
+    const int L = K >> lv, cntp = K - L;
+    float a[K / 2];
+#pragma unroll
+    for (int q = 0; q < L / 2; ++q) {
+      const float u0 = U[2 * q], u1 = U[q == 0 ? L - 1 : 2 * q - 1];
+      out[cntp + q] = fmaf(cc, u1, (-cc) * u0);
+      a[q] = fmaf(cc, u1, cc * u0);
+    }
+#pragma unroll
+    for (int q = 0; q < L / 2; ++q) U[q] = a[q];
+  }
+  constexpr int LA = K >> LV;
+#pragma unroll
+  for (int q = 0; q < LA; ++q) out[K - LA + q] = U[q];
+#pragma unroll
+  for (int q = 0; q < K; ++q) v[q] = out[q];
+}
+
+// Inverse of haar_dec (myWavRec1D.m:10-25): at each level, the detail
+// contribution and the upsampled approximation contribution are formed
+// separately and then added.
+template <int K>
+__device__ __forceinline__ void haar_rec(float* v, float cc) {
+  constexpr int LV = K < 16 ? 2 : 3;
+  float R[K];
+#pragma unroll
+  for (int q = 0; q < (K >> LV); ++q) R[q] = v[K - (K >> LV) + q];
+#pragma unroll
+  for (int s = 0; s < LV; ++s) {
+    const int lv = LV - 1 - s;
+    const int L = K >> (lv + 1), Lo = 2 * L, off = K - (K >> lv);
+    float o[K];
+#pragma unroll
+    for (int q = 0; q < L; ++q) {
+      const float dd = v[off + q];
+      o[2 * q] = ((-cc) * dd) + (cc * R[q]);
+      o[q == 0 ? Lo - 1 : 2 * q - 1] = (cc * dd) + (cc * R[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < Lo; ++q) R[q] = o[q];
+  }
+#pragma unroll
+  for (int q = 0; q < K; ++q) v[q] = R[q];
+}
+
+template <int D, int K>
+__global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
+  constexpr int DD = D * D, GS = DD * K;
+  extern __shared__ float sm[];
+  float* Tm = sm;
+  float* Ti = sm + DD;
+  float* s2 = sm + 2 * DD;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* bA = sm + 3 * DD + warp * 3 * GS;
+  float* bB = bA + GS;
+  float* bC = bB + GS;
+  for (int t = threadIdx.x; t < DD; t += blockDim.x) {
+    Tm[t] = A.T[t];
+    Ti[t] = A.Ti[t];
+    s2[t] = A.s2[t];
+  }
+  __syncthreads();
+  const int g = blockIdx.x * 4 + warp;
+  if (g >= A.M * A.N) return;
+  const float cc = 0.70710678118654752440f;
+
+  // ---- load the two groups -----------------------------------------------
+  if (A.padP) {
+    const int i = g % A.M, j = g / A.M;
+    for (int k = 0; k < K; ++k) {
+      const int e = (int)A.S[(size_t)g * K + k] - 1, a = e % A.d2, b = e / A.d2;
+      const size_t o = (size_t)(i * D + a) + (size_t)(j * D + b) * A.P;
+      for (int t = lane; t < DD; t += 32) {
+        const int r = t % D, c = t / D;
+        bA[k * DD + t] = A.padP[o + r + (size_t)c * A.P];
+        bB[k * DD + t] = A.padN[o + r + (size_t)c * A.P];
+      }
+    }
+  } else {
+    const float* v1 = A.V1 + (size_t)g * GS;
+    const float* v2 = A.V2 + (size_t)g * GS;
+    for (int t = lane; t < GS; t += 32) {
+      bA[t] = v1[t];
+      bB[t] = v2[t];
+    }
+  }
+  __syncwarp();
+
+  // ---- forward DCT of each slot page: task (k, r) produces row r of T X T'
+  auto fwd = [&](const float* X, float* Y) {
+    for (int task = lane; task < K * D; task += 32) {
+      const int k = task / D, r = task % D;
+      const float* x = X + k * DD;
+      float P[D];
+#pragma unroll
+      for (int n = 0; n < D; ++n) {
+        float acc = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < D; ++jj) acc = fmaf(Tm[r + jj * D], x[jj + n * D], acc);
+        P[n] = acc;
+      }
+#pragma unroll
+      for (int l = 0; l < D; ++l) {
+        float acc = 0.f;
+#pragma unroll
+        for (int n = 0; n < D; ++n) acc = fmaf(P[n], Tm[l + n * D], acc);
+        Y[k * DD + r + l * D] = acc;
+      }
+    }
+  };
+  fwd(bA, bC);  // pilot coefficients -> bC
+  __syncwarp();
+  fwd(bB, bA);  // noisy coefficients -> bA
+  __syncwarp();
+
+  // ---- Haar along slots, Wiener gain, inverse Haar (lane per coefficient) ----
+  for (int e = lane; e < DD; e += 32) {
+    float v1[K], v2[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      v1[k] = bC[k * DD + e];
+      v2[k] = bA[k * DD + e];
+    }
+    haar_dec<K>(v1, cc);
+    haar_dec<K>(v2, cc);
+    const float sg = s2[e];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float p = v1[k] * v1[k];
+      float f = p / (p + sg);
+      if (e == 0 && k >= 14) f = 1.f;
+      bB[k * DD + e] = f;
+      v2[k] = v2[k] * f;
+    }
+    haar_rec<K>(v2, cc);
+#pragma unroll
+    for (int k = 0; k < K; ++k) bA[k * DD + e] = v2[k];
+  }
+  __syncwarp();
+
+  // ---- n2 = norm(col(filt))^2 ------------------------------------------------
+  float s = 0.f;
+  for (int e = lane; e < GS; e += 32) s = s + bB[e] * bB[e];
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) {
+    const float nr = sqrtf(s);
+    A.n2[g] = nr * nr;
+  }
+
+  // ---- inverse DCT: P = Y Ti' (rows), X = Ti P (columns) ----------------------
+  for (int task = lane; task < K * D; task += 32) {
+    const int k = task / D, r = task % D;
+    const float* y = bA + k * DD;
+    float Prow[D];
+#pragma unroll
+    for (int l = 0; l < D; ++l) {
+      float acc = 0.f;
+#pragma unroll
+      for (int n = 0; n < D; ++n) acc = fmaf(y[r + n * D], Ti[l + n * D], acc);
+      Prow[l] = acc;
+    }
+#pragma unroll
+    for (int l = 0; l < D; ++l) bC[k * DD + r + l * D] = Prow[l];
+  }
+  __syncwarp();
+  float* og = A.out + (size_t)g * GS;
+  for (int task = lane; task < K * D; task += 32) {
+    const int k = task / D, l = task % D;
+    const float* p = bC + k * DD + l * D;
+#pragma unroll
+    for (int r = 0; r < D; ++r) {
+      float acc = 0.f;
+#pragma unroll
+      for (int jj = 0; jj < D; ++jj) acc = fmaf(Ti[r + jj * D], p[jj], acc);
+      float v = acc > 0.f ? acc : 0.f;
+      if (A.clamp_one && v > 1.f) v = 1.f;
+      og[k * DD + r + l * D] = v;
+    }
+  }
+}
+
+bool wiener_supported(int d, int K) { return (d == 4 || d == 8 || d == 16) && (K == 8 || K == 16 || K == 32); }
+
+template <int D, int K>
+static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
+  const size_t sm = (size_t)(3 * D * D + 4 * 3 * D * D * K) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_wiener<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const int G = A.M * A.N;
+  k_wiener<D, K><<<(G + 3) / 4, 128, sm, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wiener(int d, const WienerArgs& A, cudaStream_t st) {
+#define GBM3D_WIE_CASE(DD, KK) \
+  if (d == DD && A.K == KK) return launch_wiener_t<DD, KK>(A, st);
+  GBM3D_WIE_CASE(8, 16) GBM3D_WIE_CASE(8, 8) GBM3D_WIE_CASE(8, 32)
+  GBM3D_WIE_CASE(4, 16) GBM3D_WIE_CASE(4, 8) GBM3D_WIE_CASE(4, 32)
+  GBM3D_WIE_CASE(16, 16) GBM3D_WIE_CASE(16, 8)
+#undef GBM3D_WIE_CASE
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace gbm3d

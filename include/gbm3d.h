@@ -1,0 +1,148 @@
+/*
+ * gbm3d.h — C ABI of the B200 (sm_100a) GBM3D two-step denoising library.
+ *
+ * Drop-in boundary for the MATLAB reference toby-sanders/GBM3D.  Each entry
+ * point below replaces one MATLAB function that source/GBM3D.m calls; a MEX
+ * gateway per function (gbm3d_b200/mex/) binds them under the reference's own
+ * names so GBM3D.m / GBM3D_distributed.m / setBM3Dopts.m run unchanged.
+ *
+ * Conventions
+ *   - Arrays are MATLAB column-major: element (r,c) of an m x n image is at
+ *     r + c*m.  Host pointers unless the name ends in _device.
+ *   - S (the match sets) is a uint32 array of K x M x N: S[k + K*(i + M*j)]
+ *     is entry k of cell S{i+1,j+1}, a 1-based column-major index into the
+ *     d2 x d2 search window (matchBlocksCPU.m:88,100-103).  S_count (M x N,
+ *     may be NULL) holds numel(S{i,j}) when numMin < numMax lets a cell hold
+ *     fewer than K matches; unused entries are 0.
+ *   - Every call returns GBM3D_OK or an error code; gbm3d_last_error() gives
+ *     the message.  The library never exits or aborts the process.
+ *   - A context is bound to one device and one stream and is not thread-safe;
+ *     use one context per host thread (MATLAB parfor workers are separate
+ *     processes, each with its own context).
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     call fails with GBM3D_ERR_CUDA.
+ */
+#ifndef GBM3D_H
+#define GBM3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GBM3D_OK 0
+#define GBM3D_ERR_ARG 1         /* invalid argument / unsupported size */
+#define GBM3D_ERR_CUDA 2        /* CUDA runtime error (or no device) */
+#define GBM3D_ERR_NOMEM 3       /* device allocation failed */
+#define GBM3D_ERR_NONFINITE 4   /* input holds NaN or Inf */
+#define GBM3D_ERR_UNSUPPORTED 5 /* option value the reference has but this library does not */
+
+typedef struct gbm3d_ctx gbm3d_ctx;
+
+/* Option struct with the reference's field names (utilities/setBM3Dopts.m:17-86,
+ * utilities/checkBM3Dopts.m:10-24).  filtType: 0 = 'ht', 1 = 'median'.
+ * refStride: reference-block spacing; 0 means blockSize (the reference's tiling).
+ * staleWeights: 1 mirrors GBM3D.m:26-27,82 (step 2 reuses the step-1 weight
+ * slices it does not overwrite). */
+typedef struct gbm3d_opts {
+  int numMax, numMin;
+  int blockSize, blockSizeWie, matchSize, refStride;
+  int levels, cycleSpin, tauMode;
+  int Wiener, filtType;
+  int nMatchSpins, matchSpins[8];
+  int nMatchSpinsWie, matchSpinsWie[8];
+  int staleWeights;
+} gbm3d_opts;
+
+/* Separable 3D wavelet bank: 1D analysis (a_) and synthesis (s_) filters for the
+ * two spatial axes (len_xy taps) and for the slot axis (len_z taps).  The
+ * reference's Psi/Psi2 (waveTransforms3D/getWaveFilters3Dbior.m:39-58) are the
+ * outer products of these factors. */
+typedef struct gbm3d_filters {
+  int len_xy;
+  double a_lo_xy[16], a_hi_xy[16], s_lo_xy[16], s_hi_xy[16];
+  int len_z;
+  double a_lo_z[16], a_hi_z[16], s_lo_z[16], s_hi_z[16];
+} gbm3d_filters;
+
+/* ---- context -------------------------------------------------------------- */
+int gbm3d_ctx_create(int device, gbm3d_ctx** out);
+void gbm3d_ctx_destroy(gbm3d_ctx* ctx);
+/* Run subsequent work on this cudaStream_t (NULL = the context's own stream). */
+int gbm3d_ctx_set_stream(gbm3d_ctx* ctx, void* cuda_stream);
+const char* gbm3d_last_error(const gbm3d_ctx* ctx);
+int gbm3d_version(void);
+
+/* ---- option helpers ----------------------------------------------------------
+ * gbm3d_default_opts   <- setBM3Dopts(profile)       utilities/setBM3Dopts.m:12-86
+ * gbm3d_get_tau        <- getTau(levels,mode)        utilities/getTau.m:9-51
+ * gbm3d_bior_filters   <- getWaveFilters3Dbior       waveTransforms3D/getWaveFilters3Dbior.m:12-58
+ */
+void gbm3d_default_opts(const char* profile, gbm3d_opts* out);
+void gbm3d_get_tau(int levels, int mode, double* tau /* levels x 7 */);
+void gbm3d_bior_filters(gbm3d_filters* out);
+
+/* ---- the reference's hot-path functions -------------------------------------- */
+
+/* [S,Volume] = matchBlocksCPU(I,sigma,opts)           source/matchBlocksCPU.m:1-116
+ * I: m x n double.  S: K x M x N, M=floor(m/d), N=floor(n/d).  S_count: M x N or
+ * NULL.  Volume: m x n x K single, or NULL to skip the gather. */
+int gbm3d_matchBlocksCPU(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
+                         const gbm3d_opts* opts, uint32_t* S, int32_t* S_count, float* Volume);
+
+/* [U,W] = denoiseAndAggregateGPU(Volume,S,tau,Psi,Psi2,opts)   source/denoiseAndAggregateGPU.m:1-92
+ * Volume: (M*d) x (N*d) x K single; S: K x M x N; S_count may be NULL;
+ * tau: levels x 7 double; filters: the separable factors of Psi/Psi2.
+ * U, W: (M*d) x (N*d) double. */
+int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* ctx, const float* Volume, const uint32_t* S,
+                                 const int32_t* S_count, int M, int N, const double* tau,
+                                 const gbm3d_filters* filters, const gbm3d_opts* opts,
+                                 double* U, double* W);
+
+/* [S,V1,V2] = matchBlocksWie(I,In,sigma,opts)            source/matchBlocksWie.m:1-92
+ * I (pilot) and In (noisy): m x n double.  V1, V2: d x d x K x M x N single
+ * (either may be NULL). */
+int gbm3d_matchBlocksWie(gbm3d_ctx* ctx, const double* I, const double* In, int m, int n,
+                         double sigma, const gbm3d_opts* opts, uint32_t* S, float* V1, float* V2);
+
+/* [U,W] = denoiseAndAggregateWieFast(V1,V2,S,sigma,opts)  source/denoiseAndAggregateWieFast.m:1-100
+ * sigma: one double, or d x d doubles when sigma_is_matrix (broadcast over slots). */
+int gbm3d_denoiseAndAggregateWieFast(gbm3d_ctx* ctx, const float* V1, const float* V2,
+                                     const uint32_t* S, int M, int N, const double* sigma,
+                                     int sigma_is_matrix, const gbm3d_opts* opts,
+                                     double* U, double* W);
+
+/* [U,W] = denoiseAndAggregateWie(V1,V2,S,sigma,opts)      source/denoiseAndAggregateWie.m:1-90
+ * Legacy variant: inverse DCT by the transpose and output clamped to [0,1]. */
+int gbm3d_denoiseAndAggregateWie(gbm3d_ctx* ctx, const float* V1, const float* V2,
+                                 const uint32_t* S, int M, int N, double sigma,
+                                 const gbm3d_opts* opts, double* U, double* W);
+
+/* [U,out] = GBM3D(I,sigma,opts)                            source/GBM3D.m:1-84
+ * Whole two-step pipeline on the device.  I, U: m x n double host arrays;
+ * U1 (out.U1, the step-1 estimate) may be NULL. */
+int gbm3d_denoise(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
+                  const gbm3d_opts* opts, double* U, double* U1);
+
+/* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
+ * the context stream (synchronise before reading U). */
+int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
+                         const gbm3d_opts* opts, double* U, double* U1);
+
+/* Per-stage device times (ms) of the last pipeline call, by CUDA events:
+ * [0] prepare, [1] step-1 matching, [2] step-1 wavelet, [3] step-1 aggregation,
+ * [4] step-2 matching, [5] step-2 Wiener, [6] step-2 aggregation, [7] total.
+ * Returns the number of entries written.  Timing is recorded only after
+ * gbm3d_ctx_enable_timing(ctx, 1). */
+int gbm3d_ctx_enable_timing(gbm3d_ctx* ctx, int on);
+int gbm3d_stage_times(const gbm3d_ctx* ctx, float* ms, int n);
+
+/* Number of kernels the last pipeline call launched. */
+int gbm3d_last_launch_count(const gbm3d_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GBM3D_H */

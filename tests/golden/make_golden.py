@@ -1,0 +1,73 @@
+"""Generate the golden vectors in tests/golden/*.npz.
+
+    python tests/golden/make_golden.py
+
+The vectors come from oracle/fft_route.py, the restatement that follows the
+MATLAB reference's FFT route operation by operation in float64 (the reference
+itself needs MATLAB, which cannot run here).  Inputs are seeded synthetic
+images (gbm3d_b200.synth), so every case is reproducible.  Each file holds the
+inputs and, per stage, the outputs of the reference function with that name.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from gbm3d_b200 import options, synth  # noqa: E402
+from oracle import fft_route as F  # noqa: E402
+
+
+def banks(fac):
+    Psi, Psi2 = options.bank_from_factors(fac)
+    # float64 banks built from the same factors (the FFT route runs in float64)
+    order = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 1)]
+    A = [(fac["a_lo_xy"], fac["a_hi_xy"]), (fac["a_lo_z"], fac["a_hi_z"])]
+    S = [(fac["s_lo_xy"], fac["s_hi_xy"]), (fac["s_lo_z"], fac["s_hi_z"])]
+    o3 = lambda a, b, c: a[:, None, None] * b[None, :, None] * c[None, None, :]  # noqa: E731
+    P = np.stack([o3(A[0][a], A[0][b], A[1][c]) for a, b, c in order], -1)
+    P2 = np.stack([o3(S[0][a], S[0][b], S[1][c]) for a, b, c in order], -1)
+    return P, P2
+
+
+CASES = [
+    # name, m, n, sigma, seed, profile, wavelet
+    ("default_64x96_s25", 64, 96, 25.0, 3, "default", "bior"),
+    ("default_70x90_s10", 70, 90, 10.0, 5, "default", "bior"),
+    ("fast_64x64_s50", 64, 64, 50.0, 7, "fast", "bior"),
+    ("haar_64x64_s25", 64, 64, 25.0, 11, "default", "haar"),
+]
+
+
+def make(name, m, n, sigma, seed, profile, wav):
+    clean, noisy = synth.noisy_image(m, n, sigma, seed=seed)
+    opts = options.resolve_opts({"profile": profile})
+    fac = options.bior_factors() if wav == "bior" else options.haar_factors()
+    P, P2 = banks(fac)
+    tau_unit = options.getTau(opts["levels"], opts["tauMode"])
+    d, dw, d2, K = opts["blockSize"], opts["blockSizeWie"], opts["matchSize"], opts["numMax"]
+    out = dict(clean=clean, noisy=noisy, sigma=sigma, profile=profile, wavelet=wav)
+    # stage tests on the unpadded image size multiple of d
+    Mp, Np = -(-m // d) * d, -(-n // d) * d
+    Ip = options.myMirrorPadImage(noisy, Mp, Np)
+    S1, Vol, _, _ = F.match_blocks(Ip, d, d2, K)
+    U1, W1 = F.denoise_ht(Vol, S1, sigma * tau_unit, P, P2, d, d2, opts["levels"], opts["cycleSpin"])
+    pilot = U1 / W1
+    S2, _, V1, V2 = F.match_blocks(pilot, dw, d2, K, In=Ip)
+    U2, W2 = F.denoise_wiener(V1, V2, S2, sigma, d2)
+    out.update(padded=Ip, S1=S1, U1=U1, W1=W1, pilot=pilot, S2=S2, U2=U2, W2=W2)
+    if wav == "bior":
+        U, Ustep1 = F.gbm3d(noisy, sigma, opts, P, P2, tau_unit)
+        out.update(U=U, Ustep1=Ustep1)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: getattr(v, "shape", v) for k, v in out.items() if k not in ("profile", "wavelet")})
+
+
+if __name__ == "__main__":
+    for c in CASES:
+        make(*c)

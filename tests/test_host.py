@@ -1,0 +1,144 @@
+"""Host logic and the C ABI surface (no GPU needed)."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from gbm3d_b200 import options
+
+
+def test_profiles_match_reference():
+    d = options.setBM3Dopts("default")
+    assert d["matchSpins"] == [0, 4] and d["matchSpinsWie"] == [0, 4]
+    assert (d["blockSize"], d["blockSizeWie"], d["matchSize"], d["numMax"]) == (16, 8, 32, 16)
+    f = options.setBM3Dopts("fast")
+    assert f["matchSpins"] == [0, 4, 6] and f["matchSpinsWie"] == [0]
+    s = options.setBM3Dopts("superFast")
+    assert s["blockSize"] == 32 and s["Wiener"] is False
+    a = options.setBM3Dopts("accuracy")
+    assert a["matchSpinsWie"] == [0, 4, 6]
+    assert options.setBM3Dopts("nonsense") == d
+
+
+def test_checkBM3Dopts_defaults():
+    o = options.checkBM3Dopts({"blockSize": 8})
+    assert o["matchSize"] == 32 and o["matchSpins"] == [0, 4] and o["cycleSpin"] == 2
+    o = options.checkBM3Dopts({"blockSize": 64})
+    assert o["matchSize"] == 64
+
+
+def test_profile_overrides_fields():
+    o = options.resolve_opts({"profile": "fast", "numMax": 4})
+    assert o["numMax"] == 16  # GBM3D.m:16-19 replaces every field
+
+
+def test_getTau_modes():
+    t = options.getTau(3, 1)
+    assert np.allclose(t[:, 0], [3.3, 3.0, 2.7]) and np.allclose(t, t[:, :1])
+    t2 = options.getTau(3, 2)
+    assert np.allclose(t2[0], [3.3, 3.3, 3.3, 3.8, 3.8, 3.8, 4.3])
+    t4 = options.getTau(2, 4)
+    assert np.allclose(t4[1], [2.9] * 3 + [3.4] * 3 + [3.9])
+
+
+def test_getTau_matches_oracle(oracle):
+    for mode in (1, 2, 3, 4):
+        assert np.array_equal(options.getTau(3, mode), oracle.get_tau(3, mode))
+
+
+def test_filter_bank_roundtrip():
+    Psi, Psi2 = options.getWaveFilters3Dbior()
+    assert Psi.shape == (10, 10, 2, 8) and Psi.dtype == np.float32
+    fac = options.factors_from_bank(Psi, Psi2)
+    ref = options.bior_factors()
+    for k in ref:
+        assert np.array_equal(fac[k], ref[k])
+    # a scaled (non-catalogued) separable bank is factorised numerically
+    P3, P4 = options.bank_from_factors({k: v * (1.5 if k.startswith("a_") else 1.0) for k, v in ref.items()})
+    f2 = options.factors_from_bank(P3, P4)
+    Q, Q2 = options.bank_from_factors(f2)
+    assert np.allclose(Q, P3, atol=1e-5) and np.allclose(Q2, P4, atol=1e-5)
+    with pytest.raises(ValueError):
+        bad = np.random.default_rng(0).normal(size=(10, 10, 2, 8)).astype(np.float32)
+        options.factors_from_bank(bad, bad)
+
+
+def test_mirror_pad():
+    I = np.arange(20.0).reshape(4, 5, order="F")
+    O = options.myMirrorPadImage(I, 6, 8)
+    assert np.array_equal(O[:4, :5], I)
+    assert np.array_equal(O[4:6, :5], np.flipud(I[2:4, :]))
+    assert np.array_equal(O[:4, 5:8], np.fliplr(I[:, 2:5]))
+
+
+def test_mirror_pad_matches_oracle(oracle):
+    rng = np.random.default_rng(0)
+    I = np.asfortranarray(rng.normal(size=(13, 11)))
+    O = np.zeros((16, 16), order="F")
+    oracle.lib().orc_mirror_pad(I.ctypes.data_as(C.c_void_p), 13, 11, O.ctypes.data_as(C.c_void_p), 16, 16)
+    assert np.array_equal(O, options.myMirrorPadImage(I, 16, 16))
+
+
+def test_psnr():
+    a = np.zeros((4, 4))
+    b = np.full((4, 4), 1.0)
+    assert abs(options.myPSNR(a, b, 255) - 20 * np.log10(255)) < 1e-12
+
+
+def test_dct_matrices_agree(oracle):
+    from oracle import fft_route
+    T, Ti = oracle.dct_matrices(8)
+    assert np.allclose(T, fft_route.dct_matrix(8), atol=1e-15)
+    assert np.allclose(Ti @ T, np.eye(8), atol=1e-14)
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    from gbm3d_b200 import _lib, build
+    path = build.build()
+    assert os.path.exists(path)
+    L = C.CDLL(path)
+    syms = _lib.header_symbols()
+    assert len(syms) >= 18
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    # every declared symbol has a ctypes signature in the binding
+    assert set(syms) <= set(_lib._SIGS)
+    # nm confirms the exports are plain C symbols
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    for s in syms:
+        assert f" T {s}\n" in out or out.endswith(f" T {s}"), s
+
+
+def test_library_option_helpers_match_host():
+    """Calls that need no device: profiles, tau table and filter factors."""
+    from gbm3d_b200 import _lib
+    L = _lib.lib()
+    for prof in ("default", "fast", "superFast", "accuracy"):
+        c = _lib.gbm3d_opts()
+        L.gbm3d_default_opts(prof.encode(), C.byref(c))
+        o = options.setBM3Dopts(prof)
+        assert (c.numMax, c.blockSize, c.blockSizeWie, c.matchSize, c.levels, c.cycleSpin) == \
+            (o["numMax"], o["blockSize"], o["blockSizeWie"], o["matchSize"], o["levels"], o["cycleSpin"])
+        assert list(c.matchSpins[:c.nMatchSpins]) == o["matchSpins"]
+        assert list(c.matchSpinsWie[:c.nMatchSpinsWie]) == o["matchSpinsWie"]
+        assert bool(c.Wiener) == o["Wiener"]
+    t = np.zeros((3, 7), order="F")
+    L.gbm3d_get_tau(3, 2, t.ctypes.data_as(C.c_void_p))
+    assert np.array_equal(t, options.getTau(3, 2))
+    f = _lib.gbm3d_filters()
+    L.gbm3d_bior_filters(C.byref(f))
+    ref = options.bior_factors()
+    assert np.array_equal(np.array(f.a_lo_xy[:10]), ref["a_lo_xy"])
+    assert np.array_equal(np.array(f.s_hi_xy[:10]), ref["s_hi_xy"])
+
+
+def test_no_device_fails_loudly():
+    """Without a usable CUDA device the library reports an error (no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from gbm3d_b200 import _lib
+    with pytest.raises(_lib.GBM3DError):
+        _lib.Context(0)

@@ -1,0 +1,154 @@
+"""The CPU oracle against the golden vectors and known-answer tests (no GPU).
+
+The golden vectors (tests/golden/*.npz, made by tests/golden/make_golden.py)
+come from the FFT-route restatement of the reference; the oracle computes the
+same functions by direct arithmetic.  Agreement to ~1e-9 relative in FP64 with
+identical match sets pins the two restatements to each other.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import max_abs
+from gbm3d_b200 import options, synth
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+FP64_TOL = 1e-9  # relative, FFT route vs direct arithmetic, both float64
+
+
+def _load(p):
+    z = np.load(p, allow_pickle=False)
+    return {k: z[k] for k in z.files}
+
+
+def _filters(O, wav):
+    return O.bior_filters() if wav == "bior" else O.haar_filters()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_oracle_matches_golden_stages(oracle, path):
+    g = _load(path)
+    O = oracle
+    opts = options.resolve_opts({"profile": str(g["profile"])})
+    sigma = float(g["sigma"])
+    f = _filters(O, str(g["wavelet"]))
+    S1, Vol, cnt = O.matchBlocksCPU(g["padded"], sigma, opts, prec=64)
+    assert np.array_equal(S1, g["S1"]), "step-1 match sets differ from the FFT route"
+    tau = sigma * options.getTau(opts["levels"], opts["tauMode"])
+    U1, W1 = O.denoiseAndAggregateGPU(Vol, S1, tau, opts, filters=f, prec=64)
+    assert max_abs(U1, g["U1"]) <= FP64_TOL * np.abs(g["U1"]).max()
+    assert max_abs(W1, g["W1"]) <= FP64_TOL * np.abs(g["W1"]).max()
+    S2, V1, V2 = O.matchBlocksWie(g["pilot"], g["padded"], sigma, opts, prec=64)
+    assert np.array_equal(S2, g["S2"]), "step-2 match sets differ from the FFT route"
+    U2, W2 = O.denoiseAndAggregateWieFast(V1, V2, S2, sigma, opts, prec=64)
+    assert max_abs(U2, g["U2"]) <= FP64_TOL * np.abs(g["U2"]).max()
+    assert max_abs(W2, g["W2"]) <= FP64_TOL * np.abs(g["W2"]).max()
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDEN if "haar" not in p],
+                         ids=[os.path.basename(p)[:-4] for p in GOLDEN if "haar" not in p])
+def test_oracle_matches_golden_pipeline(oracle, path):
+    g = _load(path)
+    opts = options.resolve_opts({"profile": str(g["profile"])})
+    U, U1 = oracle.GBM3D(g["noisy"], float(g["sigma"]), opts, prec=64)
+    assert max_abs(U1, g["Ustep1"]) <= 1e-9
+    assert max_abs(U, g["U"]) <= 1e-9
+    # FP32 GPU-order mode stays within the parity tolerance of the FP64 run here
+    U32, _ = oracle.GBM3D(g["noisy"], float(g["sigma"]), opts, prec=32)
+    assert max_abs(U32, g["U"]) < 1e-2
+
+
+@pytest.mark.parametrize("filters", ["bior", "haar"])
+@pytest.mark.parametrize("prec,tol", [(64, 1e-10), (32, 5e-4)])
+def test_wavelet_perfect_reconstruction(oracle, filters, prec, tol):
+    """analysis -> synthesis without threshold is the identity (filter-bank PR).
+
+    Holds while every level's input is at least as long as the filter; shorter
+    axes truncate the filter exactly as fftn(Psi, size) does in the reference.
+    """
+    rng = np.random.default_rng(0)
+    V = rng.uniform(0, 255, (80, 96, 16))
+    tau = -np.ones((3, 7))  # |c| > -1 keeps every coefficient
+    R = oracle.wavelet_ht(V, 3, tau, filters=_filters(oracle, filters), prec=prec)
+    assert max_abs(R, V) < tol
+
+
+def test_haar_slot_pairing(oracle):
+    """myWavDec1D pairs slots (L-1,0),(1,2),...: a spike at slot 0 mixes with slot L-1 only."""
+    V = np.zeros((16, 16, 16))
+    V[:, :, 0] = 1.0
+    V[:, :, 15] = 1.0  # pair (15, 0) is constant -> no level-1 z detail
+    O = oracle
+    f = O.bior_filters()
+    # threshold all details away except keep approximation: a constant pair survives exactly
+    tau = np.full((1, 7), 1e9)
+    R = O.wavelet_ht(V, 1, tau, filters=f, prec=64)
+    # the (15,0) pair is averaged as a pair: both slots stay equal
+    assert np.allclose(R[:, :, 0], R[:, :, 15])
+
+
+def test_padding_quirk_and_slot1(oracle):
+    """Rows 0..h-1 of the search image hold rows h..2h-1, and S(1) is the reference."""
+    O = oracle
+    opts = options.resolve_opts({"profile": "default"})
+    rng = np.random.default_rng(1)
+    I = rng.uniform(0, 255, (64, 64))
+    S, Vol, cnt = O.matchBlocksCPU(I, 25.0, opts, prec=64)
+    d2, d = opts["matchSize"], opts["blockSize"]
+    h = d2 // 2
+    assert np.all(S[0] == h * d2 + h + 1)
+    # slot 1 of the Volume is the reference block itself
+    assert np.array_equal(Vol[:, :, 0], I)
+    # a match at window offset (a, b) of ref (0, 0) reads Ipad rows a.., with the quirk
+    from oracle.fft_route import _search_pad
+    Ipad = _search_pad(I, d2)
+    for k in range(16):
+        e = int(S[k, 0, 0]) - 1
+        a, b = e % d2, e // d2
+        assert np.array_equal(Vol[:d, :d, k], Ipad[a:a + d, b:b + d])
+    assert np.array_equal(Ipad[:h, h:h + 64], I[h:2 * h, :])
+
+
+def test_tie_order_and_duplicate_reference(oracle):
+    """A flat image: every distance ties, mink keeps the lowest indices, S(1) forced."""
+    O = oracle
+    opts = options.resolve_opts({"profile": "default"})
+    I = np.full((64, 64), 100.0)
+    S, _, _ = O.matchBlocksCPU(I, 25.0, opts, prec=32)
+    d2 = opts["matchSize"]
+    want = np.arange(1, 17, dtype=np.uint32)
+    want[0] = d2 * d2 // 2 + d2 // 2 + 1
+    assert np.all(S == want[:, None, None])
+
+
+def test_scale_equivariance(oracle):
+    """GBM3D(2 I, 2 sigma) = 2 GBM3D(I, sigma): every step is scale-equivariant."""
+    _, noisy = synth.noisy_image(64, 64, 25.0, seed=2)
+    opts = options.resolve_opts({"profile": "default"})
+    U, _ = oracle.GBM3D(noisy, 25.0, opts, prec=64)
+    U2, _ = oracle.GBM3D(2 * noisy, 50.0, opts, prec=64)
+    assert max_abs(U2, 2 * U) < 1e-9
+
+
+def test_denoising_improves_psnr(oracle):
+    clean, noisy = synth.noisy_image(128, 128, 25.0, seed=4)
+    opts = options.resolve_opts({"profile": "default"})
+    U, U1 = oracle.GBM3D(noisy, 25.0, opts, prec=32)
+    p0 = options.myPSNR(clean, noisy, 255)
+    p1 = options.myPSNR(clean, U1, 255)
+    p2 = options.myPSNR(clean, U, 255)
+    assert p1 > p0 + 5 and p2 > p0 + 5
+
+
+def test_tolerance_branch(oracle):
+    """numMin < numMax: variable group sizes (matchBlocksCPU.m:89-99)."""
+    _, noisy = synth.noisy_image(64, 64, 10.0, seed=6)
+    opts = options.resolve_opts({"profile": "default"})
+    opts = dict(opts, numMin=4, numMax=16)
+    S, Vol, cnt = oracle.matchBlocksCPU(noisy, 10.0, opts, prec=32)
+    assert cnt.min() >= 4 and cnt.max() <= 16
+    for i in range(S.shape[1]):
+        for j in range(S.shape[2]):
+            assert np.all(S[cnt[i, j]:, i, j] == 0)
