@@ -37,6 +37,13 @@ WORKLOAD = ("GBM3D 'default' profile (blockSize 16 / blockSizeWie 8, matchSize 3
             "4096x4096 synthetic image, sigma 25, float64 in/out")
 
 
+def _set_size(size: int) -> None:
+    global SIZE, WORKLOAD
+    if size != SIZE:
+        WORKLOAD = WORKLOAD.replace(f"{SIZE}x{SIZE}", f"{size}x{size}")
+        SIZE = size
+
+
 def _config(extra=None):
     c = {"workload": WORKLOAD, "image": [SIZE, SIZE], "sigma": SIGMA, "profile": PROFILE,
          "parallelism": "replicas: one image per GPU",
@@ -154,7 +161,11 @@ def run_ours(args):
     from gbm3d_b200 import _lib, api, build, synth
     build.build()
     ctx = _lib.Context(local)
-    stream = torch.cuda.current_stream(dev)
+    # an explicit stream shared by the library and the timing events (torch's
+    # default stream is the legacy NULL stream, which the library's own
+    # non-blocking stream does not order against)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     _, noisy = synth.noisy_image(SIZE, SIZE, SIGMA, seed=100 + rank)
@@ -272,7 +283,9 @@ def main():
     ap.add_argument("--cpu-size", type=int, default=1024)
     ap.add_argument("--ref-size", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=SIZE, help="image side (profiling runs use smaller images)")
     args = ap.parse_args()
+    _set_size(args.size)
     if args.impl == "reference":
         run_reference(args)
     else:

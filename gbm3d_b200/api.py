@@ -55,7 +55,8 @@ def c_opts(opts: dict) -> gbm3d_opts:
     c = gbm3d_opts()
     c.numMax, c.numMin = int(o["numMax"]), int(o["numMin"])
     c.blockSize, c.blockSizeWie, c.matchSize = int(o["blockSize"]), int(o["blockSizeWie"]), int(o["matchSize"])
-    c.refStride = 0 if int(o["refStride"]) == int(o["blockSize"]) else int(o["refStride"])
+    rs = o.get("refStride")
+    c.refStride = 0 if rs is None or int(rs) == int(o["blockSize"]) else int(rs)
     c.levels, c.cycleSpin, c.tauMode = int(o["levels"]), int(o["cycleSpin"]), int(o["tauMode"])
     c.Wiener = 1 if o["Wiener"] else 0
     ft = o.get("filtType", "ht")

@@ -291,6 +291,23 @@ void check_match(gbm3d_ctx* c, int d, int d2, int K) {
 
 int pitch4(int rows) { return (rows + 3) & ~3; }
 
+// Match sets and counts that come from the caller are checked on the host
+// before any kernel indexes memory with them.
+void check_match_set(gbm3d_ctx* c, const uint32_t* S, const int32_t* cnt, size_t groups, int K, int d2) {
+  const uint32_t hi = (uint32_t)d2 * (uint32_t)d2;
+  for (size_t g = 0; g < groups; ++g) {
+    int nm = K;
+    if (cnt) {
+      nm = cnt[g];
+      if (nm < 1 || nm > K) argfail(c, "S_count entry out of range 1..numMax");
+    }
+    for (int k = 0; k < nm; ++k) {
+      const uint32_t v = S[g * K + k];
+      if (v < 1 || v > hi) argfail(c, "S holds an index outside the matchSize x matchSize window");
+    }
+  }
+}
+
 // ---- pipelines ----------------------------------------------------------------------
 
 // Block matching on a single-precision image already on the device.
@@ -742,6 +759,7 @@ int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* c, const float* Volume, const uint32
     const WaveletBank bk = make_bank(c, &fb);
     const int m = M * d, n = N * d;
     const size_t px = (size_t)m * n;
+    check_match_set(c, S, S_count, (size_t)M * N, K, d2);
     float* dV = buf<float>(c, "io.V", px * K);
     uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
     int32_t* dc = nullptr;
@@ -806,6 +824,7 @@ static int wiener_entry(gbm3d_ctx* c, const float* V1, const float* V2, const ui
     if (M < 1 || N < 1) argfail(c, "empty match set");
     if (d * d > 256) argfail(c, "blockSizeWie too large", GBM3D_ERR_UNSUPPORTED);
     const size_t gs = (size_t)d * d * K * M * N, px = (size_t)M * d * N * d;
+    check_match_set(c, S, nullptr, (size_t)M * N, K, d2);
     float* d1 = buf<float>(c, "io.V1", gs);
     float* d2p = buf<float>(c, "io.V2", gs);
     uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);

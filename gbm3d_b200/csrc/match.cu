@@ -171,7 +171,10 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
     const size_t mn = (size_t)A.m * A.n;
     for (int k = 0; k < K; ++k) {
       int aa = H, bb = H;
-      if (k < count) { const int e = (int)lS[k] - 1; aa = e % D2; bb = e / D2; }
+      if (k < count) {
+        const int e = (int)lS[k] - 1;
+        if ((unsigned)e < (unsigned)(D2 * D2)) { aa = e % D2; bb = e / D2; }
+      }
       for (int c = 0; c < D; ++c)
         for (int r = lane; r < D; r += 32)
           A.volume[(size_t)(i * D + r) + (size_t)A.m * (j * D + c) + mn * k] = win[(aa + r) + (bb + c) * WD];
@@ -180,7 +183,9 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
   if (A.V1 || A.V2) {
     const float* src2 = A.pad2 + (size_t)i * D + (size_t)j * D * A.P;
     for (int k = 0; k < K; ++k) {
-      const int e = (int)lS[k] - 1, aa = e % D2, bb = e / D2;
+      int e = (int)lS[k] - 1;
+      if ((unsigned)e >= (unsigned)(D2 * D2)) e = H + H * D2;
+      const int aa = e % D2, bb = e / D2;
       float* o1 = A.V1 ? A.V1 + (size_t)D * D * (k + (size_t)K * g) : nullptr;
       float* o2 = A.V2 ? A.V2 + (size_t)D * D * (k + (size_t)K * g) : nullptr;
       for (int t = lane; t < D * D; t += 32) {

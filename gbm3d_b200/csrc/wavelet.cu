@@ -224,6 +224,254 @@ __global__ void __launch_bounds__(128) k_ht_weights(const float* __restrict__ V,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fast path for the two banks GBM3D uses: bior1.5 x Haar (the reference's
+// getWaveFilters3Dbior) and 3D Haar.  Both have the shape
+//   analysis  lo: taps 0..LA-1      hi: taps HA0, HA0+1
+//   synthesis lo: taps SL0, SL0+1   hi: taps 0..SH-1
+//   slot axis: taps 0, 1 for all four filters
+// (bior: LA=SH=10, HA0=SL0=4; Haar: LA=SH=2, HA0=SL0=0).  With the tap
+// positions known at compile time every loop unrolls, even and odd outputs
+// are produced together (no divergent parity tests), shared memory rows that
+// a stride-2 filter reads are stored de-interleaved, and no division is left
+// in the inner loops.  Each output is the same serial fmaf chain, in the same
+// tap order, as the generic kernels and the oracle.
+// ---------------------------------------------------------------------------
+struct FastBank {
+  float alo[16], ahi[2], slo[2], shi[16];
+  float azl[2], azh[2], szl[2], szh[2];
+};
+
+__device__ __forceinline__ int wrap1(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
+
+template <int LA, int HA0>
+__global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restrict__ in, int Ly, int Lx, int Lz,
+                                                           int shift, float* __restrict__ out, FastBank fb,
+                                                           LevelBands th) {
+  constexpr int HALO = LA - 1;
+  constexpr int NY = 2 * TQ + HALO;  // staged rows/cols
+  constexpr int NYH = (NY + 1) / 2;  // de-interleaved half rows
+  extern __shared__ float sm[];
+  float* tz = sm;                    // [2 fz][NY x][NY y]
+  float* tx = sm + 2 * NY * NY;      // [4 comb][TQ qx][2 parity][NYH]
+  const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
+  const int qy0 = blockIdx.x * TQ, qx0 = blockIdx.y * TQ, qz = blockIdx.z;
+  const int y0 = 2 * qy0 - HALO - shift, x0 = 2 * qx0 - HALO - shift;
+  const size_t plane = (size_t)Ly * Lx;
+  const size_t zA = plane * pmod(2 * qz - shift, Lz), zB = plane * pmod(2 * qz - 1 - shift, Lz);
+
+  // stage 1: load the input tile of two slots and apply the slot-axis pass
+#pragma unroll 4
+  for (int e = threadIdx.x; e < NY * NY; e += 256) {
+    const int yy = e % NY, xx = e / NY;
+    const int gy = wrap1(y0 + yy, Ly), gx = wrap1(x0 + xx, Lx);
+    const float* col = in + gy + (size_t)Ly * gx;
+    const float u0 = __ldg(col + zA), u1 = __ldg(col + zB);  // taps k=0 (slot 2qz), k=1 (slot 2qz-1)
+    tz[e] = fmaf(fb.azl[1], u1, fmaf(fb.azl[0], u0, 0.f));
+    tz[NY * NY + e] = fmaf(fb.azh[1], u1, fmaf(fb.azh[0], u0, 0.f));
+  }
+  __syncthreads();
+  // stage 2: pass along the slow axis, lo and hi together from the same inputs
+  for (int e = threadIdx.x; e < 2 * TQ * NY; e += 256) {
+    const int yy = e % NY, r = e / NY, qx = r % TQ, fz = r / TQ;
+    const float* src = tz + fz * NY * NY + yy + (2 * qx + HALO) * NY;  // input x = 2qx - k
+    float v[LA];
+#pragma unroll
+    for (int k = 0; k < LA; ++k) v[k] = src[-k * NY];
+    float lo = 0.f, hi = 0.f;
+#pragma unroll
+    for (int k = 0; k < LA; ++k) lo = fmaf(fb.alo[k], v[k], lo);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[HA0 + k], hi);
+    float* dst = tx + (yy & 1) * NYH + (yy >> 1);
+    dst[((0 + 2 * fz) * TQ + qx) * 2 * NYH] = lo;
+    dst[((1 + 2 * fz) * TQ + qx) * 2 * NYH] = hi;
+  }
+  __syncthreads();
+  // stage 3: pass along the fast axis, threshold, store (lanes along qy)
+  const int qy = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const size_t bsz = (size_t)Oy * Ox * Oz;
+  const bool row_ok = qy0 + qy < Oy;
+  for (int j = w; j < 4 * TQ; j += 8) {
+    const int qx = j % TQ, comb = j / TQ;
+    if (!row_ok || qx0 + qx >= Ox) continue;
+    const float* src = tx + (comb * TQ + qx) * 2 * NYH;
+    float v[LA];
+#pragma unroll
+    for (int k = 0; k < LA; ++k) {
+      const int R = HALO - k;  // row 2qy + HALO - k
+      v[k] = src[(R & 1) * NYH + qy + (R >> 1)];
+    }
+    float lo = 0.f, hi = 0.f;
+#pragma unroll
+    for (int k = 0; k < LA; ++k) lo = fmaf(fb.alo[k], v[k], lo);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[HA0 + k], hi);
+    const int code_lo = 2 * comb, code_hi = 2 * comb + 1;
+    if (code_lo) lo = lo * (fabsf(lo) > th.tau[code_lo] ? 1.f : 0.f);
+    hi = hi * (fabsf(hi) > th.tau[code_hi] ? 1.f : 0.f);
+    const size_t o = (qy0 + qy) + (size_t)Oy * ((qx0 + qx) + (size_t)Ox * qz);
+    out[code_lo * bsz + o] = lo;
+    out[code_hi * bsz + o] = hi;
+  }
+}
+
+template <int SL0, int SH>
+__global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restrict__ bands,
+                                                            const float* __restrict__ approx, int Oy, int Ox,
+                                                            int Oz, SynthOut o, FastBank fb) {
+  constexpr int TS = 64;                             // output samples per axis
+  constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
+  constexpr int NQ = (TS - 1 + REACH) / 2 + 1;       // staged coefficients per axis
+  extern __shared__ float sm[];
+  float* B = sm;                  // [8 code][NQ qx][NQ qy]
+  float* Y = sm + 8 * NQ * NQ;    // [4 comb][NQ qx][TS py]
+  float* X = sm;                  // [2 fz][TS px][TS py]  (reuses B after the y-pass)
+  const int Iy = Oy >> 1, Ix = Ox >> 1, Iz = Oz >> 1;
+  const int py0 = blockIdx.x * TS, px0 = blockIdx.y * TS, qz = blockIdx.z;
+  const int qy0 = py0 >> 1, qx0 = px0 >> 1;
+  const size_t bsz = (size_t)Iy * Ix * Iz, zoff = (size_t)Iy * Ix * qz;
+
+  for (int e = threadIdx.x; e < 8 * NQ * NQ; e += 256) {
+    const int qyl = e % NQ, r = e / NQ, qxl = r % NQ, code = r / NQ;
+    const int qy = wrap1(qy0 + qyl, Iy), qx = wrap1(qx0 + qxl, Ix);
+    const float* src = code ? bands + code * bsz : approx;
+    B[e] = __ldg(src + zoff + qy + (size_t)Iy * qx);
+  }
+  __syncthreads();
+  // y-pass: rows py = 2t and 2t+1 from coefficients t + j
+  for (int e = threadIdx.x; e < 4 * NQ * (TS / 2); e += 256) {
+    const int t = e % (TS / 2), r = e / (TS / 2), qxl = r % NQ, comb = r / NQ;
+    const float* bl = B + ((0 + 2 * comb) * NQ + qxl) * NQ + t;
+    const float* bh = B + ((1 + 2 * comb) * NQ + qxl) * NQ + t;
+    float ev = 0.f, od = 0.f;
+    // even output 2t: taps k even, coefficient t + k/2; odd output 2t+1: k odd, t + (k+1)/2
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int k = SL0 + u;
+      if (k % 2 == 0) ev = fmaf(fb.slo[u], bl[k / 2], ev);
+      else od = fmaf(fb.slo[u], bl[(k + 1) / 2], od);
+    }
+#pragma unroll
+    for (int k = 0; k < SH; ++k) {
+      if (k % 2 == 0) ev = fmaf(fb.shi[k], bh[k / 2], ev);
+      else od = fmaf(fb.shi[k], bh[(k + 1) / 2], od);
+    }
+    float* dst = Y + (comb * NQ + qxl) * TS + 2 * t;
+    dst[0] = ev;
+    dst[1] = od;
+  }
+  __syncthreads();
+  // x-pass: columns px = 2t and 2t+1 (lanes along py)
+  const int py = threadIdx.x % TS, grp = threadIdx.x / TS;  // 4 groups
+  for (int j = grp; j < 2 * (TS / 2); j += 4) {
+    const int t = j % (TS / 2), fz = j / (TS / 2);
+    const float* yl = Y + ((0 + 2 * fz) * NQ + t) * TS + py;
+    const float* yh = Y + ((1 + 2 * fz) * NQ + t) * TS + py;
+    float ev = 0.f, od = 0.f;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int k = SL0 + u;
+      if (k % 2 == 0) ev = fmaf(fb.slo[u], yl[(k / 2) * TS], ev);
+      else od = fmaf(fb.slo[u], yl[((k + 1) / 2) * TS], od);
+    }
+#pragma unroll
+    for (int k = 0; k < SH; ++k) {
+      if (k % 2 == 0) ev = fmaf(fb.shi[k], yh[(k / 2) * TS], ev);
+      else od = fmaf(fb.shi[k], yh[((k + 1) / 2) * TS], od);
+    }
+    // X aliases B, which no thread reads after the barrier above
+    X[(fz * TS + 2 * t) * TS + py] = ev;
+    X[(fz * TS + 2 * t + 1) * TS + py] = od;
+  }
+  __syncthreads();
+  // slot-axis pass: slot 2qz from tap 0, slot 2qz-1 from tap 1; write or accumulate
+  const int oz0 = pmod(2 * qz - o.shift, Oz), oz1 = pmod(2 * qz - 1 - o.shift, Oz);
+  const int gy = py0 + py;
+  if (gy < Oy) {
+    const int oy = wrap1(gy - o.shift, Oy);
+    for (int px = grp; px < TS; px += 4) {
+      if (px0 + px >= Ox) break;
+      const float x0 = X[(0 * TS + px) * TS + py], x1 = X[(1 * TS + px) * TS + py];
+      const float v0 = fmaf(fb.szh[0], x1, fmaf(fb.szl[0], x0, 0.f));
+      const float v1 = fmaf(fb.szh[1], x1, fmaf(fb.szl[1], x0, 0.f));
+      const int ox = wrap1(px0 + px - o.shift, Ox);
+      float* d0 = o.out + oy + (size_t)Oy * (ox + (size_t)Ox * oz0);
+      float* d1 = o.out + oy + (size_t)Oy * (ox + (size_t)Ox * oz1);
+      float a0 = o.first ? v0 : *d0 + v0;
+      float a1 = o.first ? v1 : *d1 + v1;
+      if (o.last) {
+        a0 = a0 / o.cycles;
+        a0 = a0 > 0.f ? a0 : 0.f;
+        a1 = a1 / o.cycles;
+        a1 = a1 > 0.f ? a1 : 0.f;
+      }
+      *d0 = a0;
+      *d1 = a1;
+    }
+  }
+}
+
+// Which fast kernel (if any) a bank maps to: 1 = bior shape, 2 = Haar shape.
+static bool taps_are(const Taps& t, int first, int count) {
+  if (t.n != count) return false;
+  for (int u = 0; u < count; ++u)
+    if (t.k[u] != first + u) return false;
+  return true;
+}
+
+static int fast_kind(const WaveletBank& bk) {
+  for (int f = 0; f < 2; ++f)
+    if (!taps_are(bk.z.a[f], 0, 2) || !taps_are(bk.z.s[f], 0, 2)) return 0;
+  if (taps_are(bk.xy.a[0], 0, 10) && taps_are(bk.xy.a[1], 4, 2) && taps_are(bk.xy.s[0], 4, 2) &&
+      taps_are(bk.xy.s[1], 0, 10))
+    return 1;
+  if (taps_are(bk.xy.a[0], 0, 2) && taps_are(bk.xy.a[1], 0, 2) && taps_are(bk.xy.s[0], 0, 2) &&
+      taps_are(bk.xy.s[1], 0, 2))
+    return 2;
+  return 0;
+}
+
+static FastBank fast_bank(const WaveletBank& bk) {
+  FastBank f{};
+  for (int u = 0; u < bk.xy.a[0].n; ++u) f.alo[u] = bk.xy.a[0].h[u];
+  for (int u = 0; u < 2; ++u) {
+    f.ahi[u] = bk.xy.a[1].h[u];
+    f.slo[u] = bk.xy.s[0].h[u];
+    f.azl[u] = bk.z.a[0].h[u];
+    f.azh[u] = bk.z.a[1].h[u];
+    f.szl[u] = bk.z.s[0].h[u];
+    f.szh[u] = bk.z.s[1].h[u];
+  }
+  for (int u = 0; u < bk.xy.s[1].n; ++u) f.shi[u] = bk.xy.s[1].h[u];
+  return f;
+}
+
+template <int LA, int HA0>
+static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
+                                        const FastBank& fb, const LevelBands& th, cudaStream_t st) {
+  constexpr int NY = 2 * TQ + LA - 1, NYH = (NY + 1) / 2;
+  const size_t sm = (size_t)(2 * NY * NY + 4 * TQ * 2 * NYH) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_fast<LA, HA0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid((Ly / 2 + TQ - 1) / TQ, (Lx / 2 + TQ - 1) / TQ, Lz / 2);
+  k_wav_analysis_fast<LA, HA0><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, fb, th);
+  return cudaGetLastError();
+}
+
+template <int SL0, int SH>
+static cudaError_t launch_synthesis_fast(const float* bands, const float* approx, int Oy, int Ox, int Oz,
+                                         const SynthOut& o, const FastBank& fb, cudaStream_t st) {
+  constexpr int TS = 64, REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1, NQ = (TS - 1 + REACH) / 2 + 1;
+  const size_t a = (size_t)8 * NQ * NQ, x = (size_t)2 * TS * TS;
+  const size_t sm = ((a > x ? a : x) + (size_t)4 * NQ * TS) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_fast<SL0, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid((Oy + TS - 1) / TS, (Ox + TS - 1) / TS, Oz / 2);
+  k_wav_synthesis_fast<SL0, SH><<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, fb);
+  return cudaGetLastError();
+}
+
 static size_t analysis_smem(int reach) {
   const int NY = 2 * TQ + reach;
   return (size_t)(2 * NY * NY + 4 * TQ * NY) * sizeof(float);
@@ -236,6 +484,13 @@ static size_t synthesis_smem(int reach) {
 
 cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
                                 const WaveletBank& bk, const LevelBands& th, cudaStream_t st) {
+  const int kind = fast_kind(bk);
+  // the fast kernel wraps each halo coordinate at most once
+  if (kind && Ly > 2 * TQ + 16 && Lx > 2 * TQ + 16 && Lz >= 2) {
+    const FastBank fb = fast_bank(bk);
+    if (kind == 1) return launch_analysis_fast<10, 4>(in, Ly, Lx, Lz, shift, out, fb, th, st);
+    return launch_analysis_fast<2, 0>(in, Ly, Lx, Lz, shift, out, fb, th, st);
+  }
   const size_t sm = analysis_smem(bk.reach_a);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
@@ -246,6 +501,13 @@ cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shi
 
 cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy, int Ox, int Oz,
                                  const SynthOut& o, const WaveletBank& bk, cudaStream_t st) {
+  const int kind = fast_kind(bk);
+  // coefficient tiles of 37 per axis must wrap at most once; shifts below the size
+  if (kind && Oy >= 128 && Ox >= 128 && Oz >= 2 && o.shift >= 0 && o.shift < Oy && o.shift < Ox) {
+    const FastBank fb = fast_bank(bk);
+    if (kind == 1) return launch_synthesis_fast<4, 10>(bands, approx, Oy, Ox, Oz, o, fb, st);
+    return launch_synthesis_fast<0, 2>(bands, approx, Oy, Ox, Oz, o, fb, st);
+  }
   const size_t sm = synthesis_smem(bk.reach_s);
   cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;

@@ -99,7 +99,9 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   if (A.padP) {
     const int i = g % A.M, j = g / A.M;
     for (int k = 0; k < K; ++k) {
-      const int e = (int)A.S[(size_t)g * K + k] - 1, a = e % A.d2, b = e / A.d2;
+      int e = (int)A.S[(size_t)g * K + k] - 1;
+      if ((unsigned)e >= (unsigned)(A.d2 * A.d2)) e = (A.d2 / 2) * (A.d2 + 1);  // never read outside the window
+      const int a = e % A.d2, b = e / A.d2;
       const size_t o = (size_t)(i * D + a) + (size_t)(j * D + b) * A.P;
       for (int t = lane; t < DD; t += 32) {
         const int r = t % D, c = t / D;

@@ -10,9 +10,10 @@ Host-side mirror of the reference's utility layer (toby-sanders/GBM3D):
   myPSNR                 utilities/myPSNR.m:7-12
 
 Options are plain dicts with the reference's field names.  Two fields exist
-only here: ``refStride`` (reference-block stride, defaults to the block size,
-which is the reference's tiling) and ``staleWeights`` (mirror GBM3D.m's reuse
-of step-1 weight slices when step 2 has fewer spins; default True).
+only here: ``refStride`` (reference-block stride; absent or None means the
+block size, which is the reference's tiling) and ``staleWeights`` (mirror
+GBM3D.m's reuse of step-1 weight slices when step 2 has fewer spins; default
+True).
 """
 from __future__ import annotations
 
@@ -59,7 +60,6 @@ def checkBM3Dopts(opts: dict | None) -> dict:
     o.setdefault("Wiener", True)
     # present in every profile; checkBM3Dopts does not default it
     o.setdefault("matchSpinsWie", list(o["matchSpins"]))
-    o.setdefault("refStride", o["blockSize"])
     o.setdefault("staleWeights", True)
     return o
 
