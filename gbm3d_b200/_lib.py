@@ -15,7 +15,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "gbm3d.h")
 
 GBM3D_OK = 0
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
-          4: "non-finite input", 5: "unsupported option"}
+          4: "non-finite input", 5: "unsupported option", 6: "image too large for the fixed scratch"}
 
 
 class GBM3DError(RuntimeError):
@@ -70,6 +70,7 @@ _SIGS = {
     "gbm3d_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "gbm3d_stage_times": (C.c_int, [_P, _P, C.c_int]),
     "gbm3d_last_launch_count": (C.c_int, [_P]),
+    "gbm3d_matchBlocks_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P, _P]),
 }
 
 _lib = None

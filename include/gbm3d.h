@@ -38,6 +38,11 @@ extern "C" {
 #define GBM3D_ERR_NOMEM 3       /* device allocation failed */
 #define GBM3D_ERR_NONFINITE 4   /* input holds NaN or Inf */
 #define GBM3D_ERR_UNSUPPORTED 5 /* option value the reference has but this library does not */
+#define GBM3D_ERR_TOO_LARGE 6   /* image exceeds the fixed scratch of gbm3d_matchBlocks_noalloc */
+
+/* Size of the fixed device scratch of gbm3d_matchBlocks_noalloc, in floats
+ * (16 MiB, held by every GPU that loads the library until the process exits). */
+#define GBM3D_NOALLOC_MAX_FLOATS (4u << 20)
 
 typedef struct gbm3d_ctx gbm3d_ctx;
 
@@ -141,6 +146,27 @@ int gbm3d_stage_times(const gbm3d_ctx* ctx, float* ms, int n);
 
 /* Number of kernels the last pipeline call launched. */
 int gbm3d_last_launch_count(const gbm3d_ctx* ctx);
+
+/* Step-1 block matching that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that may not allocate device memory while
+ * they run (servers and video pipelines that reserve all GPU memory at
+ * start-up so no call can run out of memory or stall in the device-wide
+ * synchronisation of cudaFree, and host applications whose own allocator owns
+ * every device buffer).  Same search and selection as gbm3d_matchBlocksCPU.
+ *   I: single-precision m x n image on the device (the single(I) of
+ *      matchBlocksCPU.m:31); S: K x M x N uint32 and S_count: M x N int32
+ *      (may be NULL) on the device; stream: a cudaStream_t (NULL = default).
+ * The work is queued on the stream and not waited for.  Scratch is a fixed
+ * device array of GBM3D_NOALLOC_MAX_FLOATS floats shared by all calls: an
+ * image whose search image needs more, ((m+matchSize+3)/4*4) * (n+matchSize)
+ * floats (about 2000 x 2000 pixels at matchSize 32), returns
+ * GBM3D_ERR_TOO_LARGE before any work, and calls that overlap on the GPU (other streams or
+ * host threads) race on it.  The first call on each device looks the
+ * scratch's address up with cudaGetSymbolAddress; make that first call
+ * before any stream capture.  No context, no gbm3d_last_error: the return
+ * code is the whole report. */
+int gbm3d_matchBlocks_noalloc(const float* I, int m, int n, double sigma, const gbm3d_opts* opts,
+                              uint32_t* S, int32_t* S_count, void* stream);
 
 #ifdef __cplusplus
 }
