@@ -244,37 +244,40 @@ struct FastBank {
 
 __device__ __forceinline__ int wrap1(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
+constexpr int FQY = 32, FQX = 16;  // fast analysis tile: coefficients along y (fast axis) and x
+
 template <int LA, int HA0>
 __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restrict__ in, int Ly, int Lx, int Lz,
                                                            int shift, float* __restrict__ out, FastBank fb,
                                                            LevelBands th) {
   constexpr int HALO = LA - 1;
-  constexpr int NY = 2 * TQ + HALO;  // staged rows/cols
-  constexpr int NYH = (NY + 1) / 2;  // de-interleaved half rows
+  constexpr int NY = 2 * FQY + HALO;  // staged rows
+  constexpr int NX = 2 * FQX + HALO;  // staged columns
+  constexpr int NYH = (NY + 1) / 2;   // de-interleaved half rows
   extern __shared__ float sm[];
-  float* tz = sm;                    // [2 fz][NY x][NY y]
-  float* tx = sm + 2 * NY * NY;      // [4 comb][TQ qx][2 parity][NYH]
+  float* tz = sm;                     // [2 fz][NX x][NY y]
+  float* tx = sm + 2 * NX * NY;       // [4 comb][FQX qx][2 parity][NYH]
   const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
-  const int qy0 = blockIdx.x * TQ, qx0 = blockIdx.y * TQ, qz = blockIdx.z;
+  const int qy0 = blockIdx.x * FQY, qx0 = blockIdx.y * FQX, qz = blockIdx.z;
   const int y0 = 2 * qy0 - HALO - shift, x0 = 2 * qx0 - HALO - shift;
   const size_t plane = (size_t)Ly * Lx;
   const size_t zA = plane * pmod(2 * qz - shift, Lz), zB = plane * pmod(2 * qz - 1 - shift, Lz);
 
   // stage 1: load the input tile of two slots and apply the slot-axis pass
 #pragma unroll 4
-  for (int e = threadIdx.x; e < NY * NY; e += 256) {
+  for (int e = threadIdx.x; e < NX * NY; e += 256) {
     const int yy = e % NY, xx = e / NY;
     const int gy = wrap1(y0 + yy, Ly), gx = wrap1(x0 + xx, Lx);
     const float* col = in + gy + (size_t)Ly * gx;
     const float u0 = __ldg(col + zA), u1 = __ldg(col + zB);  // taps k=0 (slot 2qz), k=1 (slot 2qz-1)
     tz[e] = fmaf(fb.azl[1], u1, fmaf(fb.azl[0], u0, 0.f));
-    tz[NY * NY + e] = fmaf(fb.azh[1], u1, fmaf(fb.azh[0], u0, 0.f));
+    tz[NX * NY + e] = fmaf(fb.azh[1], u1, fmaf(fb.azh[0], u0, 0.f));
   }
   __syncthreads();
   // stage 2: pass along the slow axis, lo and hi together from the same inputs
-  for (int e = threadIdx.x; e < 2 * TQ * NY; e += 256) {
-    const int yy = e % NY, r = e / NY, qx = r % TQ, fz = r / TQ;
-    const float* src = tz + fz * NY * NY + yy + (2 * qx + HALO) * NY;  // input x = 2qx - k
+  for (int e = threadIdx.x; e < 2 * FQX * NY; e += 256) {
+    const int yy = e % NY, r = e / NY, qx = r % FQX, fz = r / FQX;
+    const float* src = tz + fz * NX * NY + yy + (2 * qx + HALO) * NY;  // input x = 2qx - k
     float v[LA];
 #pragma unroll
     for (int k = 0; k < LA; ++k) v[k] = src[-k * NY];
@@ -284,18 +287,18 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
 #pragma unroll
     for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[HA0 + k], hi);
     float* dst = tx + (yy & 1) * NYH + (yy >> 1);
-    dst[((0 + 2 * fz) * TQ + qx) * 2 * NYH] = lo;
-    dst[((1 + 2 * fz) * TQ + qx) * 2 * NYH] = hi;
+    dst[((0 + 2 * fz) * FQX + qx) * 2 * NYH] = lo;
+    dst[((1 + 2 * fz) * FQX + qx) * 2 * NYH] = hi;
   }
   __syncthreads();
   // stage 3: pass along the fast axis, threshold, store (lanes along qy)
   const int qy = threadIdx.x & 31, w = threadIdx.x >> 5;
   const size_t bsz = (size_t)Oy * Ox * Oz;
   const bool row_ok = qy0 + qy < Oy;
-  for (int j = w; j < 4 * TQ; j += 8) {
-    const int qx = j % TQ, comb = j / TQ;
+  for (int j = w; j < 4 * FQX; j += 8) {
+    const int qx = j % FQX, comb = j / FQX;
     if (!row_ok || qx0 + qx >= Ox) continue;
-    const float* src = tx + (comb * TQ + qx) * 2 * NYH;
+    const float* src = tx + (comb * FQX + qx) * 2 * NYH;
     float v[LA];
 #pragma unroll
     for (int k = 0; k < LA; ++k) {
@@ -316,34 +319,36 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
   }
 }
 
+constexpr int FSY = 64, FSX = 32;  // fast synthesis tile: samples along y and x
+
 template <int SL0, int SH>
 __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restrict__ bands,
                                                             const float* __restrict__ approx, int Oy, int Ox,
                                                             int Oz, SynthOut o, FastBank fb) {
-  constexpr int TS = 64;                             // output samples per axis
   constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
-  constexpr int NQ = (TS - 1 + REACH) / 2 + 1;       // staged coefficients per axis
+  constexpr int NQY = (FSY - 1 + REACH) / 2 + 1;  // staged coefficients along y
+  constexpr int NQX = (FSX - 1 + REACH) / 2 + 1;  // and along x
   extern __shared__ float sm[];
-  float* B = sm;                  // [8 code][NQ qx][NQ qy]
-  float* Y = sm + 8 * NQ * NQ;    // [4 comb][NQ qx][TS py]
-  float* X = sm;                  // [2 fz][TS px][TS py]  (reuses B after the y-pass)
+  float* B = sm;                    // [8 code][NQX qx][NQY qy]
+  float* Y = sm + 8 * NQX * NQY;    // [4 comb][NQX qx][FSY py]
+  float* X = sm;                    // [2 fz][FSX px][FSY py]  (reuses B after the y-pass)
   const int Iy = Oy >> 1, Ix = Ox >> 1, Iz = Oz >> 1;
-  const int py0 = blockIdx.x * TS, px0 = blockIdx.y * TS, qz = blockIdx.z;
+  const int py0 = blockIdx.x * FSY, px0 = blockIdx.y * FSX, qz = blockIdx.z;
   const int qy0 = py0 >> 1, qx0 = px0 >> 1;
   const size_t bsz = (size_t)Iy * Ix * Iz, zoff = (size_t)Iy * Ix * qz;
 
-  for (int e = threadIdx.x; e < 8 * NQ * NQ; e += 256) {
-    const int qyl = e % NQ, r = e / NQ, qxl = r % NQ, code = r / NQ;
+  for (int e = threadIdx.x; e < 8 * NQX * NQY; e += 256) {
+    const int qyl = e % NQY, r = e / NQY, qxl = r % NQX, code = r / NQX;
     const int qy = wrap1(qy0 + qyl, Iy), qx = wrap1(qx0 + qxl, Ix);
     const float* src = code ? bands + code * bsz : approx;
     B[e] = __ldg(src + zoff + qy + (size_t)Iy * qx);
   }
   __syncthreads();
   // y-pass: rows py = 2t and 2t+1 from coefficients t + j
-  for (int e = threadIdx.x; e < 4 * NQ * (TS / 2); e += 256) {
-    const int t = e % (TS / 2), r = e / (TS / 2), qxl = r % NQ, comb = r / NQ;
-    const float* bl = B + ((0 + 2 * comb) * NQ + qxl) * NQ + t;
-    const float* bh = B + ((1 + 2 * comb) * NQ + qxl) * NQ + t;
+  for (int e = threadIdx.x; e < 4 * NQX * (FSY / 2); e += 256) {
+    const int t = e % (FSY / 2), r = e / (FSY / 2), qxl = r % NQX, comb = r / NQX;
+    const float* bl = B + ((0 + 2 * comb) * NQX + qxl) * NQY + t;
+    const float* bh = B + ((1 + 2 * comb) * NQX + qxl) * NQY + t;
     float ev = 0.f, od = 0.f;
     // even output 2t: taps k even, coefficient t + k/2; odd output 2t+1: k odd, t + (k+1)/2
 #pragma unroll
@@ -357,32 +362,32 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restr
       if (k % 2 == 0) ev = fmaf(fb.shi[k], bh[k / 2], ev);
       else od = fmaf(fb.shi[k], bh[(k + 1) / 2], od);
     }
-    float* dst = Y + (comb * NQ + qxl) * TS + 2 * t;
+    float* dst = Y + (comb * NQX + qxl) * FSY + 2 * t;
     dst[0] = ev;
     dst[1] = od;
   }
   __syncthreads();
   // x-pass: columns px = 2t and 2t+1 (lanes along py)
-  const int py = threadIdx.x % TS, grp = threadIdx.x / TS;  // 4 groups
-  for (int j = grp; j < 2 * (TS / 2); j += 4) {
-    const int t = j % (TS / 2), fz = j / (TS / 2);
-    const float* yl = Y + ((0 + 2 * fz) * NQ + t) * TS + py;
-    const float* yh = Y + ((1 + 2 * fz) * NQ + t) * TS + py;
+  const int py = threadIdx.x % FSY, grp = threadIdx.x / FSY;  // 4 groups
+  for (int j = grp; j < 2 * (FSX / 2); j += 4) {
+    const int t = j % (FSX / 2), fz = j / (FSX / 2);
+    const float* yl = Y + ((0 + 2 * fz) * NQX + t) * FSY + py;
+    const float* yh = Y + ((1 + 2 * fz) * NQX + t) * FSY + py;
     float ev = 0.f, od = 0.f;
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
       const int k = SL0 + u;
-      if (k % 2 == 0) ev = fmaf(fb.slo[u], yl[(k / 2) * TS], ev);
-      else od = fmaf(fb.slo[u], yl[((k + 1) / 2) * TS], od);
+      if (k % 2 == 0) ev = fmaf(fb.slo[u], yl[(k / 2) * FSY], ev);
+      else od = fmaf(fb.slo[u], yl[((k + 1) / 2) * FSY], od);
     }
 #pragma unroll
     for (int k = 0; k < SH; ++k) {
-      if (k % 2 == 0) ev = fmaf(fb.shi[k], yh[(k / 2) * TS], ev);
-      else od = fmaf(fb.shi[k], yh[((k + 1) / 2) * TS], od);
+      if (k % 2 == 0) ev = fmaf(fb.shi[k], yh[(k / 2) * FSY], ev);
+      else od = fmaf(fb.shi[k], yh[((k + 1) / 2) * FSY], od);
     }
     // X aliases B, which no thread reads after the barrier above
-    X[(fz * TS + 2 * t) * TS + py] = ev;
-    X[(fz * TS + 2 * t + 1) * TS + py] = od;
+    X[(fz * FSX + 2 * t) * FSY + py] = ev;
+    X[(fz * FSX + 2 * t + 1) * FSY + py] = od;
   }
   __syncthreads();
   // slot-axis pass: slot 2qz from tap 0, slot 2qz-1 from tap 1; write or accumulate
@@ -390,9 +395,9 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restr
   const int gy = py0 + py;
   if (gy < Oy) {
     const int oy = wrap1(gy - o.shift, Oy);
-    for (int px = grp; px < TS; px += 4) {
+    for (int px = grp; px < FSX; px += 4) {
       if (px0 + px >= Ox) break;
-      const float x0 = X[(0 * TS + px) * TS + py], x1 = X[(1 * TS + px) * TS + py];
+      const float x0 = X[(0 * FSX + px) * FSY + py], x1 = X[(1 * FSX + px) * FSY + py];
       const float v0 = fmaf(fb.szh[0], x1, fmaf(fb.szl[0], x0, 0.f));
       const float v1 = fmaf(fb.szh[1], x1, fmaf(fb.szl[1], x0, 0.f));
       const int ox = wrap1(px0 + px - o.shift, Ox);
@@ -450,11 +455,11 @@ static FastBank fast_bank(const WaveletBank& bk) {
 template <int LA, int HA0>
 static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
                                         const FastBank& fb, const LevelBands& th, cudaStream_t st) {
-  constexpr int NY = 2 * TQ + LA - 1, NYH = (NY + 1) / 2;
-  const size_t sm = (size_t)(2 * NY * NY + 4 * TQ * 2 * NYH) * sizeof(float);
+  constexpr int NY = 2 * FQY + LA - 1, NX = 2 * FQX + LA - 1, NYH = (NY + 1) / 2;
+  const size_t sm = (size_t)(2 * NX * NY + 4 * FQX * 2 * NYH) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_fast<LA, HA0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((Ly / 2 + TQ - 1) / TQ, (Lx / 2 + TQ - 1) / TQ, Lz / 2);
+  dim3 grid((Ly / 2 + FQY - 1) / FQY, (Lx / 2 + FQX - 1) / FQX, Lz / 2);
   k_wav_analysis_fast<LA, HA0><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, fb, th);
   return cudaGetLastError();
 }
@@ -462,14 +467,59 @@ static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz,
 template <int SL0, int SH>
 static cudaError_t launch_synthesis_fast(const float* bands, const float* approx, int Oy, int Ox, int Oz,
                                          const SynthOut& o, const FastBank& fb, cudaStream_t st) {
-  constexpr int TS = 64, REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1, NQ = (TS - 1 + REACH) / 2 + 1;
-  const size_t a = (size_t)8 * NQ * NQ, x = (size_t)2 * TS * TS;
-  const size_t sm = ((a > x ? a : x) + (size_t)4 * NQ * TS) * sizeof(float);
+  constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
+  constexpr int NQY = (FSY - 1 + REACH) / 2 + 1, NQX = (FSX - 1 + REACH) / 2 + 1;
+  const size_t a = (size_t)8 * NQX * NQY, x = (size_t)2 * FSX * FSY;
+  const size_t sm = ((a > x ? a : x) + (size_t)4 * NQX * FSY) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_fast<SL0, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((Oy + TS - 1) / TS, (Ox + TS - 1) / TS, Oz / 2);
+  dim3 grid((Oy + FSY - 1) / FSY, (Ox + FSX - 1) / FSX, Oz / 2);
   k_wav_synthesis_fast<SL0, SH><<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, fb);
   return cudaGetLastError();
+}
+
+// Compile-time block size version of k_ht_weights: the index decompositions
+// become multiplications by constants, and each lane walks its elements
+// (e = lane + 32 t of each difference array, in increasing e) exactly as the
+// generic kernel and the oracle do.
+template <int D>
+__global__ void __launch_bounds__(128) k_ht_weights_t(const float* __restrict__ V, int m, int n, int M, int N,
+                                                      int K, const int32_t* __restrict__ cnt,
+                                                      float* __restrict__ wgt) {
+  constexpr int DM = D - 3;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * 4 + warp;
+  if (g >= M * N) return;
+  const int i = g % M, j = g / M;
+  const int nm = cnt ? cnt[g] : K;
+  const size_t sz = (size_t)m * n;
+  const float* base = V + (size_t)i * D + (size_t)j * D * m;
+  float tx = 0.f, ty = 0.f, tz = 0.f;
+  const int nx = D * DM * nm;
+  for (int e = lane; e < nx; e += 32) {
+    const int r = e % D, q = e / D, c = q % DM, k = q / DM;
+    const float* p = base + r + (size_t)c * m + sz * k;
+    tx = tx + fabsf(d3(__ldg(p), __ldg(p + m), __ldg(p + 2 * m), __ldg(p + 3 * m)));
+  }
+  for (int e = lane; e < nx; e += 32) {
+    const int r = e % DM, q = e / DM, c = q % D, k = q / D;
+    const float* p = base + r + (size_t)c * m + sz * k;
+    ty = ty + fabsf(d3(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)));
+  }
+  const int nzz = D * D * (nm - 1);
+  for (int e = lane; e < nzz; e += 32) {
+    const int r = e % D, q = e / D, c = q % D, k = q / D;
+    const float* p = base + r + (size_t)c * m + sz * k;
+    tz = tz + fabsf(__ldg(p + sz) - __ldg(p));
+  }
+  tx = warp_sum(tx);
+  ty = warp_sum(ty);
+  tz = warp_sum(tz);
+  if (lane == 0) {
+    float w = tx * 0.25f + ty * 0.25f;
+    w = w + tz;
+    wgt[g] = 1.f / (w + 2.220446049250313e-16f);
+  }
 }
 
 static size_t analysis_smem(int reach) {
@@ -519,6 +569,18 @@ cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy
 cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int d, int K,
                               const int32_t* cnt, float* wgt, cudaStream_t st) {
   const int G = M * N;
+  if (d == 16) {
+    k_ht_weights_t<16><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    return cudaGetLastError();
+  }
+  if (d == 8) {
+    k_ht_weights_t<8><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    return cudaGetLastError();
+  }
+  if (d == 32) {
+    k_ht_weights_t<32><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    return cudaGetLastError();
+  }
   k_ht_weights<<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, d, K, cnt, wgt);
   return cudaGetLastError();
 }

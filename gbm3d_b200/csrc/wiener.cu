@@ -77,14 +77,15 @@ __device__ __forceinline__ void haar_rec(float* v, float cc) {
 template <int D, int K>
 __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   constexpr int DD = D * D, GS = DD * K;
+  constexpr int DDP = DD + 1, GSP = DDP * K;  // slot pages padded by one word: no bank conflicts
   extern __shared__ float sm[];
   float* Tm = sm;
   float* Ti = sm + DD;
   float* s2 = sm + 2 * DD;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* bA = sm + 3 * DD + warp * 3 * GS;
-  float* bB = bA + GS;
-  float* bC = bB + GS;
+  float* bA = sm + 3 * DD + warp * 3 * GSP;
+  float* bB = bA + GSP;
+  float* bC = bB + GSP;
   for (int t = threadIdx.x; t < DD; t += blockDim.x) {
     Tm[t] = A.T[t];
     Ti[t] = A.Ti[t];
@@ -105,16 +106,16 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       const size_t o = (size_t)(i * D + a) + (size_t)(j * D + b) * A.P;
       for (int t = lane; t < DD; t += 32) {
         const int r = t % D, c = t / D;
-        bA[k * DD + t] = A.padP[o + r + (size_t)c * A.P];
-        bB[k * DD + t] = A.padN[o + r + (size_t)c * A.P];
+        bA[k * DDP + t] = A.padP[o + r + (size_t)c * A.P];
+        bB[k * DDP + t] = A.padN[o + r + (size_t)c * A.P];
       }
     }
   } else {
     const float* v1 = A.V1 + (size_t)g * GS;
     const float* v2 = A.V2 + (size_t)g * GS;
     for (int t = lane; t < GS; t += 32) {
-      bA[t] = v1[t];
-      bB[t] = v2[t];
+      bA[(t / DD) * DDP + t % DD] = v1[t];
+      bB[(t / DD) * DDP + t % DD] = v2[t];
     }
   }
   __syncwarp();
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   auto fwd = [&](const float* X, float* Y) {
     for (int task = lane; task < K * D; task += 32) {
       const int k = task / D, r = task % D;
-      const float* x = X + k * DD;
+      const float* x = X + k * DDP;
       float P[D];
 #pragma unroll
       for (int n = 0; n < D; ++n) {
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
         float acc = 0.f;
 #pragma unroll
         for (int n = 0; n < D; ++n) acc = fmaf(P[n], Tm[l + n * D], acc);
-        Y[k * DD + r + l * D] = acc;
+        Y[k * DDP + r + l * D] = acc;
       }
     }
   };
@@ -151,8 +152,8 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
     float v1[K], v2[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      v1[k] = bC[k * DD + e];
-      v2[k] = bA[k * DD + e];
+      v1[k] = bC[k * DDP + e];
+      v2[k] = bA[k * DDP + e];
     }
     haar_dec<K>(v1, cc);
     haar_dec<K>(v2, cc);
@@ -162,18 +163,21 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       const float p = v1[k] * v1[k];
       float f = p / (p + sg);
       if (e == 0 && k >= 14) f = 1.f;
-      bB[k * DD + e] = f;
+      bB[k * DDP + e] = f;
       v2[k] = v2[k] * f;
     }
     haar_rec<K>(v2, cc);
 #pragma unroll
-    for (int k = 0; k < K; ++k) bA[k * DD + e] = v2[k];
+    for (int k = 0; k < K; ++k) bA[k * DDP + e] = v2[k];
   }
   __syncwarp();
 
   // ---- n2 = norm(col(filt))^2 ------------------------------------------------
   float s = 0.f;
-  for (int e = lane; e < GS; e += 32) s = s + bB[e] * bB[e];
+  for (int e = lane; e < GS; e += 32) {
+    const float f = bB[(e / DD) * DDP + e % DD];
+    s = s + f * f;
+  }
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
   if (lane == 0) {
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   // ---- inverse DCT: P = Y Ti' (rows), X = Ti P (columns) ----------------------
   for (int task = lane; task < K * D; task += 32) {
     const int k = task / D, r = task % D;
-    const float* y = bA + k * DD;
+    const float* y = bA + k * DDP;
     float Prow[D];
 #pragma unroll
     for (int l = 0; l < D; ++l) {
@@ -194,13 +198,13 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       Prow[l] = acc;
     }
 #pragma unroll
-    for (int l = 0; l < D; ++l) bC[k * DD + r + l * D] = Prow[l];
+    for (int l = 0; l < D; ++l) bC[k * DDP + r + l * D] = Prow[l];
   }
   __syncwarp();
   float* og = A.out + (size_t)g * GS;
   for (int task = lane; task < K * D; task += 32) {
     const int k = task / D, l = task % D;
-    const float* p = bC + k * DD + l * D;
+    const float* p = bC + k * DDP + l * D;
 #pragma unroll
     for (int r = 0; r < D; ++r) {
       float acc = 0.f;
@@ -217,7 +221,7 @@ bool wiener_supported(int d, int K) { return (d == 4 || d == 8 || d == 16) && (K
 
 template <int D, int K>
 static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
-  const size_t sm = (size_t)(3 * D * D + 4 * 3 * D * D * K) * sizeof(float);
+  const size_t sm = (size_t)(3 * D * D + 4 * 3 * (D * D + 1) * K) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wiener<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
