@@ -7,169 +7,88 @@
 // contributions in exactly that order, so the result is bit-identical to the
 // sequential loop and needs no atomics.
 //
-// One warp owns a tile of TR x TC pixels.  The warp walks the candidate
-// contributions of the tile (every (reference, match) whose search window can
-// reach it) in reference loop order, 32 at a time, tests them against the tile
-// with a ballot and compacts the hits into a shared-memory list in the same
-// order.  Each lane then walks the list for its own pixel.  Contributions
-// falling outside the cropped image are never produced (the reference crops
-// them away, :207-208).
+// Contributions falling outside the cropped image are never produced (the
+// reference crops them away, denoiseAndAggregateGPU.m:207-208).
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace gbm3d {
 
-constexpr int TR = 8, TC = 4;  // tile rows (fast axis) x cols
-
 __host__ __device__ inline int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 __host__ __device__ inline int ceil_div(int a, int b) { return -floor_div(-a, b); }
 
-static int list_max(int d, int d2, int K) {
-  const int ni = (d + d2 - 2 + TR) / d + 2, nj = (d + d2 - 2 + TC) / d + 2;
-  return ni * nj * K;
-}
+constexpr int TR = 8, TC = 4;  // warp tile: 8 rows (fast axis) x 4 columns, one pixel per lane
+constexpr int LCAP = 96;       // list chunk per warp (entries); walked whenever it may overflow
+constexpr int BIAS = 1 << 12;  // offset added to tile-relative block origins before packing
 
-__global__ void __launch_bounds__(128) k_aggregate(AggArgs A, int lmax) {
+// One warp owns TR x TC pixels, one per lane.  Candidates (reference i, j,
+// slot k) whose search window can reach the tile are enumerated in the
+// reference's loop order, 32 per round; the ones whose block intersects the
+// tile are compacted, in order, into a shared-memory list of entries
+//   {packed tile-relative block origin, offset of the block data, weight bits}.
+// Each lane then walks the list four entries at a time: the four coverage
+// tests and the four (predicated) loads are issued together, then the
+// covered contributions are added to the lane's pixel in list order.
+template <int D, bool WIE>
+__global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   extern __shared__ int smi[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int d = A.d, dd = d * d, K = A.K;
   float* win = reinterpret_cast<float*>(smi);
-  int* lst = smi + dd + warp * 2 * lmax;
-  for (int t = threadIdx.x; t < dd; t += blockDim.x) win[t] = A.win[t];
+  int4* lst = reinterpret_cast<int4*>(smi + ((D * D + 3) & ~3)) + warp * LCAP;
+  for (int t = threadIdx.x; t < D * D; t += blockDim.x) win[t] = A.win[t];
   __syncthreads();
   const int tiles_r = (A.m + TR - 1) / TR, tiles_c = (A.n + TC - 1) / TC;
   const int tile = blockIdx.x * 4 + warp;
   if (tile >= tiles_r * tiles_c) return;
   const int R0 = (tile % tiles_r) * TR, C0 = (tile / tiles_r) * TC;
-  const int h = A.d2 / 2;
-  const int PR0 = R0 + h, PC0 = C0 + h;  // tile origin in the padded U of the reference
-  const int i_lo = max(0, ceil_div(PR0 - d - A.d2 + 2, d)), i_hi = min(A.M - 1, floor_div(PR0 + TR - 1, d));
-  const int j_lo = max(0, ceil_div(PC0 - d - A.d2 + 2, d)), j_hi = min(A.N - 1, floor_div(PC0 + TC - 1, d));
-  const int NI = i_hi - i_lo + 1, NJ = j_hi - j_lo + 1;
-  const int total = (NI > 0 && NJ > 0) ? NI * NJ * K : 0;
-  const unsigned FULL = 0xffffffffu;
-  int count = 0;
-  for (int base = 0; base < total; base += 32) {
-    const int q = base + lane;
-    bool hit = false;
-    int packed = 0, id = 0;
-    if (q < total) {
-      const int k = q % K, jj = (q / K) % NJ, ii = q / (K * NJ);
-      const int i = i_lo + ii, j = j_lo + jj, g = i + A.M * j;
-      const int nm = A.cnt ? A.cnt[g] : K;
-      if (k < nm) {
-        const int e = (int)A.S[(size_t)g * K + k] - 1;
-        const int r0 = i * d + e % A.d2, c0 = j * d + e / A.d2;
-        hit = r0 <= PR0 + TR - 1 && r0 + d - 1 >= PR0 && c0 <= PC0 + TC - 1 && c0 + d - 1 >= PC0;
-        packed = r0 | (c0 << 16);
-        id = g * K + k;
-      }
-    }
-    const unsigned bal = __ballot_sync(FULL, hit);
-    if (hit) {
-      const int pos = count + __popc(bal & ((1u << lane) - 1u));
-      lst[2 * pos] = packed;
-      lst[2 * pos + 1] = id;
-    }
-    count += __popc(bal);
-  }
-  __syncwarp();
-  const int pr = PR0 + (lane % TR), pc = PC0 + (lane / TR);
-  const size_t mn = (size_t)A.m * A.n;
-  float u = 0.f, w = 0.f;
-  for (int e = 0; e < count; ++e) {
-    const int packed = lst[2 * e];
-    const unsigned rr = (unsigned)(pr - (packed & 0xffff)), cc = (unsigned)(pc - (packed >> 16));
-    if (rr < (unsigned)d && cc < (unsigned)d) {
-      const int id = lst[2 * e + 1];
-      const int g = id / K, k = id % K;
-      const float wk = win[rr + cc * d];
-      float val, wv;
-      if (!A.wiener) {
-        const int i = g % A.M, j = g / A.M;
-        const float blk = A.blocks[(size_t)(i * d + rr) + (size_t)A.m * (j * d + cc) + mn * k];
-        const float wg = A.gw[g];
-        val = (wg * blk) * wk;
-        wv = wg * wk;
-      } else {
-        const float blk = A.blocks[(size_t)id * dd + rr + cc * d];
-        wv = wk / A.gw[g];
-        val = wv * blk;
-      }
-      u = u + val;
-      w = w + wv;
-    }
-  }
-  const int orow = R0 + lane % TR, ocol = C0 + lane / TR;
-  if (orow < A.m && ocol < A.n) {
-    A.U[orow + (size_t)A.m * ocol] = u;
-    A.W[orow + (size_t)A.m * ocol] = w;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Strided-ownership version (D = 8, 16, 32).  A warp owns a 32 x 32 tile; lane
-// (r, c) = (lane & 7, lane >> 3) owns the pixels (r + 8a, c + 4b), a < 4, b < 8.
-// A D x D block at any offset covers D/8 rows and D/4 columns of every lane's
-// pixels, so all lanes work on every contribution instead of the few whose
-// pixel it happens to cover.  Per-pixel accumulators sit in shared memory,
-// interleaved by lane (conflict-free).  Contributions are filtered in reference
-// loop order into a chunked list whose entries carry the block's tile-relative
-// origin, its data offset and its group weight; each pixel still receives its
-// contributions in exactly the reference order.
-// ---------------------------------------------------------------------------
-constexpr int AT = 32;     // warp tile side
-constexpr int LCAP = 256;  // list chunk capacity per warp
-
-template <int D, bool WIE>
-__global__ void __launch_bounds__(128) k_aggregate_tiled(AggArgs A) {
-  extern __shared__ float sma[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* mask = sma;                                          // D*D
-  float* acc = sma + D * D + warp * (2 * 32 * 32 + 4 * LCAP);  // [2][32 pixels][32 lanes]
-  int4* lst = reinterpret_cast<int4*>(acc + 2 * 32 * 32);
-  for (int t = threadIdx.x; t < D * D; t += blockDim.x) mask[t] = A.win[t];
-  for (int t = lane; t < 2 * 32 * 32; t += 32) acc[t] = 0.f;
-  __syncthreads();
-  const int tiles_r = (A.m + AT - 1) / AT, tiles_c = (A.n + AT - 1) / AT;
-  const int tile = blockIdx.x * 4 + warp;
-  if (tile >= tiles_r * tiles_c) return;
-  const int R0 = (tile % tiles_r) * AT, C0 = (tile / tiles_r) * AT;
   const int d2 = A.d2, K = A.K, h = d2 / 2;
   const int PR0 = R0 + h, PC0 = C0 + h;  // tile origin in the reference's padded U
-  const int i_lo = max(0, ceil_div(PR0 - D - d2 + 2, D)), i_hi = min(A.M - 1, floor_div(PR0 + AT - 1, D));
-  const int j_lo = max(0, ceil_div(PC0 - D - d2 + 2, D)), j_hi = min(A.N - 1, floor_div(PC0 + AT - 1, D));
+  const int i_lo = max(0, ceil_div(PR0 - D - d2 + 2, D)), i_hi = min(A.M - 1, floor_div(PR0 + TR - 1, D));
+  const int j_lo = max(0, ceil_div(PC0 - D - d2 + 2, D)), j_hi = min(A.N - 1, floor_div(PC0 + TC - 1, D));
   const int NI = i_hi - i_lo + 1, NJ = j_hi - j_lo + 1;
   const int total = (NI > 0 && NJ > 0) ? NI * NJ * K : 0;
   const size_t mn = (size_t)A.m * A.n;
-  const int r = lane & 7, c = lane >> 3;
   const unsigned FULL = 0xffffffffu;
+  // lane's candidate: slot k = lane % K (K divides 32) or by division otherwise
+  const bool kdiv = (32 % K) == 0;
+  const int step = kdiv ? 32 / K : 0;
+  int k_l = kdiv ? lane % K : 0, rq = kdiv ? lane / K : 0;
+  int ii = rq / max(NJ, 1), jj = rq - ii * max(NJ, 1);
 
+  const int pr = lane & 7, pc = lane >> 3;  // lane's pixel in the tile
+  float u = 0.f, w = 0.f;
   auto walk = [&](int count) {
-    for (int e = 0; e < count; ++e) {
-      const int4 ent = lst[e];
-      const int r0 = ent.x, c0 = ent.y;
-      const float wgt = __int_as_float(ent.w);
-      const int a_lo = max(0, (r0 - r + 7) >> 3), a_hi = min(3, (r0 + D - 1 - r) >> 3);
-      const int b_lo = max(0, (c0 - c + 3) >> 2), b_hi = min(7, (c0 + D - 1 - c) >> 2);
-      for (int a = a_lo; a <= a_hi; ++a) {
-        const int rr = r + 8 * a - r0;
-        for (int b = b_lo; b <= b_hi; ++b) {
-          const int cc = c + 4 * b - c0;
-          const float mk = mask[rr + cc * D];
+    for (int e0 = 0; e0 < count; e0 += 4) {
+      int4 en[4];
+      bool cov[4];
+      float blk[4];
+      int rr[4], cc[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const bool valid = e0 + t < count;
+        en[t] = lst[valid ? e0 + t : 0];
+        rr[t] = pr - ((en[t].x & 0xffff) - BIAS);
+        cc[t] = pc - ((en[t].x >> 16) - BIAS);
+        cov[t] = valid && (unsigned)rr[t] < (unsigned)D && (unsigned)cc[t] < (unsigned)D;
+        const size_t off = WIE ? (size_t)en[t].y * (D * D) + rr[t] + cc[t] * D
+                               : (size_t)(unsigned)en[t].y + rr[t] + (size_t)A.m * cc[t];
+        blk[t] = cov[t] ? __ldg(A.blocks + off) : 0.f;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (cov[t]) {
+          const float wk = win[rr[t] + cc[t] * D];
+          const float wg = __int_as_float(en[t].z);
           float val, wv;
           if (!WIE) {
-            const float blk = A.blocks[(size_t)ent.z + rr + (size_t)A.m * cc];
-            val = (wgt * blk) * mk;
-            wv = wgt * mk;
+            val = (wg * blk[t]) * wk;
+            wv = wg * wk;
           } else {
-            const float blk = A.blocks[(size_t)ent.z * (D * D) + rr + cc * D];
-            wv = mk / wgt;
-            val = wv * blk;
+            wv = wk / wg;
+            val = wv * blk[t];
           }
-          float* p = acc + (a * 8 + b) * 32 + lane;
-          p[0] = p[0] + val;
-          p[32 * 32] = p[32 * 32] + wv;
+          u = u + val;
+          w = w + wv;
         }
       }
     }
@@ -177,30 +96,37 @@ __global__ void __launch_bounds__(128) k_aggregate_tiled(AggArgs A) {
 
   int count = 0;
   for (int base = 0; base < total; base += 32) {
-    const int q = base + lane;
     bool hit = false;
     int4 ent = make_int4(0, 0, 0, 0);
-    if (q < total) {
-      const int k = q % K, rq = q / K, jj = rq % NJ, ii = rq / NJ;
-      const int i = i_lo + ii, j = j_lo + jj, g = i + A.M * j;
+    int k, i, j;
+    if (kdiv) {
+      k = k_l;
+      i = i_lo + ii;
+      j = j_lo + jj;
+    } else {
+      const int q = base + lane, r2 = q / K;
+      k = q - r2 * K;
+      const int i2 = r2 / NJ;
+      i = i_lo + i2;
+      j = j_lo + (r2 - i2 * NJ);
+    }
+    if (base + lane < total) {
+      const int g = i + A.M * j;
       const int nm = A.cnt ? A.cnt[g] : K;
       if (k < nm) {
         const int e = (int)A.S[(size_t)g * K + k] - 1;
         const int r0 = i * D + e % d2 - PR0, c0 = j * D + e / d2 - PC0;
-        hit = r0 < AT && r0 + D > 0 && c0 < AT && c0 + D > 0;
+        hit = r0 < TR && r0 + D > 0 && c0 < TC && c0 + D > 0;
         if (hit) {
-          ent.x = r0;
-          ent.y = c0;
-          // block data: step 1 reads the group tile of the image-shaped Vavg,
-          // step 2 the filtered group (offset in units of D*D)
-          ent.z = WIE ? g * K + k : 0;
-          if (!WIE) {
-            const size_t off = (size_t)i * D + (size_t)A.m * (j * D) + mn * k;
-            ent.z = (int)off;  // fits: checked on the host (m*n*K < 2^31)
-          }
-          ent.w = __float_as_int(A.gw[g]);
+          ent.x = (r0 + BIAS) | ((c0 + BIAS) << 16);
+          ent.y = WIE ? g * K + k : (int)((size_t)i * D + (size_t)A.m * (j * D) + mn * k);
+          ent.z = __float_as_int(A.gw[g]);
         }
       }
+    }
+    if (kdiv) {  // advance this lane's reference by 32/K positions in loop order
+      jj += step;
+      while (jj >= NJ) { jj -= NJ; ++ii; }
     }
     const unsigned bal = __ballot_sync(FULL, hit);
     if (hit) lst[count + __popc(bal & ((1u << lane) - 1u))] = ent;
@@ -214,43 +140,32 @@ __global__ void __launch_bounds__(128) k_aggregate_tiled(AggArgs A) {
   }
   __syncwarp();
   walk(count);
-  __syncwarp();
-  for (int a = 0; a < 4; ++a)
-    for (int b = 0; b < 8; ++b) {
-      const int orow = R0 + r + 8 * a, ocol = C0 + c + 4 * b;
-      if (orow < A.m && ocol < A.n) {
-        const float* p = acc + (a * 8 + b) * 32 + lane;
-        A.U[orow + (size_t)A.m * ocol] = p[0];
-        A.W[orow + (size_t)A.m * ocol] = p[32 * 32];
-      }
-    }
+  const int orow = R0 + pr, ocol = C0 + pc;
+  if (orow < A.m && ocol < A.n) {
+    A.U[orow + (size_t)A.m * ocol] = u;
+    A.W[orow + (size_t)A.m * ocol] = w;
+  }
 }
 
 template <int D, bool WIE>
-static cudaError_t launch_tiled(const AggArgs& A, cudaStream_t st) {
-  const size_t sm = (size_t)(D * D + 4 * (2 * 32 * 32 + 4 * LCAP)) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(k_aggregate_tiled<D, WIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+static cudaError_t launch_px(const AggArgs& A, cudaStream_t st) {
+  const size_t sm = (size_t)((D * D + 3) & ~3) * sizeof(float) + (size_t)4 * LCAP * sizeof(int4);
+  cudaError_t e = cudaFuncSetAttribute(k_aggregate_px<D, WIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int tiles = ((A.m + AT - 1) / AT) * ((A.n + AT - 1) / AT);
-  k_aggregate_tiled<D, WIE><<<(tiles + 3) / 4, 128, sm, st>>>(A);
+  const int tiles = ((A.m + TR - 1) / TR) * ((A.n + TC - 1) / TC);
+  k_aggregate_px<D, WIE><<<(tiles + 3) / 4, 128, sm, st>>>(A);
   return cudaGetLastError();
 }
 
 cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st) {
-  const bool offsets_fit = (size_t)A.m * A.n * A.K < ((size_t)1 << 31) && (size_t)A.M * A.N * A.K < ((size_t)1 << 31);
-  if (offsets_fit) {
-#define GBM3D_AGG_CASE(DD)                                                           \
-  if (A.d == DD) return A.wiener ? launch_tiled<DD, true>(A, st) : launch_tiled<DD, false>(A, st);
-    GBM3D_AGG_CASE(8) GBM3D_AGG_CASE(16) GBM3D_AGG_CASE(32)
+  // block data offsets are 32-bit in the list entries
+  if ((size_t)A.m * A.n * A.K >= ((size_t)1 << 31) || (size_t)A.M * A.N * A.K >= ((size_t)1 << 31))
+    return cudaErrorInvalidValue;
+#define GBM3D_AGG_CASE(DD) \
+  if (A.d == DD) return A.wiener ? launch_px<DD, true>(A, st) : launch_px<DD, false>(A, st);
+  GBM3D_AGG_CASE(4) GBM3D_AGG_CASE(8) GBM3D_AGG_CASE(16) GBM3D_AGG_CASE(32)
 #undef GBM3D_AGG_CASE
-  }
-  const int lmax = list_max(A.d, A.d2, A.K);
-  const size_t sm = (size_t)(A.d * A.d + 4 * 2 * lmax) * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(k_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  const int tiles = ((A.m + TR - 1) / TR) * ((A.n + TC - 1) / TC);
-  k_aggregate<<<(tiles + 3) / 4, 128, sm, st>>>(A, lmax);
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace gbm3d

@@ -254,56 +254,72 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
   constexpr int NY = 2 * FQY + HALO;  // staged rows
   constexpr int NX = 2 * FQX + HALO;  // staged columns
   constexpr int NYH = (NY + 1) / 2;   // de-interleaved half rows
+  constexpr int NYHP = ((NYH + 15) / 32) * 32 + 16;  // = 16 mod 32: even and odd rows in different banks
+  constexpr int RT = (NY + 31) / 32;  // row chunks per lane
   extern __shared__ float sm[];
   float* tz = sm;                     // [2 fz][NX x][NY y]
-  float* tx = sm + 2 * NX * NY;       // [4 comb][FQX qx][2 parity][NYH]
+  float* tx = sm + 2 * NX * NY;       // [4 comb][FQX qx][2 parity][NYHP]
   const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
   const int qy0 = blockIdx.x * FQY, qx0 = blockIdx.y * FQX, qz = blockIdx.z;
   const int y0 = 2 * qy0 - HALO - shift, x0 = 2 * qx0 - HALO - shift;
-  const size_t plane = (size_t)Ly * Lx;
-  const size_t zA = plane * pmod(2 * qz - shift, Lz), zB = plane * pmod(2 * qz - 1 - shift, Lz);
+  const size_t zA = (size_t)Ly * Lx * pmod(2 * qz - shift, Lz), zB = (size_t)Ly * Lx * pmod(2 * qz - 1 - shift, Lz);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 
   // stage 1: load the input tile of two slots and apply the slot-axis pass
-#pragma unroll 4
-  for (int e = threadIdx.x; e < NX * NY; e += 256) {
-    const int yy = e % NY, xx = e / NY;
-    const int gy = wrap1(y0 + yy, Ly), gx = wrap1(x0 + xx, Lx);
-    const float* col = in + gy + (size_t)Ly * gx;
-    const float u0 = __ldg(col + zA), u1 = __ldg(col + zB);  // taps k=0 (slot 2qz), k=1 (slot 2qz-1)
-    tz[e] = fmaf(fb.azl[1], u1, fmaf(fb.azl[0], u0, 0.f));
-    tz[NX * NY + e] = fmaf(fb.azh[1], u1, fmaf(fb.azh[0], u0, 0.f));
+  // (warps over columns, lanes over rows)
+  int gy[RT];
+#pragma unroll
+  for (int t = 0; t < RT; ++t) gy[t] = wrap1(y0 + lane + 32 * t, Ly);
+#pragma unroll 2
+  for (int xx = w; xx < NX; xx += 8) {
+    const float* col = in + (size_t)Ly * wrap1(x0 + xx, Lx);
+#pragma unroll
+    for (int t = 0; t < RT; ++t) {
+      const int yy = lane + 32 * t;
+      if (yy < NY) {
+        const float u0 = __ldg(col + gy[t] + zA), u1 = __ldg(col + gy[t] + zB);  // taps k=0, k=1
+        tz[xx * NY + yy] = fmaf(fb.azl[1], u1, fmaf(fb.azl[0], u0, 0.f));
+        tz[NX * NY + xx * NY + yy] = fmaf(fb.azh[1], u1, fmaf(fb.azh[0], u0, 0.f));
+      }
+    }
   }
   __syncthreads();
   // stage 2: pass along the slow axis, lo and hi together from the same inputs
-  for (int e = threadIdx.x; e < 2 * FQX * NY; e += 256) {
-    const int yy = e % NY, r = e / NY, qx = r % FQX, fz = r / FQX;
-    const float* src = tz + fz * NX * NY + yy + (2 * qx + HALO) * NY;  // input x = 2qx - k
-    float v[LA];
+  // (warps over (fz, qx), lanes over rows)
+  for (int pq = w; pq < 2 * FQX; pq += 8) {
+    const int fz = pq / FQX, qx = pq % FQX;
 #pragma unroll
-    for (int k = 0; k < LA; ++k) v[k] = src[-k * NY];
-    float lo = 0.f, hi = 0.f;
+    for (int t = 0; t < RT; ++t) {
+      const int yy = lane + 32 * t;
+      if (yy >= NY) continue;
+      const float* src = tz + fz * NX * NY + yy + (2 * qx + HALO) * NY;  // input x = 2qx - k
+      float v[LA];
 #pragma unroll
-    for (int k = 0; k < LA; ++k) lo = fmaf(fb.alo[k], v[k], lo);
+      for (int k = 0; k < LA; ++k) v[k] = src[-k * NY];
+      float lo = 0.f, hi = 0.f;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[HA0 + k], hi);
-    float* dst = tx + (yy & 1) * NYH + (yy >> 1);
-    dst[((0 + 2 * fz) * FQX + qx) * 2 * NYH] = lo;
-    dst[((1 + 2 * fz) * FQX + qx) * 2 * NYH] = hi;
+      for (int k = 0; k < LA; ++k) lo = fmaf(fb.alo[k], v[k], lo);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[HA0 + k], hi);
+      float* dst = tx + (yy & 1) * NYHP + (yy >> 1);
+      dst[((0 + 2 * fz) * FQX + qx) * 2 * NYHP] = lo;
+      dst[((1 + 2 * fz) * FQX + qx) * 2 * NYHP] = hi;
+    }
   }
   __syncthreads();
   // stage 3: pass along the fast axis, threshold, store (lanes along qy)
-  const int qy = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int qy = lane;
   const size_t bsz = (size_t)Oy * Ox * Oz;
   const bool row_ok = qy0 + qy < Oy;
   for (int j = w; j < 4 * FQX; j += 8) {
     const int qx = j % FQX, comb = j / FQX;
     if (!row_ok || qx0 + qx >= Ox) continue;
-    const float* src = tx + (comb * FQX + qx) * 2 * NYH;
+    const float* src = tx + (comb * FQX + qx) * 2 * NYHP;
     float v[LA];
 #pragma unroll
     for (int k = 0; k < LA; ++k) {
       const int R = HALO - k;  // row 2qy + HALO - k
-      v[k] = src[(R & 1) * NYH + qy + (R >> 1)];
+      v[k] = src[(R & 1) * NYHP + qy + (R >> 1)];
     }
     float lo = 0.f, hi = 0.f;
 #pragma unroll
@@ -456,7 +472,8 @@ template <int LA, int HA0>
 static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
                                         const FastBank& fb, const LevelBands& th, cudaStream_t st) {
   constexpr int NY = 2 * FQY + LA - 1, NX = 2 * FQX + LA - 1, NYH = (NY + 1) / 2;
-  const size_t sm = (size_t)(2 * NX * NY + 4 * FQX * 2 * NYH) * sizeof(float);
+  constexpr int NYHP = ((NYH + 15) / 32) * 32 + 16;
+  const size_t sm = (size_t)(2 * NX * NY + 4 * FQX * 2 * NYHP) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_fast<LA, HA0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   dim3 grid((Ly / 2 + FQY - 1) / FQY, (Lx / 2 + FQX - 1) / FQX, Lz / 2);
@@ -478,15 +495,17 @@ static cudaError_t launch_synthesis_fast(const float* bands, const float* approx
   return cudaGetLastError();
 }
 
-// Compile-time block size version of k_ht_weights: the index decompositions
-// become multiplications by constants, and each lane walks its elements
-// (e = lane + 32 t of each difference array, in increasing e) exactly as the
-// generic kernel and the oracle do.
+// Compile-time block size version of k_ht_weights.  The group is streamed one
+// slot at a time through a shared-memory slice (read once, coalesced).  Every
+// difference array is slot-major, so walking the slots in order keeps each
+// lane's elements (e = lane + 32 t of each array) in increasing e: the sums
+// are the same fixed-order reductions as the generic kernel and the oracle.
 template <int D>
 __global__ void __launch_bounds__(128) k_ht_weights_t(const float* __restrict__ V, int m, int n, int M, int N,
                                                       int K, const int32_t* __restrict__ cnt,
                                                       float* __restrict__ wgt) {
-  constexpr int DM = D - 3;
+  constexpr int DM = D - 3, SL = D * D, SX = D * DM;  // slice size, per-slot elements of the x/y terms
+  __shared__ float sl[4][2][SL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = blockIdx.x * 4 + warp;
   if (g >= M * N) return;
@@ -495,22 +514,27 @@ __global__ void __launch_bounds__(128) k_ht_weights_t(const float* __restrict__ 
   const size_t sz = (size_t)m * n;
   const float* base = V + (size_t)i * D + (size_t)j * D * m;
   float tx = 0.f, ty = 0.f, tz = 0.f;
-  const int nx = D * DM * nm;
-  for (int e = lane; e < nx; e += 32) {
-    const int r = e % D, q = e / D, c = q % DM, k = q / DM;
-    const float* p = base + r + (size_t)c * m + sz * k;
-    tx = tx + fabsf(d3(__ldg(p), __ldg(p + m), __ldg(p + 2 * m), __ldg(p + 3 * m)));
-  }
-  for (int e = lane; e < nx; e += 32) {
-    const int r = e % DM, q = e / DM, c = q % D, k = q / D;
-    const float* p = base + r + (size_t)c * m + sz * k;
-    ty = ty + fabsf(d3(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)));
-  }
-  const int nzz = D * D * (nm - 1);
-  for (int e = lane; e < nzz; e += 32) {
-    const int r = e % D, q = e / D, c = q % D, k = q / D;
-    const float* p = base + r + (size_t)c * m + sz * k;
-    tz = tz + fabsf(__ldg(p + sz) - __ldg(p));
+  for (int k = 0; k < nm; ++k) {
+    float* cur = sl[warp][k & 1];
+    const float* prv = sl[warp][(k & 1) ^ 1];
+    for (int t = lane; t < SL; t += 32) cur[t] = __ldg(base + (t % D) + (size_t)(t / D) * m + sz * k);
+    __syncwarp();
+    // x term: element r + D (c + DM k); this lane's first element of slot k
+    for (int e = ((lane - k * SX) % 32 + 32) % 32; e < SX; e += 32) {
+      const int r = e % D, c = e / D;
+      const float* p = cur + r + c * D;
+      tx = tx + fabsf(d3(p[0], p[D], p[2 * D], p[3 * D]));
+    }
+    // y term: element r + DM (c + D k)
+    for (int e = ((lane - k * SX) % 32 + 32) % 32; e < SX; e += 32) {
+      const int r = e % DM, c = e / DM;
+      const float* p = cur + r + c * D;
+      ty = ty + fabsf(d3(p[0], p[1], p[2], p[3]));
+    }
+    // slot term: element r + D (c + D (k-1)) for the pair (k-1, k)
+    if (k > 0)
+      for (int e = ((lane - (k - 1) * SL) % 32 + 32) % 32; e < SL; e += 32) tz = tz + fabsf(cur[e] - prv[e]);
+    __syncwarp();
   }
   tx = warp_sum(tx);
   ty = warp_sum(ty);

@@ -77,15 +77,18 @@ __device__ __forceinline__ void haar_rec(float* v, float cc) {
 template <int D, int K>
 __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   constexpr int DD = D * D, GS = DD * K;
-  constexpr int DDP = DD + 1, GSP = DDP * K;  // slot pages padded by one word: no bank conflicts
+  // shared layout of one group: element (r, c) of slot k at k*PG + r + CS*c.
+  // Column stride d+1 and page stride d(d+1) keep every access pattern below
+  // (rows of a page, columns of a page, one coefficient across slots) free
+  // of bank conflicts.
+  constexpr int CS = D + 1, PG = D * CS, GSP = PG * K;
   extern __shared__ float sm[];
   float* Tm = sm;
   float* Ti = sm + DD;
   float* s2 = sm + 2 * DD;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* bA = sm + 3 * DD + warp * 3 * GSP;
-  float* bB = bA + GSP;
-  float* bC = bB + GSP;
+  float* b1 = sm + 3 * DD + warp * 2 * GSP;  // pilot group, later its Wiener gains
+  float* b2 = b1 + GSP;                      // noisy group
   for (int t = threadIdx.x; t < DD; t += blockDim.x) {
     Tm[t] = A.T[t];
     Ti[t] = A.Ti[t];
@@ -106,54 +109,61 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       const size_t o = (size_t)(i * D + a) + (size_t)(j * D + b) * A.P;
       for (int t = lane; t < DD; t += 32) {
         const int r = t % D, c = t / D;
-        bA[k * DDP + t] = A.padP[o + r + (size_t)c * A.P];
-        bB[k * DDP + t] = A.padN[o + r + (size_t)c * A.P];
+        b1[k * PG + r + CS * c] = A.padP[o + r + (size_t)c * A.P];
+        b2[k * PG + r + CS * c] = A.padN[o + r + (size_t)c * A.P];
       }
     }
   } else {
     const float* v1 = A.V1 + (size_t)g * GS;
     const float* v2 = A.V2 + (size_t)g * GS;
     for (int t = lane; t < GS; t += 32) {
-      bA[(t / DD) * DDP + t % DD] = v1[t];
-      bB[(t / DD) * DDP + t % DD] = v2[t];
+      const int k = t / DD, r = t % D, c = (t % DD) / D;
+      b1[k * PG + r + CS * c] = v1[t];
+      b2[k * PG + r + CS * c] = v2[t];
     }
   }
   __syncwarp();
 
-  // ---- forward DCT of each slot page: task (k, r) produces row r of T X T'
-  auto fwd = [&](const float* X, float* Y) {
-    for (int task = lane; task < K * D; task += 32) {
-      const int k = task / D, r = task % D;
-      const float* x = X + k * DDP;
+  // ---- forward DCT of each slot page, in place: task (k, r) -> row r of T X T'.
+  // K*D is a multiple of 32 and 32 a multiple of D, so each round holds whole
+  // pages: all their rows are read before any is written back.
+  auto fwd = [&](float* X) {
+    for (int t0 = 0; t0 < K * D; t0 += 32) {
+      const int k = (t0 + lane) / D, r = (t0 + lane) % D;
+      const float* x = X + k * PG;
       float P[D];
 #pragma unroll
       for (int n = 0; n < D; ++n) {
         float acc = 0.f;
 #pragma unroll
-        for (int jj = 0; jj < D; ++jj) acc = fmaf(Tm[r + jj * D], x[jj + n * D], acc);
+        for (int jj = 0; jj < D; ++jj) acc = fmaf(Tm[r + jj * D], x[jj + CS * n], acc);
         P[n] = acc;
       }
+      float Y[D];
 #pragma unroll
       for (int l = 0; l < D; ++l) {
         float acc = 0.f;
 #pragma unroll
         for (int n = 0; n < D; ++n) acc = fmaf(P[n], Tm[l + n * D], acc);
-        Y[k * DDP + r + l * D] = acc;
+        Y[l] = acc;
       }
+      __syncwarp();
+#pragma unroll
+      for (int l = 0; l < D; ++l) X[k * PG + r + CS * l] = Y[l];
+      __syncwarp();
     }
   };
-  fwd(bA, bC);  // pilot coefficients -> bC
-  __syncwarp();
-  fwd(bB, bA);  // noisy coefficients -> bA
-  __syncwarp();
+  fwd(b1);
+  fwd(b2);
 
   // ---- Haar along slots, Wiener gain, inverse Haar (lane per coefficient) ----
   for (int e = lane; e < DD; e += 32) {
+    const int off = e % D + CS * (e / D);
     float v1[K], v2[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      v1[k] = bC[k * DDP + e];
-      v2[k] = bA[k * DDP + e];
+      v1[k] = b1[k * PG + off];
+      v2[k] = b2[k * PG + off];
     }
     haar_dec<K>(v1, cc);
     haar_dec<K>(v2, cc);
@@ -163,19 +173,20 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       const float p = v1[k] * v1[k];
       float f = p / (p + sg);
       if (e == 0 && k >= 14) f = 1.f;
-      bB[k * DDP + e] = f;
+      b1[k * PG + off] = f;
       v2[k] = v2[k] * f;
     }
     haar_rec<K>(v2, cc);
 #pragma unroll
-    for (int k = 0; k < K; ++k) bA[k * DDP + e] = v2[k];
+    for (int k = 0; k < K; ++k) b2[k * PG + off] = v2[k];
   }
   __syncwarp();
 
-  // ---- n2 = norm(col(filt))^2 ------------------------------------------------
+  // ---- n2 = norm(col(filt))^2: lane l adds elements o = l, l+32, ... ----------
   float s = 0.f;
-  for (int e = lane; e < GS; e += 32) {
-    const float f = bB[(e / DD) * DDP + e % DD];
+  for (int o = lane; o < GS; o += 32) {
+    const int k = o / DD, e = o % DD;
+    const float f = b1[k * PG + e % D + CS * (e / D)];
     s = s + f * f;
   }
 #pragma unroll
@@ -184,27 +195,28 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
     const float nr = sqrtf(s);
     A.n2[g] = nr * nr;
   }
+  __syncwarp();
 
-  // ---- inverse DCT: P = Y Ti' (rows), X = Ti P (columns) ----------------------
+  // ---- inverse DCT: P = Y Ti' (rows, into b1), X = Ti P (columns, to global) ----
   for (int task = lane; task < K * D; task += 32) {
     const int k = task / D, r = task % D;
-    const float* y = bA + k * DDP;
+    const float* y = b2 + k * PG;
     float Prow[D];
 #pragma unroll
     for (int l = 0; l < D; ++l) {
       float acc = 0.f;
 #pragma unroll
-      for (int n = 0; n < D; ++n) acc = fmaf(y[r + n * D], Ti[l + n * D], acc);
+      for (int n = 0; n < D; ++n) acc = fmaf(y[r + CS * n], Ti[l + n * D], acc);
       Prow[l] = acc;
     }
 #pragma unroll
-    for (int l = 0; l < D; ++l) bC[k * DDP + r + l * D] = Prow[l];
+    for (int l = 0; l < D; ++l) b1[k * PG + r + CS * l] = Prow[l];
   }
   __syncwarp();
   float* og = A.out + (size_t)g * GS;
   for (int task = lane; task < K * D; task += 32) {
     const int k = task / D, l = task % D;
-    const float* p = bC + k * DDP + l * D;
+    const float* p = b1 + k * PG + CS * l;
 #pragma unroll
     for (int r = 0; r < D; ++r) {
       float acc = 0.f;
@@ -221,7 +233,7 @@ bool wiener_supported(int d, int K) { return (d == 4 || d == 8 || d == 16) && (K
 
 template <int D, int K>
 static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
-  const size_t sm = (size_t)(3 * D * D + 4 * 3 * (D * D + 1) * K) * sizeof(float);
+  const size_t sm = (size_t)(3 * D * D + 4 * 2 * D * (D + 1) * K) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wiener<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
