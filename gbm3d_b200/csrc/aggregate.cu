@@ -24,71 +24,73 @@ constexpr int BIAS = 1 << 12;  // offset added to tile-relative block origins be
 // One warp owns TR x TC pixels, one per lane.  Candidates (reference i, j,
 // slot k) whose search window can reach the tile are enumerated in the
 // reference's loop order, 32 per round; the ones whose block intersects the
-// tile are compacted, in order, into a shared-memory list of entries
-//   {packed tile-relative block origin, offset of the block data, weight bits}.
-// Each lane then walks the list four entries at a time: the four coverage
-// tests and the four (predicated) loads are issued together, then the
-// covered contributions are added to the lane's pixel in list order.
-template <int D, bool WIE>
+// tile are compacted, in order, into a shared-memory list.  An entry holds the
+// block's tile-relative origin and the offsets of its data and weights minus
+// that origin, so a lane reaches its own element by adding a lane constant.
+// Each lane walks the list four entries at a time: four coverage tests and
+// four (predicated) loads are issued together, then the covered
+// contributions are added to the lane's pixel in list order.
+//   step 1: value (wg * Vavg) * mask, weight wg * mask   (denoiseAndAggregateGPU.m:200-201)
+//   step 2: value and weight precomputed by the Wiener kernel (:84-90 of
+//           denoiseAndAggregateWieFast.m), the same single-precision products
+template <int D, int D2, bool WIE>
 __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   extern __shared__ int smi[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* win = reinterpret_cast<float*>(smi);
   int4* lst = reinterpret_cast<int4*>(smi + ((D * D + 3) & ~3)) + warp * LCAP;
-  for (int t = threadIdx.x; t < D * D; t += blockDim.x) win[t] = A.win[t];
+  if (!WIE)
+    for (int t = threadIdx.x; t < D * D; t += blockDim.x) win[t] = A.win[t];
   __syncthreads();
   const int tiles_r = (A.m + TR - 1) / TR, tiles_c = (A.n + TC - 1) / TC;
   const int tile = blockIdx.x * 4 + warp;
   if (tile >= tiles_r * tiles_c) return;
   const int R0 = (tile % tiles_r) * TR, C0 = (tile / tiles_r) * TC;
-  const int d2 = A.d2, K = A.K, h = d2 / 2;
-  const int PR0 = R0 + h, PC0 = C0 + h;  // tile origin in the reference's padded U
-  const int i_lo = max(0, ceil_div(PR0 - D - d2 + 2, D)), i_hi = min(A.M - 1, floor_div(PR0 + TR - 1, D));
-  const int j_lo = max(0, ceil_div(PC0 - D - d2 + 2, D)), j_hi = min(A.N - 1, floor_div(PC0 + TC - 1, D));
+  const int K = A.K, m = A.m;
+  constexpr int H = D2 / 2;
+  const int PR0 = R0 + H, PC0 = C0 + H;  // tile origin in the reference's padded U
+  const int i_lo = max(0, ceil_div(PR0 - D - D2 + 2, D)), i_hi = min(A.M - 1, floor_div(PR0 + TR - 1, D));
+  const int j_lo = max(0, ceil_div(PC0 - D - D2 + 2, D)), j_hi = min(A.N - 1, floor_div(PC0 + TC - 1, D));
   const int NI = i_hi - i_lo + 1, NJ = j_hi - j_lo + 1;
   const int total = (NI > 0 && NJ > 0) ? NI * NJ * K : 0;
-  const size_t mn = (size_t)A.m * A.n;
+  const size_t mn = (size_t)m * A.n;
   const unsigned FULL = 0xffffffffu;
-  // lane's candidate: slot k = lane % K (K divides 32) or by division otherwise
+  // lane's candidate: slot k = lane % K when K divides 32, else by division
   const bool kdiv = (32 % K) == 0;
   const int step = kdiv ? 32 / K : 0;
-  int k_l = kdiv ? lane % K : 0, rq = kdiv ? lane / K : 0;
+  const int k_l = kdiv ? lane % K : 0, rq = kdiv ? lane / K : 0;
   int ii = rq / max(NJ, 1), jj = rq - ii * max(NJ, 1);
 
   const int pr = lane & 7, pc = lane >> 3;  // lane's pixel in the tile
+  const int vlane = WIE ? pr + pc * D : pr + m * pc;
+  const int wlane = pr + pc * D;
   float u = 0.f, w = 0.f;
   auto walk = [&](int count) {
     for (int e0 = 0; e0 < count; e0 += 4) {
       int4 en[4];
       bool cov[4];
-      float blk[4];
-      int rr[4], cc[4];
+      float val[4], wv[4];
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const bool valid = e0 + t < count;
         en[t] = lst[valid ? e0 + t : 0];
-        rr[t] = pr - ((en[t].x & 0xffff) - BIAS);
-        cc[t] = pc - ((en[t].x >> 16) - BIAS);
-        cov[t] = valid && (unsigned)rr[t] < (unsigned)D && (unsigned)cc[t] < (unsigned)D;
-        const size_t off = WIE ? (size_t)en[t].y * (D * D) + rr[t] + cc[t] * D
-                               : (size_t)(unsigned)en[t].y + rr[t] + (size_t)A.m * cc[t];
-        blk[t] = cov[t] ? __ldg(A.blocks + off) : 0.f;
+        const int rr = pr - ((en[t].x & 0xffff) - BIAS), cc = pc - ((en[t].x >> 16) - BIAS);
+        cov[t] = valid && (unsigned)rr < (unsigned)D && (unsigned)cc < (unsigned)D;
+        val[t] = cov[t] ? __ldg(A.blocks + ((size_t)(unsigned)(en[t].y + vlane))) : 0.f;
+        if (WIE) wv[t] = cov[t] ? __ldg(A.gw + ((size_t)(unsigned)(en[t].z + wlane))) : 0.f;
+        else wv[t] = cov[t] ? win[rr + cc * D] : 0.f;
       }
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         if (cov[t]) {
-          const float wk = win[rr[t] + cc[t] * D];
-          const float wg = __int_as_float(en[t].z);
-          float val, wv;
-          if (!WIE) {
-            val = (wg * blk[t]) * wk;
-            wv = wg * wk;
+          if (WIE) {
+            u = u + val[t];
+            w = w + wv[t];
           } else {
-            wv = wk / wg;
-            val = wv * blk[t];
+            const float wg = __int_as_float(en[t].z);
+            u = u + (wg * val[t]) * wv[t];
+            w = w + wg * wv[t];
           }
-          u = u + val;
-          w = w + wv;
         }
       }
     }
@@ -115,12 +117,17 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
       const int nm = A.cnt ? A.cnt[g] : K;
       if (k < nm) {
         const int e = (int)A.S[(size_t)g * K + k] - 1;
-        const int r0 = i * D + e % d2 - PR0, c0 = j * D + e / d2 - PC0;
+        const int r0 = i * D + e % D2 - PR0, c0 = j * D + e / D2 - PC0;
         hit = r0 < TR && r0 + D > 0 && c0 < TC && c0 + D > 0;
         if (hit) {
           ent.x = (r0 + BIAS) | ((c0 + BIAS) << 16);
-          ent.y = WIE ? g * K + k : (int)((size_t)i * D + (size_t)A.m * (j * D) + mn * k);
-          ent.z = __float_as_int(A.gw[g]);
+          if (WIE) {
+            ent.y = (g * K + k) * (D * D) - r0 - c0 * D;
+            ent.z = g * (D * D) - r0 - c0 * D;
+          } else {
+            ent.y = (int)((size_t)i * D + (size_t)m * (j * D) + mn * k) - r0 - m * c0;
+            ent.z = __float_as_int(A.gw[g]);
+          }
         }
       }
     }
@@ -147,23 +154,27 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   }
 }
 
-template <int D, bool WIE>
+template <int D, int D2, bool WIE>
 static cudaError_t launch_px(const AggArgs& A, cudaStream_t st) {
   const size_t sm = (size_t)((D * D + 3) & ~3) * sizeof(float) + (size_t)4 * LCAP * sizeof(int4);
-  cudaError_t e = cudaFuncSetAttribute(k_aggregate_px<D, WIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = cudaFuncSetAttribute(k_aggregate_px<D, D2, WIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = ((A.m + TR - 1) / TR) * ((A.n + TC - 1) / TC);
-  k_aggregate_px<D, WIE><<<(tiles + 3) / 4, 128, sm, st>>>(A);
+  k_aggregate_px<D, D2, WIE><<<(tiles + 3) / 4, 128, sm, st>>>(A);
   return cudaGetLastError();
 }
 
 cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st) {
   // block data offsets are 32-bit in the list entries
-  if ((size_t)A.m * A.n * A.K >= ((size_t)1 << 31) || (size_t)A.M * A.N * A.K >= ((size_t)1 << 31))
+  if ((size_t)A.m * A.n * A.K >= ((size_t)1 << 31) || (size_t)A.M * A.N * A.K * A.d * A.d >= ((size_t)1 << 31))
     return cudaErrorInvalidValue;
-#define GBM3D_AGG_CASE(DD) \
-  if (A.d == DD) return A.wiener ? launch_px<DD, true>(A, st) : launch_px<DD, false>(A, st);
-  GBM3D_AGG_CASE(4) GBM3D_AGG_CASE(8) GBM3D_AGG_CASE(16) GBM3D_AGG_CASE(32)
+#define GBM3D_AGG_CASE(DD, DD2)                                                                 \
+  if (A.d == DD && A.d2 == DD2)                                                                 \
+    return A.wiener ? launch_px<DD, DD2, true>(A, st) : launch_px<DD, DD2, false>(A, st);
+  GBM3D_AGG_CASE(8, 16) GBM3D_AGG_CASE(8, 24) GBM3D_AGG_CASE(8, 32)
+  GBM3D_AGG_CASE(16, 16) GBM3D_AGG_CASE(16, 24) GBM3D_AGG_CASE(16, 32)
+  GBM3D_AGG_CASE(32, 16) GBM3D_AGG_CASE(32, 24) GBM3D_AGG_CASE(32, 32)
+  GBM3D_AGG_CASE(4, 16) GBM3D_AGG_CASE(4, 24) GBM3D_AGG_CASE(4, 32)
 #undef GBM3D_AGG_CASE
   return cudaErrorInvalidValue;
 }

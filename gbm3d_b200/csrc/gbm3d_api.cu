@@ -418,8 +418,10 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
 }
 
 void fill_wiener_consts(WienerArgs& A, int d, const double* sigma, int is_matrix, int variant) {
-  std::vector<double> Tm(d * d), Ti(d * d);
+  std::vector<double> Tm(d * d), Ti(d * d), wk(d * d);
   dct_matrices(d, Tm.data(), Ti.data());
+  sine_window(d, 0.2, 0.8, wk.data());  // w = outer(sin(pi*linspace(.2,.8,d))) (denoiseAndAggregateWieFast.m:73-76)
+  for (int e = 0; e < d * d; ++e) A.win[e] = (float)wk[e];
   for (int e = 0; e < d * d; ++e) {
     A.T[e] = (float)Tm[e];
     A.Ti[e] = variant == 0 ? (float)Ti[e] : (float)Tm[(e / d) + (e % d) * d];
@@ -434,6 +436,7 @@ void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float*
   if (!wiener_supported(d, K))
     argfail(c, "unsupported (blockSizeWie, numMax) pair for the Wiener step", GBM3D_ERR_UNSUPPORTED);
   A.out = buf<float>(c, "wie.out", (size_t)d * d * K * M * N);
+  A.wt = buf<float>(c, "wie.wt", (size_t)d * d * M * N);
   A.n2 = buf<float>(c, "wie.n2", (size_t)M * N);
   {
     StageTimer t(c, 5);
@@ -450,10 +453,7 @@ void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float*
   G.K = K;
   G.wiener = 1;
   G.blocks = A.out;
-  G.gw = A.n2;
-  std::vector<double> wk(d * d);
-  sine_window(d, 0.2, 0.8, wk.data());
-  for (int e = 0; e < d * d; ++e) G.win[e] = (float)wk[e];
+  G.gw = A.wt;
   G.m = M * d;
   G.n = N * d;
   G.U = U;

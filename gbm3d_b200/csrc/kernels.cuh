@@ -71,7 +71,9 @@ struct WienerArgs {
   float T[256];       // DCT-II matrix (d x d, column-major)
   float Ti[256];      // inverse used by the inverse transform
   int clamp_one;      // legacy variant: clamp to [0,1]
-  float* out;         // filtered groups, d x d x K x M x N
+  float win[256];     // aggregation window w (d x d), single precision
+  float* out;         // weighted filtered groups fl(wv .* block), d x d x K x M x N
+  float* wt;          // per-group weights wv = fl(w / n2), d x d x M x N
   float* n2;          // ||filt||^2 per group (sqrt then square, single)
 };
 bool wiener_supported(int d, int K);
@@ -82,10 +84,10 @@ struct AggArgs {
   const uint32_t* S;
   const int32_t* cnt;   // may be null (every group holds K)
   int M, N, d, d2, K;
-  int wiener;           // 0: step-1 weights (scalar x mask); 1: step-2 (window / n2)
-  const float* blocks;  // step 1: image-shaped Vavg (m x n x K); step 2: d x d x K per group
-  const float* gw;      // step 1: weight per group; step 2: n2 per group
-  float win[1024];      // step 1: mask; step 2: Wiener window (d x d)
+  int wiener;           // 0: step-1 weights (scalar x mask); 1: step-2 (precomputed)
+  const float* blocks;  // step 1: image-shaped Vavg (m x n x K); step 2: weighted values, d x d x K per group
+  const float* gw;      // step 1: weight per group; step 2: weight table, d x d per group
+  float win[1024];      // step 1: mask (d x d)
   int m, n;             // output size (m = M*d, n = N*d)
   float* U;             // m x n
   float* W;

@@ -8,7 +8,8 @@
 // (it is the candidate at offset (d2/2, d2/2)) by warp-uniform broadcasts.
 //
 // Distances are exact FP32 sums of squared differences, row-major over the
-// block: t = x - y; acc = fmaf(t, t, acc).  The K best candidates are the K
+// block: t = x - y; acc = fmaf(t, t, acc), two candidates per paired
+// instruction.  The K best candidates are the K
 // smallest (distance, column-major window index) pairs — the stable order of
 // MATLAB's mink — found by a bitwise radix search for the K-th smallest
 // distance with warp reductions, then an index-ordered pick among ties.
@@ -16,6 +17,29 @@
 #include "kernels.cuh"
 
 namespace gbm3d {
+
+typedef unsigned long long u64;
+
+// Paired single-precision arithmetic of sm_100 (two IEEE round-to-nearest
+// operations per instruction on a 64-bit register pair).
+__device__ __forceinline__ u64 pack2(float lo, float hi) {
+  u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(u64 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
+  u64 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+  u64 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
 
 // Ipad of the reference for a circularly shifted image: rows (m+d2), cols
 // (n+d2), column pitch P floats.  spin is the circshift applied to the image.
@@ -36,7 +60,7 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
   extern __shared__ float smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* win = smem + warp * (WD * WD);
-  uint32_t* lst = reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 96;  // keys, idx, S
+  uint32_t* lst = reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 224;  // keys, idx, S, bounded set
   const int g = blockIdx.x * 4 + warp;
   if (g >= A.M * A.N) return;  // warp-uniform
   const int i = g % A.M, j = g / A.M;
@@ -48,29 +72,54 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
   __syncwarp();
 
   // ---- exact SSD for the lane's candidates (a = lane, b = 0..D2-1) ----------
-  float acc[D2];
+  // Accumulators are held in pairs (acc[b], acc[b+1]) and updated with the
+  // paired FP32 instructions of sm_100 (sub.rn.f32x2, fma.rn.f32x2), which
+  // round each component exactly as the scalar sub/fmaf would: candidate b
+  // still sees t = x(r, c) - y, acc = fmaf(t, t, acc) in (r, c) order.  At
+  // window column xw the pair needs x(r, xw-b) and x(r, xw-b-1), kept packed
+  // per row as xp[c] = (x(r,c), x(r,c-1)).
+  u64 acc2[D2 / 2];
 #pragma unroll
-  for (int b = 0; b < D2; ++b) acc[b] = 0.f;
+  for (int p = 0; p < D2 / 2; ++p) acc2[p] = 0ull;
   const int a = lane < D2 ? lane : 0;
 #pragma unroll 1
   for (int r = 0; r < D; ++r) {
     float xr[D];
 #pragma unroll
     for (int c = 0; c < D; ++c) xr[c] = win[(H + r) + (H + c) * WD];
+    u64 xp[D];
+#pragma unroll
+    for (int c = 1; c < D; ++c) xp[c] = pack2(xr[c], xr[c - 1]);
     const float* wrow = win + (a + r);
 #pragma unroll
     for (int xw = 0; xw < WD; ++xw) {
       const float w = wrow[xw * WD];
+      const u64 w2 = pack2(w, w);
 #pragma unroll
-      for (int b = 0; b < D2; ++b) {
-        const int c = xw - b;
-        if (c >= 0 && c < D) {
-          const float t = xr[c] - w;
-          acc[b] = fmaf(t, t, acc[b]);
+      for (int p = 0; p < D2 / 2; ++p) {
+        const int c = xw - 2 * p;  // column of candidate b = 2p; b+1 uses c-1
+        if (c >= 1 && c <= D - 1) {
+          const u64 t2 = sub2(xp[c], w2);
+          acc2[p] = fma2(t2, t2, acc2[p]);
+        } else if (c == 0) {
+          float lo, hi;
+          unpack2(acc2[p], lo, hi);
+          const float t = xr[0] - w;
+          lo = fmaf(t, t, lo);
+          acc2[p] = pack2(lo, hi);
+        } else if (c == D) {
+          float lo, hi;
+          unpack2(acc2[p], lo, hi);
+          const float t = xr[D - 1] - w;
+          hi = fmaf(t, t, hi);
+          acc2[p] = pack2(lo, hi);
         }
       }
     }
   }
+  float acc[D2];
+#pragma unroll
+  for (int p = 0; p < D2 / 2; ++p) unpack2(acc2[p], acc[2 * p], acc[2 * p + 1]);
 
   // ---- selection -------------------------------------------------------------
   const unsigned FULL = 0xffffffffu;
@@ -100,7 +149,63 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
     else { index_order = true; count = found; }
     if (!index_order) count = want;
   }
+  // Fast exact path: T = the want-th smallest of the 32 lane minima is >= the
+  // want-th smallest key, so the selection lies in {key <= T}.  When that set
+  // holds at most 64 keys, rank them by (key, index) directly.
+  uint32_t* lkey = lst;
+  uint32_t* lidx = lst + 32;
+  uint32_t* lS = lst + 64;
+  uint32_t* bkey = lst + 96;   // 64 keys and 64 indices of the bounded candidate set
+  uint32_t* bidx = lst + 160;
+  bool ranked = false;
   if (!index_order) {
+    uint32_t lm = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < D2; ++b) lm = min(lm, key[b]);
+    // bitonic sort of the lane minima across the warp (ascending by lane)
+    uint32_t v = lm;
+#pragma unroll
+    for (int k2 = 2; k2 <= 32; k2 <<= 1)
+#pragma unroll
+      for (int j2 = k2 >> 1; j2 > 0; j2 >>= 1) {
+        const uint32_t o = __shfl_xor_sync(FULL, v, j2);
+        const bool up = ((lane & k2) == 0), lower = ((lane & j2) == 0);
+        v = (lower == up) ? min(v, o) : max(v, o);
+      }
+    const uint32_t T = __shfl_sync(FULL, v, want - 1);
+    int cl = 0;
+#pragma unroll
+    for (int b = 0; b < D2; ++b) cl += key[b] <= T ? 1 : 0;
+    const int C = __reduce_add_sync(FULL, cl);
+    if (T != 0xffffffffu && C <= 64) {
+      int pos = cl;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, pos, o);
+        if (lane >= o) pos += t;
+      }
+      pos -= cl;
+#pragma unroll
+      for (int b = 0; b < D2; ++b)
+        if (key[b] <= T) {
+          bkey[pos] = key[b];
+          bidx[pos] = (uint32_t)(a + b * D2);
+          ++pos;
+        }
+      __syncwarp();
+      for (int q = lane; q < C; q += 32) {
+        const uint32_t kv = bkey[q], ix = bidx[q];
+        int rank = 0;
+        for (int t = 0; t < C; ++t) {
+          const uint32_t k2 = bkey[t], i2 = bidx[t];
+          rank += (k2 < kv || (k2 == kv && i2 < ix)) ? 1 : 0;
+        }
+        if (rank < want) lS[rank] = rank == 0 ? (uint32_t)(H + H * D2 + 1) : ix + 1;
+      }
+      ranked = true;
+    }
+  }
+  if (!index_order && !ranked) {
     // radix search for v* = the want-th smallest key (keys are >= +0 floats)
     uint32_t p = 0;
 #pragma unroll 1
@@ -131,9 +236,7 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
   }
 
   // ---- order the selection and write S ---------------------------------------
-  uint32_t* lkey = lst;
-  uint32_t* lidx = lst + 32;
-  uint32_t* lS = lst + 64;
+  if (!ranked) {
   int mine = __popc(selmask);
   int pos = mine;
 #pragma unroll
@@ -160,6 +263,7 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
       else rank += (k2 < kv || (k2 == kv && i2 < ix)) ? 1 : 0;
     }
     lS[rank] = rank == 0 ? ref_idx : ix + 1;
+  }
   }
   __syncwarp();
   uint32_t* Sg = A.S + (size_t)g * K;
@@ -199,7 +303,7 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
 
 size_t match_smem_bytes(int d, int d2) {
   const int wd = d + d2 - 1;
-  return (size_t)4 * wd * wd * sizeof(float) + 4 * 96 * sizeof(uint32_t);
+  return (size_t)4 * wd * wd * sizeof(float) + 4 * 224 * sizeof(uint32_t);
 }
 
 template <int D, int D2>

@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* b1 = sm + 3 * DD + warp * 2 * GSP;  // pilot group, later its Wiener gains
   float* b2 = b1 + GSP;                      // noisy group
+  float* wvs = sm + 3 * DD + 4 * 2 * GSP + warp * DD;  // this group's aggregation weights
   for (int t = threadIdx.x; t < DD; t += blockDim.x) {
     Tm[t] = A.T[t];
     Ti[t] = A.Ti[t];
@@ -191,9 +192,14 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   }
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, off);
-  if (lane == 0) {
-    const float nr = sqrtf(s);
-    A.n2[g] = nr * nr;
+  // weight = w / norm(col(filt))^2 (denoiseAndAggregateWieFast.m:81), one
+  // division per window position, shared by the K blocks of the group
+  const float nr = sqrtf(s), n2 = nr * nr;
+  if (lane == 0) A.n2[g] = n2;
+  for (int e = lane; e < DD; e += 32) {
+    const float wv = A.win[e] / n2;
+    wvs[e] = wv;
+    A.wt[(size_t)g * DD + e] = wv;
   }
   __syncwarp();
 
@@ -224,7 +230,7 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       for (int jj = 0; jj < D; ++jj) acc = fmaf(Ti[r + jj * D], p[jj], acc);
       float v = acc > 0.f ? acc : 0.f;
       if (A.clamp_one && v > 1.f) v = 1.f;
-      og[k * DD + r + l * D] = v;
+      og[k * DD + r + l * D] = wvs[r + l * D] * v;  // weight.*blocks(:,:,i) (:84-90)
     }
   }
 }
@@ -233,7 +239,7 @@ bool wiener_supported(int d, int K) { return (d == 4 || d == 8 || d == 16) && (K
 
 template <int D, int K>
 static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
-  const size_t sm = (size_t)(3 * D * D + 4 * 2 * D * (D + 1) * K) * sizeof(float);
+  const size_t sm = (size_t)(3 * D * D + 4 * 2 * D * (D + 1) * K + 4 * D * D) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wiener<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
