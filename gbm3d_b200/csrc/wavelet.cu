@@ -352,19 +352,29 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restr
   const int py0 = blockIdx.x * FSY, px0 = blockIdx.y * FSX, qz = blockIdx.z;
   const int qy0 = py0 >> 1, qx0 = px0 >> 1;
   const size_t bsz = (size_t)Iy * Ix * Iz, zoff = (size_t)Iy * Ix * qz;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int QT = (NQY + 31) / 32;  // coefficient rows per lane
 
-  for (int e = threadIdx.x; e < 8 * NQX * NQY; e += 256) {
-    const int qyl = e % NQY, r = e / NQY, qxl = r % NQX, code = r / NQX;
-    const int qy = wrap1(qy0 + qyl, Iy), qx = wrap1(qx0 + qxl, Ix);
-    const float* src = code ? bands + code * bsz : approx;
-    B[e] = __ldg(src + zoff + qy + (size_t)Iy * qx);
+  // stage 1: stage the 8 bands (warps over (code, qx) rows, lanes over qy)
+  int qyv[QT];
+#pragma unroll
+  for (int t = 0; t < QT; ++t) qyv[t] = wrap1(qy0 + lane + 32 * t, Iy);
+  for (int row = w; row < 8 * NQX; row += 8) {
+    const int code = row / NQX, qxl = row % NQX;
+    const float* src = (code ? bands + code * bsz : approx) + zoff + (size_t)Iy * wrap1(qx0 + qxl, Ix);
+    float* dst = B + row * NQY;
+#pragma unroll
+    for (int t = 0; t < QT; ++t) {
+      const int qyl = lane + 32 * t;
+      if (qyl < NQY) dst[qyl] = __ldg(src + qyv[t]);
+    }
   }
   __syncthreads();
-  // y-pass: rows py = 2t and 2t+1 from coefficients t + j
-  for (int e = threadIdx.x; e < 4 * NQX * (FSY / 2); e += 256) {
-    const int t = e % (FSY / 2), r = e / (FSY / 2), qxl = r % NQX, comb = r / NQX;
-    const float* bl = B + ((0 + 2 * comb) * NQX + qxl) * NQY + t;
-    const float* bh = B + ((1 + 2 * comb) * NQX + qxl) * NQY + t;
+  // y-pass: rows py = 2t and 2t+1 from coefficients t + j (warps over (comb, qx), lanes over t)
+  for (int row = w; row < 4 * NQX; row += 8) {
+    const int comb = row / NQX, qxl = row % NQX;
+    const float* bl = B + ((0 + 2 * comb) * NQX + qxl) * NQY + lane;
+    const float* bh = B + ((1 + 2 * comb) * NQX + qxl) * NQY + lane;
     float ev = 0.f, od = 0.f;
     // even output 2t: taps k even, coefficient t + k/2; odd output 2t+1: k odd, t + (k+1)/2
 #pragma unroll
@@ -378,14 +388,14 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restr
       if (k % 2 == 0) ev = fmaf(fb.shi[k], bh[k / 2], ev);
       else od = fmaf(fb.shi[k], bh[(k + 1) / 2], od);
     }
-    float* dst = Y + (comb * NQX + qxl) * FSY + 2 * t;
+    float* dst = Y + row * FSY + 2 * lane;
     dst[0] = ev;
     dst[1] = od;
   }
   __syncthreads();
   // x-pass: columns px = 2t and 2t+1 (lanes along py)
-  const int py = threadIdx.x % FSY, grp = threadIdx.x / FSY;  // 4 groups
-  for (int j = grp; j < 2 * (FSX / 2); j += 4) {
+  const int py = lane + 32 * (w & 1);
+  for (int j = w >> 1; j < FSX; j += 4) {
     const int t = j % (FSX / 2), fz = j / (FSX / 2);
     const float* yl = Y + ((0 + 2 * fz) * NQX + t) * FSY + py;
     const float* yh = Y + ((1 + 2 * fz) * NQX + t) * FSY + py;
@@ -407,18 +417,19 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restr
   }
   __syncthreads();
   // slot-axis pass: slot 2qz from tap 0, slot 2qz-1 from tap 1; write or accumulate
-  const int oz0 = pmod(2 * qz - o.shift, Oz), oz1 = pmod(2 * qz - 1 - o.shift, Oz);
   const int gy = py0 + py;
   if (gy < Oy) {
     const int oy = wrap1(gy - o.shift, Oy);
-    for (int px = grp; px < FSX; px += 4) {
-      if (px0 + px >= Ox) break;
+    float* r0 = o.out + oy + (size_t)Oy * Ox * pmod(2 * qz - o.shift, Oz);
+    float* r1 = o.out + oy + (size_t)Oy * Ox * pmod(2 * qz - 1 - o.shift, Oz);
+    const int pxe = min(FSX, Ox - px0);
+    for (int px = w >> 1; px < pxe; px += 4) {
       const float x0 = X[(0 * FSX + px) * FSY + py], x1 = X[(1 * FSX + px) * FSY + py];
       const float v0 = fmaf(fb.szh[0], x1, fmaf(fb.szl[0], x0, 0.f));
       const float v1 = fmaf(fb.szh[1], x1, fmaf(fb.szl[1], x0, 0.f));
-      const int ox = wrap1(px0 + px - o.shift, Ox);
-      float* d0 = o.out + oy + (size_t)Oy * (ox + (size_t)Ox * oz0);
-      float* d1 = o.out + oy + (size_t)Oy * (ox + (size_t)Ox * oz1);
+      const size_t col = (size_t)Oy * wrap1(px0 + px - o.shift, Ox);
+      float* d0 = r0 + col;
+      float* d1 = r1 + col;
       float a0 = o.first ? v0 : *d0 + v0;
       float a1 = o.first ? v1 : *d1 + v1;
       if (o.last) {
