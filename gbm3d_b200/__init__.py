@@ -11,10 +11,10 @@ from .options import (checkBM3Dopts, getTau, getWaveFilters3Dbior, myMirrorPadIm
                       resolve_opts, setBM3Dopts)
 from ._lib import Context, GBM3DError, context
 from .api import (GBM3D, GBM3D_device, MatchSet, denoiseAndAggregateGPU, denoiseAndAggregateWie,
-                  denoiseAndAggregateWieFast, matchBlocksCPU, matchBlocksWie)
+                  denoiseAndAggregateWieFast, matchBlocksCPU, matchBlocksGPU, matchBlocksWie)
 
 __all__ = [
-    "GBM3D", "GBM3D_device", "matchBlocksCPU", "denoiseAndAggregateGPU", "matchBlocksWie",
+    "GBM3D", "GBM3D_device", "matchBlocksCPU", "matchBlocksGPU", "denoiseAndAggregateGPU", "matchBlocksWie",
     "denoiseAndAggregateWieFast", "denoiseAndAggregateWie", "MatchSet", "Context", "context",
     "GBM3DError", "setBM3Dopts", "checkBM3Dopts", "resolve_opts", "getTau", "getWaveFilters3Dbior",
     "myMirrorPadImage", "myPSNR",

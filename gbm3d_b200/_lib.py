@@ -58,6 +58,7 @@ _SIGS = {
     "gbm3d_get_tau": (None, [C.c_int, C.c_int, _P]),
     "gbm3d_bior_filters": (None, [C.POINTER(gbm3d_filters)]),
     "gbm3d_matchBlocksCPU": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P, _P]),
+    "gbm3d_matchBlocksGPU": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoiseAndAggregateGPU": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, _P, C.POINTER(gbm3d_filters),
                                                C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_matchBlocksWie": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P, _P]),

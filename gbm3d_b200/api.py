@@ -6,6 +6,7 @@ C ABI.  Arrays follow MATLAB's column-major layout (numpy order='F'):
 
   U, out          = GBM3D(I, sigma, opts)                     source/GBM3D.m:1
   S, Volume       = matchBlocksCPU(I, sigma, opts)            source/matchBlocksCPU.m:1
+  S               = matchBlocksGPU(I, sigma, opts)            source/matchBlocksGPU.m:1
   U, W            = denoiseAndAggregateGPU(Volume, S, tau, Psi, Psi2, opts)
                                                               source/denoiseAndAggregateGPU.m:1
   S, V1, V2       = matchBlocksWie(I, In, sigma, opts)        source/matchBlocksWie.m:1
@@ -111,6 +112,23 @@ def matchBlocksCPU(I, sigma, opts: dict, ctx: Context | None = None):
     ctx.check(lib().gbm3d_matchBlocksCPU(ctx.h, _p(I), m, n, _sigma_scalar(sigma), C.byref(co),
                                          _p(S), _p(cnt), _p(V)))
     return _as_set(S, cnt), V
+
+
+def matchBlocksGPU(I, sigma, opts: dict, ctx: Context | None = None):
+    """S = matchBlocksGPU(I, sigma, opts): global circular search over the
+    whole image (indices into the m x n image, no slot-1 override), after the
+    sym4 prefilter when sigma > 30/255 (matchBlocksGPU.m:34)."""
+    ctx = ctx or context()
+    o = _opt.checkBM3Dopts(opts)
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n = I.shape
+    d, K = int(o["blockSize"]), int(o["numMax"])
+    M, N = m // d, n // d
+    S = np.zeros((K, M, N), dtype=np.uint32, order="F")
+    cnt = np.zeros((M, N), dtype=np.int32, order="F")
+    co = c_opts(o)
+    ctx.check(lib().gbm3d_matchBlocksGPU(ctx.h, _p(I), m, n, float(sigma), C.byref(co), _p(S), _p(cnt)))
+    return _as_set(S, cnt)
 
 
 def denoiseAndAggregateGPU(Volume, S, tau, Psi, Psi2, opts: dict, ctx: Context | None = None):

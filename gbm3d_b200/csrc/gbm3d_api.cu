@@ -746,6 +746,53 @@ int gbm3d_matchBlocksCPU(gbm3d_ctx* c, const double* I, int m, int n, double sig
   });
 }
 
+int gbm3d_matchBlocksGPU(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
+                         uint32_t* S, int32_t* S_count) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    const int d = o->blockSize, K = o->numMax;
+    if (!global_match_supported(d, K))
+      argfail(c, "unsupported blockSize for the global matcher", GBM3D_ERR_UNSUPPORTED);
+    if (!I || !S) argfail(c, "I and S are required");
+    if (m < d || n < d || m < 16 || n < 16) argfail(c, "image too small for the global matcher");
+    if ((sigma > 30.0 / 255.0) && (m % 8 || n % 8))
+      argfail(c, "the sym4 prefilter needs image sides divisible by 8");
+    const int M = m / d, N = n / d;
+    const size_t px = (size_t)m * n;
+    double* dI = buf<double>(c, "io.I", px);
+    ck(c, cudaMemcpyAsync(dI, I, px * sizeof(double), cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    float* If = buf<float>(c, "io.If", px);
+    k_prep<<<grid2(m, n), 256, 0, c->st>>>(dI, m, n, If, m, n, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+    if (sigma > 30.0 / 255.0) {  // matchBlocksGPU.m:34
+      float* work = buf<float>(c, "gm.work", px * 8);
+      ck(c, launch_sym4_prefilter(If, m, n, (float)(2 * sigma), work, c->st), "sym4 prefilter");
+    }
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    int32_t* dc = buf<int32_t>(c, "io.cnt", (size_t)M * N);
+    GlobalMatchArgs A{};
+    A.I = If;
+    A.m = m;
+    A.n = n;
+    A.M = M;
+    A.N = N;
+    A.K = K;
+    A.numMin = o->numMin;
+    A.tol = (float)(0.005 * sigma * sigma * d * d);
+    A.tol_branch = o->numMin != K;
+    A.S = dS;
+    A.cnt = dc;
+    launched(c, launch_match_global(d, A, c->st), "match_global");
+    ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (S_count) ck(c, cudaMemcpyAsync(S_count, dc, (size_t)M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+  });
+}
+
 int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* c, const float* Volume, const uint32_t* S, const int32_t* S_count,
                                  int M, int N, const double* tau, const gbm3d_filters* f, const gbm3d_opts* o,
                                  double* U, double* W) {

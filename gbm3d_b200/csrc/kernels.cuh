@@ -94,4 +94,18 @@ struct AggArgs {
 };
 cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st);
 
+// ---- global matching (global_match.cu) ----------------------------------------------
+struct GlobalMatchArgs {
+  const float* I;  // m x n single image (prefiltered when sigma > 30/255)
+  int m, n, M, N, K, numMin;
+  float tol;
+  int tol_branch;
+  uint32_t* S;    // K x M x N, 1-based positions in the m x n image
+  int32_t* cnt;   // M x N (may be null)
+};
+bool global_match_supported(int d, int K);
+cudaError_t launch_match_global(int d, const GlobalMatchArgs& A, cudaStream_t st);
+// in-place sym4 prefilter; work holds 8 * m * n floats
+cudaError_t launch_sym4_prefilter(float* I, int m, int n, float tau, float* work, cudaStream_t st);
+
 }  // namespace gbm3d

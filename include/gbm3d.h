@@ -97,6 +97,15 @@ void gbm3d_bior_filters(gbm3d_filters* out);
 int gbm3d_matchBlocksCPU(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
                          const gbm3d_opts* opts, uint32_t* S, int32_t* S_count, float* Volume);
 
+/* S = matchBlocksGPU(I,sigma,opts)                       source/matchBlocksGPU.m:1-91
+ * Global circular search: every block position of the m x n image is a
+ * candidate; S (K x M x N) holds 1-based positions in the image, with no
+ * slot-1 override.  When sigma > 30/255 the image is first prefiltered by the
+ * reference's 5-shift, 3-level sym4 wavelet hard threshold (tau = 2 sigma),
+ * which needs m and n divisible by 8.  Work grows as (m n)^2: small images. */
+int gbm3d_matchBlocksGPU(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
+                         const gbm3d_opts* opts, uint32_t* S, int32_t* S_count);
+
 /* [U,W] = denoiseAndAggregateGPU(Volume,S,tau,Psi,Psi2,opts)   source/denoiseAndAggregateGPU.m:1-92
  * Volume: (M*d) x (N*d) x K single; S: K x M x N; S_count may be NULL;
  * tau: levels x 7 double; filters: the separable factors of Psi/Psi2.

@@ -274,3 +274,76 @@ def gbm3d(I, sigma, opts, Psi, Psi2, tau_unit):
         Ws[..., ii] = _circshift(w, (-s, -s))
     U = Us.sum(axis=2) / Ws.sum(axis=2)
     return U[:m, :n], U1[:m, :n]
+
+
+SYM4_LO = np.array([-0.07576571478927333, -0.02963552764599851, 0.49761866763201545, 0.8037387518059161,
+                    0.29785779560527736, -0.09921954357684722, -0.012603967262037833, 0.0322231006040427])
+SYM4_HI = np.array([-0.0322231006040427, -0.012603967262037833, 0.09921954357684722, 0.29785779560527736,
+                    -0.8037387518059161, 0.49761866763201545, 0.02963552764599851, -0.07576571478927333])
+
+
+def sym4_bank():
+    """getWaveFilters2D('sym',4): Psi(:,:,1..4) = Lo'Lo, Hi'Lo, Lo'Hi, Hi'Hi."""
+    lo, hi = SYM4_LO, SYM4_HI
+    return np.stack([np.outer(lo, lo), np.outer(hi, lo), np.outer(lo, hi), np.outer(hi, hi)], -1)
+
+
+def wav_dec2(Psi, levels, U):
+    """myWavDec2DFFT.m:10-23."""
+    C = {}
+    for i in range(levels):
+        FU = np.fft.fft2(U)
+        for j in range(3):
+            C[i, j] = np.real(np.fft.ifft2(FU * np.fft.fft2(_pad_to(Psi[..., j + 1], U.shape))))[::2, ::2]
+        U = np.real(np.fft.ifft2(FU * np.fft.fft2(_pad_to(Psi[..., 0], U.shape))))[::2, ::2]
+    C[levels, 0] = U
+    return C
+
+
+def wav_rec2(Psi, levels, C):
+    """myWavRec2DGPUfast.m:10-34."""
+    Cup = {}
+    for i in range(levels):
+        sh = tuple(2 * s for s in C[i, 0].shape)
+        acc = np.zeros(sh)
+        for j in range(3):
+            tmp = np.zeros(sh)
+            tmp[::2, ::2] = C[i, j]
+            acc += np.real(np.fft.ifft2(np.fft.fft2(tmp) * np.conj(np.fft.fft2(_pad_to(Psi[..., j + 1], sh)))))
+        Cup[i] = acc
+    Cup[levels] = C[levels, 0]
+    for i in range(levels, 0, -1):
+        sh = Cup[i - 1].shape
+        tmp = np.zeros(sh)
+        tmp[::2, ::2] = Cup[i]
+        Cup[i - 1] = Cup[i - 1] + np.real(np.fft.ifft2(np.fft.fft2(tmp) * np.conj(np.fft.fft2(_pad_to(Psi[..., 0], sh)))))
+    return Cup[0]
+
+
+def match_blocks_global(I, sigma, d, K):
+    """matchBlocksGPU.m:19-91 (top-K branch); returns S (K, M, N) and the searched image."""
+    I = np.asarray(I, dtype=np.float64)
+    m, n = I.shape
+    M, N = m // d, n // d
+    if sigma > 30 / 255:
+        Psi = sym4_bank()
+        avg = np.zeros_like(I)
+        for k in range(1, 6):
+            C = wav_dec2(Psi, 3, _circshift(I, (k - 1, k - 1)))
+            for i in range(3):
+                for j in range(3):
+                    C[i, j] = C[i, j] * (np.abs(C[i, j]) > 2 * sigma)
+            avg = avg + _circshift(wav_rec2(Psi, 3, C), (1 - k, 1 - k)) / 5
+        I = avg
+    g = _pad_to(np.ones((d, d)), (m, n))
+    bn = np.real(_circshift(np.fft.ifft2(np.fft.fft2(g) * np.fft.fft2(I ** 2)), (-d + 1, -d + 1)))
+    FI = np.fft.fft2(I)
+    S = np.zeros((K, M, N), dtype=np.uint32)
+    for i in range(M):
+        for j in range(N):
+            xR = I[i * d:(i + 1) * d, j * d:(j + 1) * d]
+            cc = np.real(np.fft.ifft2(np.conj(np.fft.fft2(_pad_to(xR, (m, n)))) * FI))
+            nr = bn[i * d, j * d]
+            D = (nr + bn - 2 * cc) / nr
+            S[:, i, j] = np.argsort(D.ravel(order="F"), kind="stable")[:K] + 1
+    return S, I

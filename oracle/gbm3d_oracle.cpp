@@ -802,6 +802,135 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Global matcher — matchBlocksGPU.m:19-91 (A12)
+// ---------------------------------------------------------------------------
+
+// Symlet-4 decomposition filters (published values; Lo_d / Hi_d of the sym4
+// bank that getWaveFilters2D('sym',4) loads, matchBlocksGPU.m:36).
+const double kSym4Lo[8] = {-0.07576571478927333, -0.02963552764599851, 0.49761866763201545, 0.8037387518059161,
+                           0.29785779560527736, -0.09921954357684722, -0.012603967262037833, 0.0322231006040427};
+const double kSym4Hi[8] = {-0.0322231006040427, -0.012603967262037833, 0.09921954357684722, 0.29785779560527736,
+                           -0.8037387518059161, 0.49761866763201545, 0.02963552764599851, -0.07576571478927333};
+
+// One 2D hard-threshold denoise: myWavDec2DFFT (x-pass then y-pass per level),
+// threshold |C| > tau on the three detail bands, myWavRec2DGPUfast (y-pass
+// then x-pass per level; synthesis with the same filters, by correlation).
+template <class T>
+void wavelet2d_ht(std::vector<T>& U, int Ly, int Lx, int levels, T tau) {
+  Bank1D<T> b = make_bank<T>(8, kSym4Lo, kSym4Hi, kSym4Lo, kSym4Hi);
+  std::vector<std::vector<T>> C(levels * 4);
+  std::vector<int> dims(levels * 2);
+  std::vector<T> A = U, tx[2];
+  int y = Ly, x = Lx;
+  for (int lv = 0; lv < levels; ++lv) {
+    dims[lv * 2] = y; dims[lv * 2 + 1] = x;
+    for (int fx = 0; fx < 2; ++fx) {
+      analysis_axis(A, y, x, 1, 1, b.a[fx], tx[fx]);
+      for (int fy = 0; fy < 2; ++fy) {
+        int code = fy + 2 * fx;
+        auto& out = C[lv * 4 + code];
+        analysis_axis(tx[fx], y, x / 2, 1, 0, b.a[fy], out);
+        if (code)
+          for (auto& v : out) v = v * (T)(std::fabs(v) > tau ? 1 : 0);
+      }
+    }
+    A = C[lv * 4];
+    y /= 2; x /= 2;
+  }
+  std::vector<T> R = C[(levels - 1) * 4];
+  for (int lv = levels - 1; lv >= 0; --lv) {
+    int oy = dims[lv * 2], ox = dims[lv * 2 + 1], iy = oy / 2, ix = ox / 2;
+    auto band = [&](int code) -> const std::vector<T>& { return code ? C[lv * 4 + code] : R; };
+    std::vector<T> Y[2], out;
+    for (int fx = 0; fx < 2; ++fx) synthesis_axis(band(0 + 2 * fx), band(1 + 2 * fx), iy, ix, 1, 0, b, Y[fx]);
+    synthesis_axis(Y[0], Y[1], oy, ix, 1, 1, b, out);
+    R.swap(out);
+  }
+  U.swap(R);
+}
+
+// matchBlocksGPU.m:34-50: average of 5 shifted hard-threshold denoises.
+template <class T>
+void sym4_prefilter(std::vector<T>& I, int m, int n, double sigma) {
+  const T tau = (T)(2 * sigma);
+  std::vector<T> avg(I.size(), T(0)), sh(I.size());
+  const T five = (T)5;
+  for (int k = 0; k < 5; ++k) {
+    for (int c = 0; c < n; ++c)
+      for (int r = 0; r < m; ++r) sh[r + (size_t)c * m] = I[pmod(r - k, m) + (size_t)pmod(c - k, n) * m];
+    wavelet2d_ht(sh, m, n, 3, tau);
+    for (int c = 0; c < n; ++c)
+      for (int r = 0; r < m; ++r) {
+        size_t o = r + (size_t)c * m;
+        avg[o] = avg[o] + sh[pmod(r + k, m) + (size_t)pmod(c + k, n) * m] / five;
+      }
+  }
+  I.swap(avg);
+}
+
+// Search over every circular block position of the image: distances are exact
+// SSDs (row-major, fma(t,t,acc)) ranked with mink's stable order; indices are
+// 1-based linear positions in the m x n image; no slot-1 override.
+template <class T>
+void match_global(const std::vector<T>& I, int m, int n, int d, int K, int numMin, double tol, bool tol_branch,
+                  uint32_t* S, int32_t* cnt) {
+  const int M = m / d, N = n / d;
+  const size_t P = (size_t)m * n;
+#pragma omp parallel
+  {
+    std::vector<T> ssd(P);
+    std::vector<std::pair<T, int>> keys(P);
+#pragma omp for schedule(dynamic) collapse(2)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < M; ++i) {
+        std::fill(ssd.begin(), ssd.end(), T(0));
+        for (int r = 0; r < d; ++r)
+          for (int c = 0; c < d; ++c) {
+            const T xv = I[(i * d + r) + (size_t)(j * d + c) * m];
+            for (int pc = 0; pc < n; ++pc) {
+              const T* col = &I[(size_t)((pc + c) % n) * m];
+              T* acc = &ssd[(size_t)pc * m];
+              for (int pr = 0; pr < m; ++pr) {
+                T t = xv - col[(pr + r) % m];
+                acc[pr] = fmaT(t, t, acc[pr]);
+              }
+            }
+          }
+        for (size_t e = 0; e < P; ++e) keys[e] = {ssd[e], (int)e};
+        auto less = [](const std::pair<T, int>& x, const std::pair<T, int>& y) {
+          return x.first < y.first || (x.first == y.first && x.second < y.second);
+        };
+        std::vector<int> sel;
+        if (!tol_branch) {
+          std::partial_sort(keys.begin(), keys.begin() + K, keys.end(), less);
+          for (int k = 0; k < K; ++k) sel.push_back(keys[k].second);
+        } else {
+          T nR = T(0);
+          for (int c = 0; c < d; ++c)
+            for (int r = 0; r < d; ++r) {
+              const T xv = I[(i * d + r) + (size_t)(j * d + c) * m];
+              nR = fmaT(xv, xv, nR);
+            }
+          for (size_t e = 0; e < P; ++e)
+            if (ssd[e] / nR < (T)tol) sel.push_back((int)e);
+          int want = -1;
+          if ((int)sel.size() > K) want = K;
+          else if ((int)sel.size() < numMin) want = numMin;
+          if (want > 0) {
+            std::partial_sort(keys.begin(), keys.begin() + want, keys.end(), less);
+            sel.clear();
+            for (int k = 0; k < want; ++k) sel.push_back(keys[k].second);
+          }
+        }
+        const int g = i + M * j;
+        for (int k = 0; k < K; ++k) S[(size_t)g * K + k] = k < (int)sel.size() ? (uint32_t)(sel[k] + 1) : 0u;
+        if (cnt) cnt[g] = (int)sel.size();
+      }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -904,6 +1033,26 @@ int orc_wavelet_roundtrip(int prec, const void* V, int Ly, int Lx, int Lz, int l
     std::vector<double> v((const double*)V, (const double*)V + nv);
     wavelet_ht(v, Ly, Lx, Lz, levels, tau, bxy, bz);
     std::memcpy(out, v.data(), nv * sizeof(double));
+  }
+  return 0;
+}
+
+// S = matchBlocksGPU(I,sigma,opts); prefiltered (may be null) receives the
+// image the search ran on.
+int orc_match_blocks_global(int prec, const double* I, int m, int n, double sigma, int d, int numMax,
+                            int numMin, uint32_t* S, int32_t* cnt, double* prefiltered) {
+  const double tol = 0.005 * sigma * sigma * d * d;
+  const size_t px = (size_t)m * n;
+  if (prec == 32) {
+    auto It = to_T<float>(I, px);
+    if (sigma > 30.0 / 255.0) sym4_prefilter<float>(It, m, n, sigma);
+    if (prefiltered) for (size_t i = 0; i < px; ++i) prefiltered[i] = It[i];
+    match_global<float>(It, m, n, d, numMax, numMin, tol, numMax != numMin, S, cnt);
+  } else {
+    std::vector<double> It(I, I + px);
+    if (sigma > 30.0 / 255.0) sym4_prefilter<double>(It, m, n, sigma);
+    if (prefiltered) for (size_t i = 0; i < px; ++i) prefiltered[i] = It[i];
+    match_global<double>(It, m, n, d, numMax, numMin, tol, numMax != numMin, S, cnt);
   }
   return 0;
 }

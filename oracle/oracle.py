@@ -240,3 +240,18 @@ def GBM3D(I, sigma, opts, prec=32):
     oc = make_opts(opts)
     lib().orc_gbm3d(prec, _p(I), m, n, C.c_double(sigma), C.byref(oc), _p(U), _p(U1))
     return U, U1
+
+
+def matchBlocksGPU(I, sigma, opts, prec=32):
+    """S = matchBlocksGPU(I, sigma, opts) (source/matchBlocksGPU.m:1): global
+    circular search; S indexes the m x n image.  Returns S, counts and the
+    (prefiltered) image the search ran on."""
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n = I.shape
+    d, K = opts["blockSize"], opts["numMax"]
+    M, N = m // d, n // d
+    S = np.zeros((K, M, N), dtype=np.uint32, order="F")
+    cnt = np.zeros((M, N), dtype=np.int32, order="F")
+    pre = np.zeros((m, n), order="F")
+    lib().orc_match_blocks_global(prec, _p(I), m, n, C.c_double(sigma), d, K, opts["numMin"], _p(S), _p(cnt), _p(pre))
+    return S, cnt, pre

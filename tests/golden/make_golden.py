@@ -68,6 +68,27 @@ def make(name, m, n, sigma, seed, profile, wav):
     print(name, {k: getattr(v, "shape", v) for k, v in out.items() if k not in ("profile", "wavelet")})
 
 
+def make_global(name, m, n, sigma, seed):
+    """matchBlocksGPU (global search, sym4 prefilter when sigma > 30/255)."""
+    _, noisy = synth.noisy_image(m, n, sigma, seed=seed)
+    S, pre = F.match_blocks_global(noisy, sigma, 16, 16)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), noisy=noisy, sigma=sigma, S=S, prefiltered=pre)
+    print(name, S.shape)
+
+
+def check_sym4_data():
+    """The restated sym4 coefficients equal the reference's filter data file."""
+    p = "/root/reference/archive/waveletFilters/sym4Filters.mat"
+    if os.path.exists(p):
+        import scipy.io as sio
+        d = sio.loadmat(p)
+        assert np.array_equal(np.ravel(d["Lo_d"]), F.SYM4_LO) and np.array_equal(np.ravel(d["Hi_d"]), F.SYM4_HI)
+        print("sym4 coefficients match", p)
+
+
 if __name__ == "__main__":
     for c in CASES:
         make(*c)
+    make_global("global_64x64_s25", 64, 64, 25.0, 21)
+    make_global("global_48x64_s01", 48, 64, 0.1, 22)
+    check_sym4_data()

@@ -181,3 +181,22 @@ def test_deterministic(gpu):
     U1, _ = gpu.GBM3D(noisy, 25.0)
     U2, _ = gpu.GBM3D(noisy, 25.0)
     assert np.array_equal(U1, U2)
+
+
+@pytest.mark.parametrize("m,n,sigma,seed,d", [(64, 64, 25.0, 21, 16), (48, 64, 0.1, 22, 16), (64, 96, 10.0, 23, 8)])
+def test_matchBlocksGPU_global(gpu, oracle, m, n, sigma, seed, d):
+    _, noisy = synth.noisy_image(m, n, sigma, seed=seed)
+    o = _opts(blockSize=d)
+    S = gpu.matchBlocksGPU(noisy, sigma, o)
+    So, co, _ = oracle.matchBlocksGPU(noisy, sigma, o, prec=32)
+    assert np.array_equal(np.asarray(S), So), f"{int((np.asarray(S) != So).sum())} entries differ"
+    assert np.array_equal(S.count, co)
+
+
+def test_matchBlocksGPU_tolerance_branch(gpu, oracle):
+    _, noisy = synth.noisy_image(64, 64, 0.1, seed=24)
+    o = _opts(numMin=2, numMax=16)
+    S = gpu.matchBlocksGPU(noisy, 0.1, o)
+    So, co, _ = oracle.matchBlocksGPU(noisy, 0.1, o, prec=32)
+    assert np.array_equal(S.count, co)
+    assert np.array_equal(np.asarray(S), So)

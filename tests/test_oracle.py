@@ -14,7 +14,8 @@ import pytest
 from conftest import max_abs
 from gbm3d_b200 import options, synth
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
+                if not os.path.basename(p).startswith("global"))
 FP64_TOL = 1e-9  # relative, FFT route vs direct arithmetic, both float64
 
 
@@ -152,3 +153,13 @@ def test_tolerance_branch(oracle):
     for i in range(S.shape[1]):
         for j in range(S.shape[2]):
             assert np.all(S[cnt[i, j]:, i, j] == 0)
+
+
+@pytest.mark.parametrize("name", ["global_64x64_s25", "global_48x64_s01"])
+def test_oracle_global_matcher_matches_golden(oracle, name):
+    """matchBlocksGPU: global search with the sym4 prefilter (sigma > 30/255) or without."""
+    g = _load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    opts = options.resolve_opts({"profile": "default"})
+    S, cnt, pre = oracle.matchBlocksGPU(g["noisy"], float(g["sigma"]), opts, prec=64)
+    assert max_abs(pre, g["prefiltered"]) < 1e-9
+    assert np.array_equal(S, g["S"])
