@@ -279,7 +279,7 @@ void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
   if (o->matchSize < 2 || (o->matchSize & 1)) argfail(c, "matchSize must be even");
   if (o->refStride != 0 && o->refStride != o->blockSize)
     argfail(c, "refStride other than blockSize is not supported yet", GBM3D_ERR_UNSUPPORTED);
-  if (o->filtType != 0) argfail(c, "filtType 'median' is not supported", GBM3D_ERR_UNSUPPORTED);
+  if (o->filtType != 0 && o->filtType != 1) argfail(c, "unrecognized filtering");  // denoiseAndAggregateGPU.m:54
 }
 
 void check_match(gbm3d_ctx* c, int d, int d2, int K) {
@@ -346,8 +346,13 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
 // denoiseAndAggregateGPU on device buffers; U, W are float (M d) x (N d).
 void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cnt, int M, int N, int d,
             int d2, int K, int levels, int cycleSpin, const double* tau, const WaveletBank& bk, float* U,
-            float* W) {
+            float* W, int filtType) {
   const int m = M * d, n = N * d;
+  float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
+  if (filtType == 1) {  // medfilt3 instead of the wavelet (denoiseAndAggregateGPU.m:165-168)
+    StageTimer tw(c, 2);
+    launched(c, launch_medfilt3(vol, m, n, K, vsum, c->st), "medfilt3");
+  } else {
   const int q = 1 << levels;
   if (levels < 1 || levels > GBM3D_MAX_LEVELS) argfail(c, "levels out of range");
   if (m % q || n % q || K % q)
@@ -359,7 +364,6 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
     coef[lv] = buf<float>(c, ("ht.coef" + std::to_string(lv)).c_str(), insz);  // 8 bands = input size
     if (lv > 0) rec[lv] = buf<float>(c, ("ht.rec" + std::to_string(lv)).c_str(), insz);
   }
-  float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
   std::vector<LevelBands> th(levels);
   for (int lv = 0; lv < levels; ++lv) {
     th[lv].tau[0] = 0.f;
@@ -391,6 +395,7 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
       }
       launched(c, launch_wav_synthesis(coef[lv], approx, m >> lv, n >> lv, K >> lv, o, bk, c->st), "wav_synthesis");
     }
+  }
   }
   }
   StageTimer tagg(c, 3);
@@ -543,7 +548,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
       StageTimer t(c, 1);
       run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1");
     }
-    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws);
+    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType);
     k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
     launched(c, cudaGetLastError(), "accum");
     k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa, ii == 0);
@@ -818,7 +823,7 @@ int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* c, const float* Volume, const uint32
     }
     float* dU = buf<float>(c, "io.U", px);
     float* dW = buf<float>(c, "io.W", px);
-    run_ht(c, dV, dS, dc, M, N, d, d2, K, o->levels, o->cycleSpin, tau, bk, dU, dW);
+    run_ht(c, dV, dS, dc, M, N, d, d2, K, o->levels, o->cycleSpin, tau, bk, dU, dW, o->filtType);
     to_host_double(c, dU, px, U);
     ck(c, cudaStreamSynchronize(c->st), "sync");
     to_host_double(c, dW, px, W);

@@ -52,6 +52,8 @@ struct SynthOut {
 };
 cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy, int Ox, int Oz,
                                  const SynthOut& o, const WaveletBank& bk, cudaStream_t st);
+// medfilt3 of the volume (filtType 'median').
+cudaError_t launch_medfilt3(const float* V, int m, int n, int K, float* out, cudaStream_t st);
 // Aggregation weight 1/(TV(group)+eps) per group of the image-shaped Vavg.
 cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int d, int K,
                               const int32_t* cnt, float* wgt, cudaStream_t st);

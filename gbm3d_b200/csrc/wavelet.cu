@@ -557,6 +557,45 @@ __global__ void __launch_bounds__(128) k_ht_weights_t(const float* __restrict__ 
   }
 }
 
+// medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:165-168) with 'symmetric'
+// padding, which for a one-voxel border repeats the edge voxel.  The median
+// of 27 values is a selection, exact in any order: an odd-even transposition
+// sort in registers.
+__global__ void __launch_bounds__(256) k_medfilt3(const float* __restrict__ V, int m, int n, int K,
+                                                  float* __restrict__ out) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (idx >= (size_t)m * n * K) return;
+  const int y = (int)(idx % m);
+  const size_t r1 = idx / m;
+  const int x = (int)(r1 % n), z = (int)(r1 / n);
+  float v[27];
+  int q = 0;
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int yy = min(max(y + dy, 0), m - 1), xx = min(max(x + dx, 0), n - 1), zz = min(max(z + dz, 0), K - 1);
+        v[q++] = __ldg(V + yy + (size_t)m * (xx + (size_t)n * zz));
+      }
+#pragma unroll
+  for (int pass = 0; pass < 27; ++pass)
+#pragma unroll
+    for (int i = pass & 1; i + 1 < 27; i += 2) {
+      const float a = fminf(v[i], v[i + 1]), b = fmaxf(v[i], v[i + 1]);
+      v[i] = a;
+      v[i + 1] = b;
+    }
+  out[idx] = v[13];
+}
+
+cudaError_t launch_medfilt3(const float* V, int m, int n, int K, float* out, cudaStream_t st) {
+  const size_t N = (size_t)m * n * K;
+  k_medfilt3<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(V, m, n, K, out);
+  return cudaGetLastError();
+}
+
 static size_t analysis_smem(int reach) {
   const int NY = 2 * TQ + reach;
   return (size_t)(2 * NY * NY + 4 * TQ * NY) * sizeof(float);

@@ -139,6 +139,7 @@ typedef struct {
   int nSpins, spins[8];
   int nSpinsWie, spinsWie[8];
   int staleWeights;  // GBM3D.m:26-27,82 slice-reuse behaviour (1 = mirror it)
+  int filtType;      // 0 'ht', 1 'median' (denoiseAndAggregateGPU.m:135,165)
 } orc_opts;
 
 }  // extern "C"
@@ -450,6 +451,10 @@ void aggregate(int M, int N, int d, int d2, int K, const uint32_t* S, const int3
     }
 }
 
+template <class T>
+void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, const uint32_t* S,
+                  const int32_t* cnt, double* U, double* W);
+
 // denoiseAndAggregateGPU.m:11-92 (filtType 'ht')
 template <class T>
 void denoise_ht(const T* Volume, int M, int N, int d, int d2, int K, const uint32_t* S,
@@ -486,6 +491,45 @@ void denoise_ht(const T* Volume, int M, int N, int d, int d2, int K, const uint3
     T v = sum[o] / cs;
     sum[o] = v > T(0) ? v : T(0);
   }
+  ht_aggregate<T>(sum, M, N, d, d2, K, S, cnt, U, W);
+}
+
+// medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:165-168), 'symmetric'
+// padding (for a one-voxel border: the edge voxel repeated).
+template <class T>
+void median3(const T* V, int m, int n, int K, std::vector<T>& out) {
+  out.assign((size_t)m * n * K, T(0));
+#pragma omp parallel for collapse(2)
+  for (int z = 0; z < K; ++z)
+    for (int x = 0; x < n; ++x)
+      for (int y = 0; y < m; ++y) {
+        T v[27];
+        int q = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy) {
+              int yy = std::min(std::max(y + dy, 0), m - 1), xx = std::min(std::max(x + dx, 0), n - 1),
+                  zz = std::min(std::max(z + dz, 0), K - 1);
+              v[q++] = V[yy + (size_t)m * (xx + (size_t)n * zz)];
+            }
+        std::nth_element(v, v + 13, v + 27);
+        out[y + (size_t)m * (x + (size_t)n * z)] = v[13];
+      }
+}
+
+template <class T>
+void denoise_median(const T* Volume, int M, int N, int d, int d2, int K, const uint32_t* S, const int32_t* cnt,
+                    double* U, double* W) {
+  std::vector<T> vavg;
+  median3<T>(Volume, M * d, N * d, K, vavg);
+  ht_aggregate<T>(vavg, M, N, d, d2, K, S, cnt, U, W);
+}
+
+// Aggregation of denoiseAndAggregateGPU.m:174-208 from the filtered volume.
+template <class T>
+void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, const uint32_t* S,
+                  const int32_t* cnt, double* U, double* W) {
+  const int m = M * d, n = N * d;
   const int G = M * N;
   std::vector<T> wg(G);
 #pragma omp parallel for
@@ -749,8 +793,11 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
     std::vector<T> Vol(px * K);
     MatchOut<T> mo{S.data(), cnt.data(), Vol.data(), nullptr, nullptr};
     match_blocks<T>(It.data(), nullptr, Mp, Np, d, d2, K, o->numMin, tol, o->numMax != o->numMin, mo);
-    denoise_ht<T>(Vol.data(), M, N, d, d2, K, S.data(), cnt.data(), o->levels, o->cycleSpin,
-                  tau.data(), &f, u.data(), w.data());
+    if (o->filtType == 1)
+      denoise_median<T>(Vol.data(), M, N, d, d2, K, S.data(), cnt.data(), u.data(), w.data());
+    else
+      denoise_ht<T>(Vol.data(), M, N, d, d2, K, S.data(), cnt.data(), o->levels, o->cycleSpin,
+                    tau.data(), &f, u.data(), w.data());
     circshift2(u.data(), Mp, Np, -s, &U1s[ii * px]);
     circshift2(w.data(), Mp, Np, -s, &Ws[ii * px]);
   }
@@ -1013,6 +1060,29 @@ int orc_denoise_wiener(int prec, const void* V1, const void* V2, int M, int N, i
   else
     denoise_wiener<double>((const double*)V1, (const double*)V2, M, N, d, d2, K, S, sigma,
                            sigma_is_matrix, variant, U, W);
+  return 0;
+}
+
+// [U,W] = denoiseAndAggregateGPU(Volume,S,tau,Psi,Psi2,opts) with filtType 'median'
+int orc_denoise_median(int prec, const void* Volume, int M, int N, int d, int d2, int K, const uint32_t* S,
+                       const int32_t* cnt, double* U, double* W) {
+  if (prec == 32) denoise_median<float>((const float*)Volume, M, N, d, d2, K, S, cnt, U, W);
+  else denoise_median<double>((const double*)Volume, M, N, d, d2, K, S, cnt, U, W);
+  return 0;
+}
+
+// medfilt3(V,[3 3 3]) alone, for unit tests.
+int orc_medfilt3(int prec, const void* V, int m, int n, int K, void* out) {
+  const size_t N = (size_t)m * n * K;
+  if (prec == 32) {
+    std::vector<float> o;
+    median3<float>((const float*)V, m, n, K, o);
+    std::memcpy(out, o.data(), N * sizeof(float));
+  } else {
+    std::vector<double> o;
+    median3<double>((const double*)V, m, n, K, o);
+    std::memcpy(out, o.data(), N * sizeof(double));
+  }
   return 0;
 }
 

@@ -51,7 +51,7 @@ class orc_opts(C.Structure):
         ("levels", C.c_int), ("cycleSpin", C.c_int), ("tauMode", C.c_int), ("Wiener", C.c_int),
         ("nSpins", C.c_int), ("spins", C.c_int * 8),
         ("nSpinsWie", C.c_int), ("spinsWie", C.c_int * 8),
-        ("staleWeights", C.c_int),
+        ("staleWeights", C.c_int), ("filtType", C.c_int),
     ]
 
 
@@ -229,6 +229,7 @@ def make_opts(o: dict) -> orc_opts:
     c.nSpinsWie = len(o["matchSpinsWie"])
     c.spinsWie[: c.nSpinsWie] = [int(s) for s in o["matchSpinsWie"]]
     c.staleWeights = 1 if o.get("staleWeights", True) else 0
+    c.filtType = 1 if o.get("filtType", "ht") == "median" else 0
     return c
 
 
@@ -255,3 +256,29 @@ def matchBlocksGPU(I, sigma, opts, prec=32):
     pre = np.zeros((m, n), order="F")
     lib().orc_match_blocks_global(prec, _p(I), m, n, C.c_double(sigma), d, K, opts["numMin"], _p(S), _p(cnt), _p(pre))
     return S, cnt, pre
+
+
+def denoiseAndAggregateMedian(Volume, S, opts, cnt=None, prec=32):
+    """denoiseAndAggregateGPU with opts.filtType = 'median' (medfilt3 instead of the wavelet)."""
+    dt = np.float32 if prec == 32 else np.float64
+    Volume = np.asfortranarray(Volume, dtype=dt)
+    K, M, N = S.shape
+    d = opts["blockSize"]
+    S = np.asfortranarray(S, dtype=np.uint32)
+    U = np.zeros((M * d, N * d), order="F")
+    W = np.zeros_like(U)
+    cp = None
+    if cnt is not None:
+        cnt = np.asfortranarray(cnt, dtype=np.int32)
+        cp = _p(cnt)
+    lib().orc_denoise_median(prec, _p(Volume), M, N, d, opts["matchSize"], K, _p(S), cp, _p(U), _p(W))
+    return U, W
+
+
+def medfilt3(V, prec=64):
+    dt = np.float32 if prec == 32 else np.float64
+    V = np.asfortranarray(V, dtype=dt)
+    out = np.zeros_like(V)
+    m, n, K = V.shape
+    lib().orc_medfilt3(prec, _p(V), m, n, K, _p(out))
+    return out

@@ -200,3 +200,22 @@ def test_matchBlocksGPU_tolerance_branch(gpu, oracle):
     So, co, _ = oracle.matchBlocksGPU(noisy, 0.1, o, prec=32)
     assert np.array_equal(S.count, co)
     assert np.array_equal(np.asarray(S), So)
+
+
+def test_denoiseAndAggregateGPU_median(gpu, oracle):
+    """filtType 'median': medfilt3 of the volume replaces the wavelet (denoiseAndAggregateGPU.m:165-168)."""
+    _, noisy = synth.noisy_image(64, 96, 25.0, seed=31)
+    o = _opts(filtType="median")
+    So, Vo, co = oracle.matchBlocksCPU(noisy, 25.0, o, prec=32)
+    from gbm3d_b200.api import _as_set
+    U, W = gpu.denoiseAndAggregateGPU(Vo, _as_set(So, co), 25.0 * options.getTau(3, 1), None, None, o)
+    Uo, Wo = oracle.denoiseAndAggregateMedian(Vo, So, o, cnt=co, prec=32)
+    assert np.array_equal(U, Uo) and np.array_equal(W, Wo)
+
+
+def test_GBM3D_pipeline_median(gpu, oracle):
+    clean, noisy = synth.noisy_image(96, 96, 25.0, seed=32)
+    o = dict(_opts(), filtType="median")
+    U, out = gpu.GBM3D(noisy, 25.0, o)
+    Uo, U1o = oracle.GBM3D(noisy, 25.0, o, prec=32)
+    assert np.array_equal(out["U1"], U1o) and np.array_equal(U, Uo)

@@ -163,3 +163,11 @@ def test_oracle_global_matcher_matches_golden(oracle, name):
     S, cnt, pre = oracle.matchBlocksGPU(g["noisy"], float(g["sigma"]), opts, prec=64)
     assert max_abs(pre, g["prefiltered"]) < 1e-9
     assert np.array_equal(S, g["S"])
+
+
+def test_median_filter_matches_scipy(oracle):
+    """medfilt3 with 'symmetric' padding equals a 3x3x3 median with edge replication."""
+    import scipy.ndimage as nd
+    rng = np.random.default_rng(0)
+    V = rng.normal(size=(24, 20, 16))
+    assert np.array_equal(oracle.medfilt3(V, prec=64), nd.median_filter(V, size=3, mode="nearest"))
