@@ -10,6 +10,7 @@ and seeded synthetic images (synth).
 from .options import (checkBM3Dopts, getTau, getWaveFilters3Dbior, myMirrorPadImage, myPSNR,
                       resolve_opts, setBM3Dopts)
 from ._lib import Context, GBM3DError, context
+from .distributed import GBM3D_distributed, getBM3D_distribution, makeInterpWindow
 from .api import (GBM3D, GBM3D_device, MatchSet, denoiseAndAggregateGPU, denoiseAndAggregateWie,
                   denoiseAndAggregateWieFast, matchBlocksCPU, matchBlocksGPU, matchBlocksWie)
 
@@ -17,5 +18,5 @@ __all__ = [
     "GBM3D", "GBM3D_device", "matchBlocksCPU", "matchBlocksGPU", "denoiseAndAggregateGPU", "matchBlocksWie",
     "denoiseAndAggregateWieFast", "denoiseAndAggregateWie", "MatchSet", "Context", "context",
     "GBM3DError", "setBM3Dopts", "checkBM3Dopts", "resolve_opts", "getTau", "getWaveFilters3Dbior",
-    "myMirrorPadImage", "myPSNR",
+    "myMirrorPadImage", "myPSNR", "GBM3D_distributed", "getBM3D_distribution", "makeInterpWindow",
 ]

@@ -219,3 +219,14 @@ def test_GBM3D_pipeline_median(gpu, oracle):
     U, out = gpu.GBM3D(noisy, 25.0, o)
     Uo, U1o = oracle.GBM3D(noisy, 25.0, o, prec=32)
     assert np.array_equal(out["U1"], U1o) and np.array_equal(U, Uo)
+
+
+def test_GBM3D_distributed_cuda_matches_oracle_tiles(gpu):
+    """Tiled GBM3D: the CUDA drop-ins per tile reproduce the oracle per tile bit for bit."""
+    from gbm3d_b200 import distributed as D
+    from test_distributed import oracle_backend
+    clean, noisy = synth.noisy_image(300, 290, 25.0, seed=42)
+    U, out = D.GBM3D_distributed(noisy, 25.0, {"profile": "default"})
+    Uo, outo = D.GBM3D_distributed(noisy, 25.0, {"profile": "default"}, backend=oracle_backend())
+    assert np.array_equal(out["U2"], outo["U2"]) and np.array_equal(U, Uo)
+    assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255) + 5
