@@ -140,6 +140,7 @@ typedef struct {
   int nSpinsWie, spinsWie[8];
   int staleWeights;  // GBM3D.m:26-27,82 slice-reuse behaviour (1 = mirror it)
   int filtType;      // 0 'ht', 1 'median' (denoiseAndAggregateGPU.m:135,165)
+  int refStride, refStrideWie;  // reference spacing per step; 0 = block size (the reference)
 } orc_opts;
 
 }  // extern "C"
@@ -157,11 +158,16 @@ struct MatchOut {
   T* V1; T* V2;    // d x d x K x M x N, or null
 };
 
+// References sit at (i*s, j*s), s = refStride (the reference tiles with
+// s = d).  Volume is image-shaped (m x n x K) when s = d, as in the reference,
+// and tile-space (M*d x N*d x K) otherwise: group (i,j) always fills the tile
+// rows i*d.., columns j*d...
 template <class T>
 void match_blocks(const T* I, const T* In, int m, int n, int d, int d2, int K,
-                  int numMin, double tol, bool tol_branch, MatchOut<T> o) {
-  const int h = d2 / 2, Wd = d + d2 - 1;
-  const int M = m / d, N = n / d;
+                  int numMin, double tol, bool tol_branch, MatchOut<T> o, int stride) {
+  const int h = d2 / 2, Wd = d + d2 - 1, s = stride;
+  const int M = (m - d) / s + 1, N = (n - d) / s + 1;
+  const int vm = s == d ? m : M * d, vn = s == d ? n : N * d;
   const uint32_t ref_idx = (uint32_t)(h + h * d2 + 1);  // matchBlocksCPU.m:103
 #pragma omp parallel
   {
@@ -173,9 +179,9 @@ void match_blocks(const T* I, const T* In, int m, int n, int d, int d2, int K,
         const int g = i + M * j;
         // local search window Itmp = Ipad(i*d + (0..Wd-1), j*d + (0..Wd-1))
         for (int c = 0; c < Wd; ++c) {
-          int sc = pad_index(j * d + c, n, h);
+          int sc = pad_index(j * s + c, n, h);
           for (int r = 0; r < Wd; ++r) {
-            int sr = pad_index(i * d + r, m, h);
+            int sr = pad_index(i * s + r, m, h);
             win[r + c * Wd] = I[sr + (size_t)sc * m];
             if (In) win2[r + c * Wd] = In[sr + (size_t)sc * m];
           }
@@ -238,7 +244,7 @@ void match_blocks(const T* I, const T* In, int m, int n, int d, int d2, int K,
             for (int r = 0; r < d; ++r) {
               T v = win[(a + r) + (b + c) * Wd];
               if (o.Volume)
-                o.Volume[(size_t)(i * d + r) + (size_t)(j * d + c) * m + (size_t)k * m * n] = v;
+                o.Volume[(size_t)(i * d + r) + (size_t)(j * d + c) * vm + (size_t)k * vm * vn] = v;
               if (o.V1 && real) {
                 size_t off = r + (size_t)d * (c + (size_t)d * (k + (size_t)K * (i + (size_t)M * j)));
                 o.V1[off] = v;
@@ -409,9 +415,11 @@ T ht_weight(const T* Vt, size_t sy, size_t sx, size_t sz, int d, int Nm) {
 // the reference's loop order (ref row y, ref col x, match i), each add rounded
 // in T.  value(g, k, r, c) and wval(g, r, c) give the per-pixel terms.
 template <class T, class FV, class FW>
-void aggregate(int M, int N, int d, int d2, int K, const uint32_t* S, const int32_t* cnt,
+void aggregate(int M, int N, int d, int d2, int K, int stride, const uint32_t* S, const int32_t* cnt,
                FV value, FW wval, double* U, double* W) {
-  const int m = M * d, n = N * d, h = d2 / 2, P = m + d2, Q = n + d2;
+  const int s = stride;
+  // output (M-1)s+d x (N-1)s+d; the reference (s = d) writes M*d x N*d
+  const int m = (M - 1) * s + d, n = (N - 1) * s + d, h = d2 / 2, P = m + d2, Q = n + d2;
   std::vector<T> Up((size_t)P * Q, T(0)), Wp((size_t)P * Q, T(0));
   int nth = 1;
 #ifdef _OPENMP
@@ -426,12 +434,12 @@ void aggregate(int M, int N, int d, int d2, int K, const uint32_t* S, const int3
     const int c0 = (int)((long)Q * t / nth), c1 = (int)((long)Q * (t + 1) / nth);
     for (int y = 0; y < M; ++y)
       for (int x = 0; x < N; ++x) {
-        if (x * d + d2 + d - 1 <= c0 || x * d >= c1) continue;
+        if (x * s + d2 + d - 1 <= c0 || x * s >= c1) continue;
         const int g = y + M * x;
         const int nm = cnt ? cnt[g] : K;
         for (int i = 0; i < nm; ++i) {
           int e = (int)S[(size_t)g * K + i] - 1, a = e % d2, b = e / d2;
-          int R0 = y * d + a, C0 = x * d + b;
+          int R0 = y * s + a, C0 = x * s + b;
           for (int c = 0; c < d; ++c) {
             int C = C0 + c;
             if (C < c0 || C >= c1) continue;
@@ -452,14 +460,14 @@ void aggregate(int M, int N, int d, int d2, int K, const uint32_t* S, const int3
 }
 
 template <class T>
-void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, const uint32_t* S,
+void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, int s, const uint32_t* S,
                   const int32_t* cnt, double* U, double* W);
 
 // denoiseAndAggregateGPU.m:11-92 (filtType 'ht')
 template <class T>
 void denoise_ht(const T* Volume, int M, int N, int d, int d2, int K, const uint32_t* S,
                 const int32_t* cnt, int levels, int cycleSpin, const double* tau,
-                const orc_filters* f, double* U, double* W) {
+                const orc_filters* f, double* U, double* W, int stride) {
   const int m = M * d, n = N * d;
   const size_t vol = (size_t)m * n * K;
   Bank1D<T> bxy = make_bank<T>(f->len_xy, f->a_lo_xy, f->a_hi_xy, f->s_lo_xy, f->s_hi_xy);
@@ -491,7 +499,7 @@ void denoise_ht(const T* Volume, int M, int N, int d, int d2, int K, const uint3
     T v = sum[o] / cs;
     sum[o] = v > T(0) ? v : T(0);
   }
-  ht_aggregate<T>(sum, M, N, d, d2, K, S, cnt, U, W);
+  ht_aggregate<T>(sum, M, N, d, d2, K, stride, S, cnt, U, W);
 }
 
 // medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:165-168), 'symmetric'
@@ -519,15 +527,15 @@ void median3(const T* V, int m, int n, int K, std::vector<T>& out) {
 
 template <class T>
 void denoise_median(const T* Volume, int M, int N, int d, int d2, int K, const uint32_t* S, const int32_t* cnt,
-                    double* U, double* W) {
+                    double* U, double* W, int stride) {
   std::vector<T> vavg;
   median3<T>(Volume, M * d, N * d, K, vavg);
-  ht_aggregate<T>(vavg, M, N, d, d2, K, S, cnt, U, W);
+  ht_aggregate<T>(vavg, M, N, d, d2, K, stride, S, cnt, U, W);
 }
 
 // Aggregation of denoiseAndAggregateGPU.m:174-208 from the filtered volume.
 template <class T>
-void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, const uint32_t* S,
+void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, int stride, const uint32_t* S,
                   const int32_t* cnt, double* U, double* W) {
   const int m = M * d, n = N * d;
   const int G = M * N;
@@ -548,7 +556,7 @@ void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, const
     return (wg[g] * b) * mask[r + c * d];
   };
   auto wval = [&](int g, int r, int c) { return wg[g] * mask[r + c * d]; };
-  aggregate<T>(M, N, d, d2, K, S, cnt, value, wval, U, W);
+  aggregate<T>(M, N, d, d2, K, stride, S, cnt, value, wval, U, W);
 }
 
 // ---------------------------------------------------------------------------
@@ -603,7 +611,7 @@ void haar_rec(T* v, int K, int levels, T cc) {
 template <class T>
 void denoise_wiener(const T* V1, const T* V2, int M, int N, int d, int d2, int K,
                     const uint32_t* S, const double* sigma, int sigma_is_matrix, int variant,
-                    double* U, double* W) {
+                    double* U, double* W, int stride) {
   const int levels = K < 16 ? 2 : 3;
   const int dd = d * d, G = M * N;
   std::vector<double> Tm(dd), Ti(dd);
@@ -706,7 +714,7 @@ void denoise_wiener(const T* V1, const T* V2, int M, int N, int d, int d2, int K
     return wgt * out[(size_t)g * gsz + (size_t)i * dd + r + c * d];
   };
   auto wval = [&](int g, int r, int c) { return wf[r + c * d] / n2[g]; };
-  aggregate<T>(M, N, d, d2, K, S, nullptr, value, wval, U, W);
+  aggregate<T>(M, N, d, d2, K, stride, S, nullptr, value, wval, U, W);
 }
 
 // getTau.m:9-51
@@ -769,7 +777,16 @@ void bior_filters(orc_filters* f) {
 template <class T>
 void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, double* Uout, double* U1out) {
   const int d = o->blockSize, dw = o->blockSizeWie, d2 = o->matchSize, K = o->numMax;
-  const int Mp = (m0 + d - 1) / d * d, Np = (n0 + d - 1) / d * d;
+  const int st1 = o->refStride > 0 ? o->refStride : d, st2 = o->refStrideWie > 0 ? o->refStrideWie : dw;
+  // GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
+  // smallest size whose references of both steps end exactly at the border
+  auto padded = [&](int L) {
+    if (st1 == d && (!o->Wiener || (st2 == dw && d % dw == 0))) return (L + d - 1) / d * d;
+    int p = std::max(L, std::max(d, dw));
+    while ((p - d) % st1 != 0 || (o->Wiener && (p - dw) % st2 != 0)) ++p;
+    return p;
+  };
+  const int Mp = padded(m0), Np = padded(n0);
   const size_t px = (size_t)Mp * Np;
   std::vector<double> I(px);
   mirror_pad(I0, m0, n0, I.data(), Mp, Np);
@@ -787,17 +804,17 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
     int s = o->spins[ii];
     circshift2(I.data(), Mp, Np, s, sh.data());
     std::vector<T> It = to_T<T>(sh.data(), px);
-    int M = Mp / d, N = Np / d;
+    int M = (Mp - d) / st1 + 1, N = (Np - d) / st1 + 1;
     std::vector<uint32_t> S((size_t)M * N * K);
     std::vector<int32_t> cnt(M * N);
-    std::vector<T> Vol(px * K);
+    std::vector<T> Vol(st1 == d ? px * K : (size_t)M * d * N * d * K);
     MatchOut<T> mo{S.data(), cnt.data(), Vol.data(), nullptr, nullptr};
-    match_blocks<T>(It.data(), nullptr, Mp, Np, d, d2, K, o->numMin, tol, o->numMax != o->numMin, mo);
+    match_blocks<T>(It.data(), nullptr, Mp, Np, d, d2, K, o->numMin, tol, o->numMax != o->numMin, mo, st1);
     if (o->filtType == 1)
-      denoise_median<T>(Vol.data(), M, N, d, d2, K, S.data(), cnt.data(), u.data(), w.data());
+      denoise_median<T>(Vol.data(), M, N, d, d2, K, S.data(), cnt.data(), u.data(), w.data(), st1);
     else
       denoise_ht<T>(Vol.data(), M, N, d, d2, K, S.data(), cnt.data(), o->levels, o->cycleSpin,
-                    tau.data(), &f, u.data(), w.data());
+                    tau.data(), &f, u.data(), w.data(), st1);
     circshift2(u.data(), Mp, Np, -s, &U1s[ii * px]);
     circshift2(w.data(), Mp, Np, -s, &Ws[ii * px]);
   }
@@ -824,13 +841,13 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
     circshift2(U1.data(), Mp, Np, s, sh.data());
     circshift2(I.data(), Mp, Np, s, sh2.data());
     std::vector<T> Ip = to_T<T>(sh.data(), px), In = to_T<T>(sh2.data(), px);
-    int M = Mp / dw, N = Np / dw;
+    int M = (Mp - dw) / st2 + 1, N = (Np - dw) / st2 + 1;
     std::vector<uint32_t> S((size_t)M * N * K);
     std::vector<T> V1((size_t)dw * dw * K * M * N), V2(V1.size());
     MatchOut<T> mo{S.data(), nullptr, nullptr, V1.data(), V2.data()};
-    match_blocks<T>(Ip.data(), In.data(), Mp, Np, dw, d2, K, K, 0.0, false, mo);
+    match_blocks<T>(Ip.data(), In.data(), Mp, Np, dw, d2, K, K, 0.0, false, mo, st2);
     double sg = sigma;
-    denoise_wiener<T>(V1.data(), V2.data(), M, N, dw, d2, K, S.data(), &sg, 0, 0, u.data(), w.data());
+    denoise_wiener<T>(V1.data(), V2.data(), M, N, dw, d2, K, S.data(), &sg, 0, 0, u.data(), w.data(), st2);
     circshift2(u.data(), Mp, Np, -s, &Us[ii * px]);
     circshift2(w.data(), Mp, Np, -s, &Ws[ii * px]);
   }
@@ -1009,31 +1026,31 @@ void orc_mirror_pad(const double* I, int m, int n, double* O, int M, int N) { mi
 
 // [S,Volume] = matchBlocksCPU(I,sigma,opts); Volume is float (prec 32) or double.
 int orc_match_blocks(int prec, const double* I, int m, int n, double sigma, int d, int d2,
-                     int numMax, int numMin, uint32_t* S, int32_t* cnt, void* Volume) {
+                     int numMax, int numMin, uint32_t* S, int32_t* cnt, void* Volume, int stride) {
   const double tol = 0.005 * sigma * sigma * d * d;
   const size_t px = (size_t)m * n;
   if (prec == 32) {
     auto It = to_T<float>(I, px);
     MatchOut<float> o{S, cnt, (float*)Volume, nullptr, nullptr};
-    match_blocks<float>(It.data(), nullptr, m, n, d, d2, numMax, numMin, tol, numMax != numMin, o);
+    match_blocks<float>(It.data(), nullptr, m, n, d, d2, numMax, numMin, tol, numMax != numMin, o, stride);
   } else {
     MatchOut<double> o{S, cnt, (double*)Volume, nullptr, nullptr};
-    match_blocks<double>(I, nullptr, m, n, d, d2, numMax, numMin, tol, numMax != numMin, o);
+    match_blocks<double>(I, nullptr, m, n, d, d2, numMax, numMin, tol, numMax != numMin, o, stride);
   }
   return 0;
 }
 
 // [S,V1,V2] = matchBlocksWie(I,In,sigma,opts)
 int orc_match_blocks_wie(int prec, const double* I, const double* In, int m, int n, int d, int d2,
-                         int K, uint32_t* S, void* V1, void* V2) {
+                         int K, uint32_t* S, void* V1, void* V2, int stride) {
   const size_t px = (size_t)m * n;
   if (prec == 32) {
     auto It = to_T<float>(I, px), Int = to_T<float>(In, px);
     MatchOut<float> o{S, nullptr, nullptr, (float*)V1, (float*)V2};
-    match_blocks<float>(It.data(), Int.data(), m, n, d, d2, K, K, 0.0, false, o);
+    match_blocks<float>(It.data(), Int.data(), m, n, d, d2, K, K, 0.0, false, o, stride);
   } else {
     MatchOut<double> o{S, nullptr, nullptr, (double*)V1, (double*)V2};
-    match_blocks<double>(I, In, m, n, d, d2, K, K, 0.0, false, o);
+    match_blocks<double>(I, In, m, n, d, d2, K, K, 0.0, false, o, stride);
   }
   return 0;
 }
@@ -1041,11 +1058,11 @@ int orc_match_blocks_wie(int prec, const double* I, const double* In, int m, int
 // [U,W] = denoiseAndAggregateGPU(Volume,S,tau,Psi,Psi2,opts)
 int orc_denoise_ht(int prec, const void* Volume, int M, int N, int d, int d2, int K,
                    const uint32_t* S, const int32_t* cnt, int levels, int cycleSpin,
-                   const double* tau, const orc_filters* f, double* U, double* W) {
+                   const double* tau, const orc_filters* f, double* U, double* W, int stride) {
   if (prec == 32)
-    denoise_ht<float>((const float*)Volume, M, N, d, d2, K, S, cnt, levels, cycleSpin, tau, f, U, W);
+    denoise_ht<float>((const float*)Volume, M, N, d, d2, K, S, cnt, levels, cycleSpin, tau, f, U, W, stride);
   else
-    denoise_ht<double>((const double*)Volume, M, N, d, d2, K, S, cnt, levels, cycleSpin, tau, f, U, W);
+    denoise_ht<double>((const double*)Volume, M, N, d, d2, K, S, cnt, levels, cycleSpin, tau, f, U, W, stride);
   return 0;
 }
 
@@ -1053,21 +1070,21 @@ int orc_denoise_ht(int prec, const void* Volume, int M, int N, int d, int d2, in
 // denoiseAndAggregateWie (variant 1)
 int orc_denoise_wiener(int prec, const void* V1, const void* V2, int M, int N, int d, int d2, int K,
                        const uint32_t* S, const double* sigma, int sigma_is_matrix, int variant,
-                       double* U, double* W) {
+                       double* U, double* W, int stride) {
   if (prec == 32)
     denoise_wiener<float>((const float*)V1, (const float*)V2, M, N, d, d2, K, S, sigma,
-                          sigma_is_matrix, variant, U, W);
+                          sigma_is_matrix, variant, U, W, stride);
   else
     denoise_wiener<double>((const double*)V1, (const double*)V2, M, N, d, d2, K, S, sigma,
-                           sigma_is_matrix, variant, U, W);
+                           sigma_is_matrix, variant, U, W, stride);
   return 0;
 }
 
 // [U,W] = denoiseAndAggregateGPU(Volume,S,tau,Psi,Psi2,opts) with filtType 'median'
 int orc_denoise_median(int prec, const void* Volume, int M, int N, int d, int d2, int K, const uint32_t* S,
-                       const int32_t* cnt, double* U, double* W) {
-  if (prec == 32) denoise_median<float>((const float*)Volume, M, N, d, d2, K, S, cnt, U, W);
-  else denoise_median<double>((const double*)Volume, M, N, d, d2, K, S, cnt, U, W);
+                       const int32_t* cnt, double* U, double* W, int stride) {
+  if (prec == 32) denoise_median<float>((const float*)Volume, M, N, d, d2, K, S, cnt, U, W, stride);
+  else denoise_median<double>((const double*)Volume, M, N, d, d2, K, S, cnt, U, W, stride);
   return 0;
 }
 

@@ -52,6 +52,7 @@ class orc_opts(C.Structure):
         ("nSpins", C.c_int), ("spins", C.c_int * 8),
         ("nSpinsWie", C.c_int), ("spinsWie", C.c_int * 8),
         ("staleWeights", C.c_int), ("filtType", C.c_int),
+        ("refStride", C.c_int), ("refStrideWie", C.c_int),
     ]
 
 
@@ -141,16 +142,25 @@ def sine_window(d: int, lo: float, hi: float) -> np.ndarray:
     return w
 
 
+def _stride(opts, key, d):
+    s = opts.get(key)
+    return int(s) if s else int(d)
+
+
 def matchBlocksCPU(I, sigma, opts, prec=32):
+    """refStride s (default blockSize): references at i*s; Volume is m x n x K
+    for s = blockSize (the reference) and tile-space (M*d, N*d, K) otherwise."""
     I = np.asfortranarray(I, dtype=np.float64)
     m, n = I.shape
     d, d2, K = opts["blockSize"], opts["matchSize"], opts["numMax"]
-    M, N = m // d, n // d
+    st = _stride(opts, "refStride", d)
+    M, N = (m - d) // st + 1, (n - d) // st + 1
     S = np.zeros((K, M, N), dtype=np.uint32, order="F")
     cnt = np.zeros((M, N), dtype=np.int32, order="F")
-    Vol = np.zeros((m, n, K), dtype=np.float32 if prec == 32 else np.float64, order="F")
+    vshape = (m, n, K) if st == d else (M * d, N * d, K)
+    Vol = np.zeros(vshape, dtype=np.float32 if prec == 32 else np.float64, order="F")
     lib().orc_match_blocks(prec, _p(I), m, n, C.c_double(sigma), d, d2, K, opts["numMin"],
-                           _p(S), _p(cnt), _p(Vol))
+                           _p(S), _p(cnt), _p(Vol), st)
     return S, Vol, cnt
 
 
@@ -159,12 +169,13 @@ def matchBlocksWie(I, In, sigma, opts, prec=32):
     In = np.asfortranarray(In, dtype=np.float64)
     m, n = I.shape
     d, d2, K = opts["blockSizeWie"], opts["matchSize"], opts["numMax"]
-    M, N = m // d, n // d
+    st = _stride(opts, "refStrideWie", d)
+    M, N = (m - d) // st + 1, (n - d) // st + 1
     S = np.zeros((K, M, N), dtype=np.uint32, order="F")
     dt = np.float32 if prec == 32 else np.float64
     V1 = np.zeros((d, d, K, M, N), dtype=dt, order="F")
     V2 = np.zeros_like(V1)
-    lib().orc_match_blocks_wie(prec, _p(I), _p(In), m, n, d, d2, K, _p(S), _p(V1), _p(V2))
+    lib().orc_match_blocks_wie(prec, _p(I), _p(In), m, n, d, d2, K, _p(S), _p(V1), _p(V2), st)
     return S, V1, V2
 
 
@@ -176,14 +187,15 @@ def denoiseAndAggregateGPU(Volume, S, tau, opts, cnt=None, filters=None, prec=32
     S = np.asfortranarray(S, dtype=np.uint32)
     tau = np.asfortranarray(tau, dtype=np.float64)
     f = filters if filters is not None else bior_filters()
-    U = np.zeros((M * d, N * d), order="F")
+    st = _stride(opts, "refStride", d)
+    U = np.zeros(((M - 1) * st + d, (N - 1) * st + d), order="F")
     W = np.zeros_like(U)
     cp = None
     if cnt is not None:
         cnt = np.asfortranarray(cnt, dtype=np.int32)
         cp = _p(cnt)
     lib().orc_denoise_ht(prec, _p(Volume), M, N, d, opts["matchSize"], K, _p(S), cp,
-                         opts["levels"], opts["cycleSpin"], _p(tau), C.byref(f), _p(U), _p(W))
+                         opts["levels"], opts["cycleSpin"], _p(tau), C.byref(f), _p(U), _p(W), st)
     return U, W
 
 
@@ -195,10 +207,11 @@ def denoiseAndAggregateWieFast(V1, V2, S, sigma, opts, prec=32, variant=0):
     S = np.asfortranarray(S, dtype=np.uint32)
     sg = np.asfortranarray(np.atleast_1d(np.asarray(sigma, dtype=np.float64)))
     is_mat = 1 if sg.size > 1 else 0
-    U = np.zeros((M * d, N * d), order="F")
+    st = _stride(opts, "refStrideWie", d)
+    U = np.zeros(((M - 1) * st + d, (N - 1) * st + d), order="F")
     W = np.zeros_like(U)
     lib().orc_denoise_wiener(prec, _p(V1), _p(V2), M, N, d, opts["matchSize"], K, _p(S), _p(sg),
-                             is_mat, variant, _p(U), _p(W))
+                             is_mat, variant, _p(U), _p(W), st)
     return U, W
 
 
@@ -230,6 +243,8 @@ def make_opts(o: dict) -> orc_opts:
     c.spinsWie[: c.nSpinsWie] = [int(s) for s in o["matchSpinsWie"]]
     c.staleWeights = 1 if o.get("staleWeights", True) else 0
     c.filtType = 1 if o.get("filtType", "ht") == "median" else 0
+    c.refStride = int(o.get("refStride") or 0)
+    c.refStrideWie = int(o.get("refStrideWie") or 0)
     return c
 
 
@@ -265,13 +280,14 @@ def denoiseAndAggregateMedian(Volume, S, opts, cnt=None, prec=32):
     K, M, N = S.shape
     d = opts["blockSize"]
     S = np.asfortranarray(S, dtype=np.uint32)
-    U = np.zeros((M * d, N * d), order="F")
+    st = _stride(opts, "refStride", d)
+    U = np.zeros(((M - 1) * st + d, (N - 1) * st + d), order="F")
     W = np.zeros_like(U)
     cp = None
     if cnt is not None:
         cnt = np.asfortranarray(cnt, dtype=np.int32)
         cp = _p(cnt)
-    lib().orc_denoise_median(prec, _p(Volume), M, N, d, opts["matchSize"], K, _p(S), cp, _p(U), _p(W))
+    lib().orc_denoise_median(prec, _p(Volume), M, N, d, opts["matchSize"], K, _p(S), cp, _p(U), _p(W), st)
     return U, W
 
 
