@@ -32,7 +32,7 @@ class gbm3d_opts(C.Structure):
         ("Wiener", C.c_int), ("filtType", C.c_int),
         ("nMatchSpins", C.c_int), ("matchSpins", C.c_int * 8),
         ("nMatchSpinsWie", C.c_int), ("matchSpinsWie", C.c_int * 8),
-        ("staleWeights", C.c_int),
+        ("staleWeights", C.c_int), ("refStrideWie", C.c_int), ("wavelet", C.c_int),
     ]
 
 

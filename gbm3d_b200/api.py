@@ -56,8 +56,9 @@ def c_opts(opts: dict) -> gbm3d_opts:
     c = gbm3d_opts()
     c.numMax, c.numMin = int(o["numMax"]), int(o["numMin"])
     c.blockSize, c.blockSizeWie, c.matchSize = int(o["blockSize"]), int(o["blockSizeWie"]), int(o["matchSize"])
-    rs = o.get("refStride")
-    c.refStride = 0 if rs is None or int(rs) == int(o["blockSize"]) else int(rs)
+    s1, s2 = _opt.strides(o)
+    c.refStride = 0 if s1 == int(o["blockSize"]) else s1
+    c.refStrideWie = 0 if s2 == int(o["blockSizeWie"]) else s2
     c.levels, c.cycleSpin, c.tauMode = int(o["levels"]), int(o["cycleSpin"]), int(o["tauMode"])
     c.Wiener = 1 if o["Wiener"] else 0
     ft = o.get("filtType", "ht")
@@ -74,6 +75,10 @@ def c_opts(opts: dict) -> gbm3d_opts:
     for i, s in enumerate(mw):
         c.matchSpinsWie[i] = int(s)
     c.staleWeights = 1 if o.get("staleWeights", True) else 0
+    wn = o.get("wname", "bior")
+    if wn not in ("bior", "haar"):
+        raise GBM3DError(5, f"wname '{wn}': the pipeline's banks are 'bior' (bior1.5 x Haar) and 'haar'")
+    c.wavelet = 1 if wn == "haar" else 0
     return c
 
 
@@ -98,16 +103,20 @@ def _sigma_scalar(sigma) -> float:
 
 
 def matchBlocksCPU(I, sigma, opts: dict, ctx: Context | None = None):
-    """[S, Volume] = matchBlocksCPU(I, sigma, opts)."""
+    """[S, Volume] = matchBlocksCPU(I, sigma, opts).
+
+    With refStride s != blockSize the Volume is tile-space, (M d) x (N d) x K.
+    """
     ctx = ctx or context()
     o = _opt.checkBM3Dopts(opts)
     I = np.asfortranarray(I, dtype=np.float64)
     m, n = I.shape
     d, K = int(o["blockSize"]), int(o["numMax"])
-    M, N = m // d, n // d
+    s = _opt.strides(o)[0]
+    M, N = _opt.grid_count(m, d, s), _opt.grid_count(n, d, s)
     S = np.zeros((K, M, N), dtype=np.uint32, order="F")
     cnt = np.zeros((M, N), dtype=np.int32, order="F")
-    V = np.zeros((m, n, K), dtype=np.float32, order="F")
+    V = np.zeros((m, n, K) if s == d else (M * d, N * d, K), dtype=np.float32, order="F")
     co = c_opts(o)
     ctx.check(lib().gbm3d_matchBlocksCPU(ctx.h, _p(I), m, n, _sigma_scalar(sigma), C.byref(co),
                                          _p(S), _p(cnt), _p(V)))
@@ -152,7 +161,8 @@ def denoiseAndAggregateGPU(Volume, S, tau, Psi, Psi2, opts: dict, ctx: Context |
     tau = np.asfortranarray(tau, dtype=np.float64)
     if tau.shape != (int(o["levels"]), 7):
         raise GBM3DError(1, "tau must be levels x 7")
-    U = np.zeros((M * d, N * d), order="F")
+    s = _opt.strides(o)[0]
+    U = np.zeros(((M - 1) * s + d, (N - 1) * s + d), order="F")
     W = np.zeros_like(U)
     co, cf = c_opts(o), c_filters(fac)
     cp = None
@@ -174,7 +184,8 @@ def matchBlocksWie(I, In, sigma, opts: dict, ctx: Context | None = None):
         raise GBM3DError(1, "I and In must have the same size")
     m, n = I.shape
     d, K = int(o["blockSizeWie"]), int(o["numMax"])
-    M, N = m // d, n // d
+    s = _opt.strides(o)[1]
+    M, N = _opt.grid_count(m, d, s), _opt.grid_count(n, d, s)
     S = np.zeros((K, M, N), dtype=np.uint32, order="F")
     V1 = np.zeros((d, d, K, M, N), dtype=np.float32, order="F")
     V2 = np.zeros_like(V1)
@@ -192,10 +203,11 @@ def _wiener(V1, V2, S, sigma, opts, ctx, variant):
     d, _, K, M, N = V1.shape
     if V2.shape != V1.shape or S.shape != (K, M, N):
         raise GBM3DError(1, "V1, V2 and S sizes disagree")
-    o = dict(o, blockSizeWie=d, numMax=K, numMin=min(int(o["numMin"]), K))
+    s = _opt.strides(o)[1]
+    o = dict(o, blockSizeWie=d, numMax=K, numMin=min(int(o["numMin"]), K), refStrideWie=s)
     Sa = np.asfortranarray(S, dtype=np.uint32)
     sg = np.asfortranarray(np.atleast_1d(np.asarray(sigma, dtype=np.float64)))
-    U = np.zeros((M * d, N * d), order="F")
+    U = np.zeros(((M - 1) * s + d, (N - 1) * s + d), order="F")
     W = np.zeros_like(U)
     co = c_opts(o)
     if variant == 0:

@@ -46,14 +46,16 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   const int tile = blockIdx.x * 4 + warp;
   if (tile >= tiles_r * tiles_c) return;
   const int R0 = (tile % tiles_r) * TR, C0 = (tile / tiles_r) * TC;
-  const int K = A.K, m = A.m;
+  const int K = A.K, s = A.s;
+  const int mv = A.M * D;  // rows of the tile-space step-1 blocks
   constexpr int H = D2 / 2;
   const int PR0 = R0 + H, PC0 = C0 + H;  // tile origin in the reference's padded U
-  const int i_lo = max(0, ceil_div(PR0 - D - D2 + 2, D)), i_hi = min(A.M - 1, floor_div(PR0 + TR - 1, D));
-  const int j_lo = max(0, ceil_div(PC0 - D - D2 + 2, D)), j_hi = min(A.N - 1, floor_div(PC0 + TC - 1, D));
+  // references whose window (origin i s, extent D + D2 - 1) can reach the tile
+  const int i_lo = max(0, ceil_div(PR0 - D - D2 + 2, s)), i_hi = min(A.M - 1, floor_div(PR0 + TR - 1, s));
+  const int j_lo = max(0, ceil_div(PC0 - D - D2 + 2, s)), j_hi = min(A.N - 1, floor_div(PC0 + TC - 1, s));
   const int NI = i_hi - i_lo + 1, NJ = j_hi - j_lo + 1;
   const int total = (NI > 0 && NJ > 0) ? NI * NJ * K : 0;
-  const size_t mn = (size_t)m * A.n;
+  const size_t mn = (size_t)mv * (A.N * D);
   const unsigned FULL = 0xffffffffu;
   // lane's candidate: slot k = lane % K when K divides 32, else by division
   const bool kdiv = (32 % K) == 0;
@@ -62,7 +64,7 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   int ii = rq / max(NJ, 1), jj = rq - ii * max(NJ, 1);
 
   const int pr = lane & 7, pc = lane >> 3;  // lane's pixel in the tile
-  const int vlane = WIE ? pr + pc * D : pr + m * pc;
+  const int vlane = WIE ? pr + pc * D : pr + mv * pc;
   const int wlane = pr + pc * D;
   float u = 0.f, w = 0.f;
   auto walk = [&](int count) {
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
       const int nm = A.cnt ? A.cnt[g] : K;
       if (k < nm) {
         const int e = (int)A.S[(size_t)g * K + k] - 1;
-        const int r0 = i * D + e % D2 - PR0, c0 = j * D + e / D2 - PC0;
+        const int r0 = i * s + e % D2 - PR0, c0 = j * s + e / D2 - PC0;
         hit = r0 < TR && r0 + D > 0 && c0 < TC && c0 + D > 0;
         if (hit) {
           ent.x = (r0 + BIAS) | ((c0 + BIAS) << 16);
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
             ent.y = (g * K + k) * (D * D) - r0 - c0 * D;
             ent.z = g * (D * D) - r0 - c0 * D;
           } else {
-            ent.y = (int)((size_t)i * D + (size_t)m * (j * D) + mn * k) - r0 - m * c0;
+            ent.y = (int)((size_t)i * D + (size_t)mv * (j * D) + mn * k) - r0 - mv * c0;
             ent.z = __float_as_int(A.gw[g]);
           }
         }
@@ -166,7 +168,8 @@ static cudaError_t launch_px(const AggArgs& A, cudaStream_t st) {
 
 cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st) {
   // block data offsets are 32-bit in the list entries
-  if ((size_t)A.m * A.n * A.K >= ((size_t)1 << 31) || (size_t)A.M * A.N * A.K * A.d * A.d >= ((size_t)1 << 31))
+  if ((size_t)A.m * A.n * A.K >= ((size_t)1 << 31) || (size_t)A.M * A.N * A.K * A.d * A.d >= ((size_t)1 << 31) ||
+      A.s < 1 || A.s > A.d)
     return cudaErrorInvalidValue;
 #define GBM3D_AGG_CASE(DD, DD2)                                                                 \
   if (A.d == DD && A.d2 == DD2)                                                                 \

@@ -197,6 +197,20 @@ void bior(gbm3d_filters* f) {
   f->s_lo_z[0] = Cc; f->s_lo_z[1] = Cc; f->s_hi_z[0] = -Cc; f->s_hi_z[1] = Cc;
 }
 
+// 3D Haar bank: the two-tap Haar pair on all three axes (opts.wavelet = 1).
+void haar3d(gbm3d_filters* f) {
+  std::memset(f, 0, sizeof(*f));
+  const double Cc = std::sqrt(2.0) / 2;
+  f->len_xy = 2;
+  f->len_z = 2;
+  double* lo[4] = {f->a_lo_xy, f->s_lo_xy, f->a_lo_z, f->s_lo_z};
+  double* hi[4] = {f->a_hi_xy, f->s_hi_xy, f->a_hi_z, f->s_hi_z};
+  for (int q = 0; q < 4; ++q) {
+    lo[q][0] = Cc; lo[q][1] = Cc;
+    hi[q][0] = -Cc; hi[q][1] = Cc;
+  }
+}
+
 void tau_table(int levels, int mode, double* tau) {
   for (int j = 0; j < 7; ++j)
     for (int i = 0; i < levels; ++i) {
@@ -277,9 +291,11 @@ void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
   if (o->numMax < 1 || o->numMax > 32) argfail(c, "numMax must be in 1..32");
   if (o->numMin < 1 || o->numMin > o->numMax) argfail(c, "numMin must be in 1..numMax");
   if (o->matchSize < 2 || (o->matchSize & 1)) argfail(c, "matchSize must be even");
-  if (o->refStride != 0 && o->refStride != o->blockSize)
-    argfail(c, "refStride other than blockSize is not supported yet", GBM3D_ERR_UNSUPPORTED);
+  if (o->refStride < 0 || o->refStride > o->blockSize) argfail(c, "refStride must be in 1..blockSize (0: blockSize)");
+  if (o->refStrideWie < 0 || o->refStrideWie > o->blockSizeWie)
+    argfail(c, "refStrideWie must be in 1..blockSizeWie (0: blockSizeWie)");
   if (o->filtType != 0 && o->filtType != 1) argfail(c, "unrecognized filtering");  // denoiseAndAggregateGPU.m:54
+  if (o->wavelet != 0 && o->wavelet != 1) argfail(c, "wavelet must be 0 (bior1.5 x Haar) or 1 (3D Haar)");
 }
 
 void check_match(gbm3d_ctx* c, int d, int d2, int K) {
@@ -290,6 +306,12 @@ void check_match(gbm3d_ctx* c, int d, int d2, int K) {
 }
 
 int pitch4(int rows) { return (rows + 3) & ~3; }
+
+// Reference stride of step 1 / step 2 (0 selects the block size, the
+// reference's tiling) and the reference-grid size along an axis of L pixels.
+int stride1(const gbm3d_opts* o) { return o->refStride > 0 ? o->refStride : o->blockSize; }
+int stride2(const gbm3d_opts* o) { return o->refStrideWie > 0 ? o->refStrideWie : o->blockSizeWie; }
+int grid_count(int L, int d, int s) { return (L - d) / s + 1; }
 
 // Match sets and counts that come from the caller are checked on the host
 // before any kernel indexes memory with them.
@@ -311,9 +333,11 @@ void check_match_set(gbm3d_ctx* c, const uint32_t* S, const int32_t* cnt, size_t
 // ---- pipelines ----------------------------------------------------------------------
 
 // Block matching on a single-precision image already on the device.
+// References at stride s; the volume is m x n x K for s = d (image-shaped,
+// the reference's layout) and (M d) x (N d) x K otherwise.
 void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, int spin, int d, int d2,
                int K, int numMin, double sigma, uint32_t* S, int32_t* cnt, float* volume, float* V1,
-               float* V2, const char* tag) {
+               float* V2, const char* tag, int s) {
   const int P = pitch4(m + d2);
   const std::string t(tag);
   float* pad = buf<float>(c, (t + ".pad").c_str(), (size_t)P * (n + d2));
@@ -327,26 +351,28 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
   A.pad = pad;
   A.pad2 = pad2;
   A.P = P;
-  A.M = m / d;
-  A.N = n / d;
+  A.M = grid_count(m, d, s);
+  A.N = grid_count(n, d, s);
   A.K = K;
+  A.s = s;
   A.numMin = numMin;
   A.tol = (float)(0.005 * sigma * sigma * d * d);
   A.tol_branch = numMin != K;
   A.S = S;
   A.cnt = cnt;
   A.volume = volume;
-  A.m = m;
-  A.n = n;
+  A.m = s == d ? m : A.M * d;
+  A.n = s == d ? n : A.N * d;
   A.V1 = V1;
   A.V2 = V2;
   launched(c, launch_match(d, d2, A, c->st), "match");
 }
 
-// denoiseAndAggregateGPU on device buffers; U, W are float (M d) x (N d).
+// denoiseAndAggregateGPU on device buffers: vol is (M d) x (N d) x K and
+// U, W are float ((M-1) s + d) x ((N-1) s + d).
 void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cnt, int M, int N, int d,
             int d2, int K, int levels, int cycleSpin, const double* tau, const WaveletBank& bk, float* U,
-            float* W, int filtType) {
+            float* W, int filtType, int s) {
   const int m = M * d, n = N * d;
   float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
   if (filtType == 1) {  // medfilt3 instead of the wavelet (denoiseAndAggregateGPU.m:165-168)
@@ -415,8 +441,9 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
   std::vector<double> mk(d * d);
   sine_window(d, 0.1, 0.9, mk.data());
   for (int e = 0; e < d * d; ++e) A.win[e] = (float)mk[e];
-  A.m = m;
-  A.n = n;
+  A.s = s;
+  A.m = (M - 1) * s + d;
+  A.n = (N - 1) * s + d;
   A.U = U;
   A.W = W;
   launched(c, launch_aggregate(A, c->st), "aggregate");
@@ -459,8 +486,9 @@ void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float*
   G.wiener = 1;
   G.blocks = A.out;
   G.gw = A.wt;
-  G.m = M * d;
-  G.n = N * d;
+  G.s = A.s;
+  G.m = (M - 1) * A.s + d;
+  G.n = (N - 1) * A.s + d;
   G.U = U;
   G.W = W;
   launched(c, launch_aggregate(G, c->st), "aggregate");
@@ -508,15 +536,24 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   if (o->Wiener) check_match(c, dw, d2, K);
   if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
   if (!(sigma >= 0) || !std::isfinite(sigma)) argfail(c, "sigma must be a finite non-negative scalar");
-  const int Mp = (m + d - 1) / d * d, Np = (n + d - 1) / d * d;
+  const int st1 = stride1(o), st2 = stride2(o);
+  // GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
+  // smallest size whose references of both steps end exactly at the border
+  auto padded = [&](int L) {
+    if (st1 == d && (!o->Wiener || (st2 == dw && d % dw == 0))) return (L + d - 1) / d * d;
+    int p = std::max(L, std::max(d, dw));
+    while ((p - d) % st1 != 0 || (o->Wiener && (p - dw) % st2 != 0)) ++p;
+    return p;
+  };
+  const int Mp = padded(m), Np = padded(n);
   if (Mp - m > m || Np - n > n) argfail(c, "image smaller than the padding it needs");
   if (Mp < d2 || Np < d2) argfail(c, "image smaller than matchSize");
-  if (o->Wiener && (Mp % dw || Np % dw)) argfail(c, "padded size must be a multiple of blockSizeWie");
   const int nS = o->nMatchSpins, nW = o->Wiener ? o->nMatchSpinsWie : 0;
   if (nS < 1 || nS > 8 || nW < 0 || nW > 8 || (o->Wiener && nW < 1)) argfail(c, "match spin count out of range");
   const size_t px = (size_t)Mp * Np;
   gbm3d_filters f;
-  bior(&f);
+  if (o->wavelet == 1) haar3d(&f);
+  else bior(&f);
   const WaveletBank bk = make_bank(c, &f);
   std::vector<double> tau(o->levels * 7);
   tau_table(o->levels, o->tauMode, tau.data());
@@ -532,10 +569,10 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   }
 
   // step 1: hard-thresholding estimate over the match spins
-  const int M1 = Mp / d, N1 = Np / d;
+  const int M1 = grid_count(Mp, d, st1), N1 = grid_count(Np, d, st1);
   uint32_t* S1 = buf<uint32_t>(c, "p.S1", (size_t)K * M1 * N1);
   int32_t* cnt1 = buf<int32_t>(c, "p.cnt1", (size_t)M1 * N1);
-  float* vol = buf<float>(c, "p.vol", px * K);
+  float* vol = buf<float>(c, "p.vol", (size_t)M1 * d * N1 * d * K);
   float* Us = buf<float>(c, "p.Us", px);
   float* Ws = buf<float>(c, "p.Ws", px);
   double* Ua = buf<double>(c, "p.Ua", px);
@@ -546,9 +583,9 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     const int s = o->matchSpins[ii];
     {
       StageTimer t(c, 1);
-      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1");
+      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1", st1);
     }
-    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType);
+    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType, st1);
     k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
     launched(c, cudaGetLastError(), "accum");
     k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa, ii == 0);
@@ -569,13 +606,13 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   }
 
   // step 2: empirical Wiener estimate over the Wiener match spins
-  const int M2 = Mp / dw, N2 = Np / dw;
+  const int M2 = grid_count(Mp, dw, st2), N2 = grid_count(Np, dw, st2);
   uint32_t* S2 = buf<uint32_t>(c, "p.S2", (size_t)K * M2 * N2);
   for (int ii = 0; ii < nW; ++ii) {
     const int s = o->matchSpinsWie[ii];
     {
       StageTimer t(c, 4);
-      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2");
+      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2", st2);
     }
     float* padP = buf<float>(c, "m2.pad", 1);  // the pilot search image run_match just built
     float* padN = buf<float>(c, "m2.padN", (size_t)pitch4(Mp + d2) * (Np + d2));
@@ -589,6 +626,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     A.M = M2;
     A.N = N2;
     A.K = K;
+    A.s = st2;
     double sg = sigma;
     fill_wiener_consts(A, dw, &sg, 0, 0);
     run_wiener_agg(c, A, dw, d2, Us, Ws);
@@ -725,8 +763,10 @@ int gbm3d_matchBlocksCPU(gbm3d_ctx* c, const double* I, int m, int n, double sig
     check_match(c, d, d2, K);
     if (!I || !S) argfail(c, "I and S are required");
     if (m < d2 || n < d2 || m < d || n < d) argfail(c, "image smaller than matchSize");
-    const int M = m / d, N = n / d;
+    const int s = stride1(o);
+    const int M = grid_count(m, d, s), N = grid_count(n, d, s);
     const size_t px = (size_t)m * n;
+    const size_t vn = s == d ? px * K : (size_t)M * d * N * d * K;
     double* dI = buf<double>(c, "io.I", px);
     ck(c, cudaMemcpyAsync(dI, I, px * sizeof(double), cudaMemcpyHostToDevice, c->st), "H2D");
     ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
@@ -737,13 +777,13 @@ int gbm3d_matchBlocksCPU(gbm3d_ctx* c, const double* I, int m, int n, double sig
     int32_t* dc = buf<int32_t>(c, "io.cnt", (size_t)M * N);
     float* dV = nullptr;
     if (Volume) {
-      dV = buf<float>(c, "io.V", px * K);
-      ck(c, cudaMemsetAsync(dV, 0, px * K * sizeof(float), c->st), "memset");
+      dV = buf<float>(c, "io.V", vn);
+      ck(c, cudaMemsetAsync(dV, 0, vn * sizeof(float), c->st), "memset");
     }
-    run_match(c, If, nullptr, m, n, 0, d, d2, K, o->numMin, sigma, dS, dc, dV, nullptr, nullptr, "m1");
+    run_match(c, If, nullptr, m, n, 0, d, d2, K, o->numMin, sigma, dS, dc, dV, nullptr, nullptr, "m1", s);
     ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (S_count) ck(c, cudaMemcpyAsync(S_count, dc, (size_t)M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
-    if (Volume) ck(c, cudaMemcpyAsync(Volume, dV, px * K * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (Volume) ck(c, cudaMemcpyAsync(Volume, dV, vn * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
@@ -809,8 +849,9 @@ int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* c, const float* Volume, const uint32
     gbm3d_filters fb;
     if (f) fb = *f; else bior(&fb);
     const WaveletBank bk = make_bank(c, &fb);
-    const int m = M * d, n = N * d;
-    const size_t px = (size_t)m * n;
+    const int s = stride1(o);
+    const int m = M * d, n = N * d;  // tile-space volume
+    const size_t px = (size_t)m * n, po = (size_t)((M - 1) * s + d) * ((N - 1) * s + d);
     check_match_set(c, S, S_count, (size_t)M * N, K, d2);
     float* dV = buf<float>(c, "io.V", px * K);
     uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
@@ -821,12 +862,12 @@ int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* c, const float* Volume, const uint32
       dc = buf<int32_t>(c, "io.cnt", (size_t)M * N);
       ck(c, cudaMemcpyAsync(dc, S_count, (size_t)M * N * 4, cudaMemcpyHostToDevice, c->st), "H2D");
     }
-    float* dU = buf<float>(c, "io.U", px);
-    float* dW = buf<float>(c, "io.W", px);
-    run_ht(c, dV, dS, dc, M, N, d, d2, K, o->levels, o->cycleSpin, tau, bk, dU, dW, o->filtType);
-    to_host_double(c, dU, px, U);
+    float* dU = buf<float>(c, "io.U", po);
+    float* dW = buf<float>(c, "io.W", po);
+    run_ht(c, dV, dS, dc, M, N, d, d2, K, o->levels, o->cycleSpin, tau, bk, dU, dW, o->filtType, s);
+    to_host_double(c, dU, po, U);
     ck(c, cudaStreamSynchronize(c->st), "sync");
-    to_host_double(c, dW, px, W);
+    to_host_double(c, dW, po, W);
     ck(c, cudaStreamSynchronize(c->st), "sync");
   });
 }
@@ -838,8 +879,9 @@ int gbm3d_matchBlocksWie(gbm3d_ctx* c, const double* I, const double* In, int m,
     const int d = o->blockSizeWie, d2 = o->matchSize, K = o->numMax;
     check_match(c, d, d2, K);
     if (!I || !In || !S) argfail(c, "missing argument");
-    if (m < d2 || n < d2) argfail(c, "image smaller than matchSize");
-    const int M = m / d, N = n / d;
+    if (m < d2 || n < d2 || m < d || n < d) argfail(c, "image smaller than matchSize");
+    const int s = stride2(o);
+    const int M = grid_count(m, d, s), N = grid_count(n, d, s);
     const size_t px = (size_t)m * n, gs = (size_t)d * d * K * M * N;
     double* dI = buf<double>(c, "io.I", px);
     double* dIn = buf<double>(c, "io.In", px);
@@ -855,7 +897,7 @@ int gbm3d_matchBlocksWie(gbm3d_ctx* c, const double* I, const double* In, int m,
     uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
     float* d1 = V1 ? buf<float>(c, "io.V1", gs) : nullptr;
     float* d2p = V2 ? buf<float>(c, "io.V2", gs) : nullptr;
-    run_match(c, If, V2 ? Inf : nullptr, m, n, 0, d, d2, K, K, sigma, dS, nullptr, nullptr, d1, d2p, "m2");
+    run_match(c, If, V2 ? Inf : nullptr, m, n, 0, d, d2, K, K, sigma, dS, nullptr, nullptr, d1, d2p, "m2", s);
     ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (V1) ck(c, cudaMemcpyAsync(V1, d1, gs * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (V2) ck(c, cudaMemcpyAsync(V2, d2p, gs * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
@@ -875,7 +917,8 @@ static int wiener_entry(gbm3d_ctx* c, const float* V1, const float* V2, const ui
     const int d = o->blockSizeWie, d2 = o->matchSize, K = o->numMax;
     if (M < 1 || N < 1) argfail(c, "empty match set");
     if (d * d > 256) argfail(c, "blockSizeWie too large", GBM3D_ERR_UNSUPPORTED);
-    const size_t gs = (size_t)d * d * K * M * N, px = (size_t)M * d * N * d;
+    const int s = stride2(o);
+    const size_t gs = (size_t)d * d * K * M * N, px = (size_t)((M - 1) * s + d) * ((N - 1) * s + d);
     check_match_set(c, S, nullptr, (size_t)M * N, K, d2);
     float* d1 = buf<float>(c, "io.V1", gs);
     float* d2p = buf<float>(c, "io.V2", gs);
@@ -890,6 +933,7 @@ static int wiener_entry(gbm3d_ctx* c, const float* V1, const float* V2, const ui
     A.M = M;
     A.N = N;
     A.K = K;
+    A.s = s;
     A.d2 = d2;
     fill_wiener_consts(A, d, sigma, is_matrix, variant);
     float* dU = buf<float>(c, "io.U", px);

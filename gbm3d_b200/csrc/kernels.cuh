@@ -10,13 +10,14 @@ struct MatchArgs {
   const float* pad2;  // padded search image gathered into V2 (may be null)
   int P;              // column pitch of pad/pad2 in floats
   int M, N, K;        // reference grid and group size
+  int s;              // reference stride: reference (i, j) sits at (i s, j s)
   int numMin;         // tolerance branch: minimum group size
   float tol;          // tolerance on ssd/||xR||^2
   int tol_branch;     // numMin != numMax
   uint32_t* S;        // K x M x N
   int32_t* cnt;       // M x N (may be null)
-  float* volume;      // m x n x K gather (may be null)
-  int m, n;           // image size for the volume gather
+  float* volume;      // m x n x K gather (may be null); block (i, j) at rows i d, cols j d
+  int m, n;           // volume rows/cols: the image for s = d, (M d) x (N d) otherwise
   float* V1;          // d x d x K x M x N gathers (may be null)
   float* V2;
 };
@@ -69,6 +70,7 @@ struct WienerArgs {
   const float* V2;
   const uint32_t* S;
   int M, N, K;
+  int s;              // reference stride
   float s2[256];      // sigma^2 per DCT coefficient (d x d), single precision
   float T[256];       // DCT-II matrix (d x d, column-major)
   float Ti[256];      // inverse used by the inverse transform
@@ -86,11 +88,12 @@ struct AggArgs {
   const uint32_t* S;
   const int32_t* cnt;   // may be null (every group holds K)
   int M, N, d, d2, K;
+  int s;                // reference stride (block of reference (i, j) lands at (i s + a, j s + b))
   int wiener;           // 0: step-1 weights (scalar x mask); 1: step-2 (precomputed)
-  const float* blocks;  // step 1: image-shaped Vavg (m x n x K); step 2: weighted values, d x d x K per group
+  const float* blocks;  // step 1: tile-space Vavg ((M d) x (N d) x K); step 2: weighted values, d x d x K per group
   const float* gw;      // step 1: weight per group; step 2: weight table, d x d per group
   float win[1024];      // step 1: mask (d x d)
-  int m, n;             // output size (m = M*d, n = N*d)
+  int m, n;             // output size (m = (M-1) s + d, n = (N-1) s + d)
   float* U;             // m x n
   float* W;
 };

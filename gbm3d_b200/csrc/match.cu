@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
   const int i = g % A.M, j = g / A.M;
 
   // ---- stage the search window (column-major, stride WD) --------------------
-  const float* src = A.pad + (size_t)i * D + (size_t)j * D * A.P;
+  const float* src = A.pad + (size_t)i * A.s + (size_t)j * A.s * A.P;
   for (int c = 0; c < WD; ++c)
     for (int r = lane; r < WD; r += 32) win[r + c * WD] = src[r + (size_t)c * A.P];
   __syncwarp();
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
     }
   }
   if (A.V1 || A.V2) {
-    const float* src2 = A.pad2 + (size_t)i * D + (size_t)j * D * A.P;
+    const float* src2 = A.pad2 + (size_t)i * A.s + (size_t)j * A.s * A.P;
     for (int k = 0; k < K; ++k) {
       int e = (int)lS[k] - 1;
       if ((unsigned)e >= (unsigned)(D2 * D2)) e = H + H * D2;
@@ -325,6 +325,7 @@ bool match_supported(int d, int d2) {
 }
 
 cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st) {
+  if (A.s < 1 || A.s > d) return cudaErrorInvalidValue;
 #define GBM3D_MATCH_CASE(DD, DD2) \
   if (d == DD && d2 == DD2) return launch_match_t<DD, DD2>(A, st);
   GBM3D_MATCH_CASE(8, 16) GBM3D_MATCH_CASE(8, 24) GBM3D_MATCH_CASE(8, 32)

@@ -56,6 +56,7 @@ extern "C" int gbm3d_matchBlocks_noalloc(const float* I, int m, int n, double si
   const int d = o->blockSize, d2 = o->matchSize, K = o->numMax;
   if (o->numMin < 1 || o->numMin > K || K < 1 || K > 32 || (d2 & 1) || d2 * d2 < K) return GBM3D_ERR_ARG;
   if (!gbm3d::match_supported(d, d2)) return GBM3D_ERR_UNSUPPORTED;
+  if (o->refStride != 0 && o->refStride != d) return GBM3D_ERR_UNSUPPORTED;  // the reference's tiling only
   if (m < d2 || n < d2 || m < d || n < d) return GBM3D_ERR_ARG;
   const int P = (m + d2 + 3) & ~3;
   if ((size_t)P * (size_t)(n + d2) > (size_t)GBM3D_NOALLOC_MAX_FLOATS) return GBM3D_ERR_TOO_LARGE;
@@ -71,6 +72,7 @@ extern "C" int gbm3d_matchBlocks_noalloc(const float* I, int m, int n, double si
   A.M = m / d;
   A.N = n / d;
   A.K = K;
+  A.s = d;
   A.numMin = o->numMin;
   A.tol = (float)(0.005 * sigma * sigma * d * d);
   A.tol_branch = o->numMin != K;

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       int e = (int)A.S[(size_t)g * K + k] - 1;
       if ((unsigned)e >= (unsigned)(A.d2 * A.d2)) e = (A.d2 / 2) * (A.d2 + 1);  // never read outside the window
       const int a = e % A.d2, b = e / A.d2;
-      const size_t o = (size_t)(i * D + a) + (size_t)(j * D + b) * A.P;
+      const size_t o = (size_t)(i * A.s + a) + (size_t)(j * A.s + b) * A.P;
       for (int t = lane; t < DD; t += 32) {
         const int r = t % D, c = t / D;
         b1[k * PG + r + CS * c] = A.padP[o + r + (size_t)c * A.P];
@@ -248,6 +248,7 @@ static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
 }
 
 cudaError_t launch_wiener(int d, const WienerArgs& A, cudaStream_t st) {
+  if (A.padP && (A.s < 1 || A.s > d)) return cudaErrorInvalidValue;
 #define GBM3D_WIE_CASE(DD, KK) \
   if (d == DD && A.K == KK) return launch_wiener_t<DD, KK>(A, st);
   GBM3D_WIE_CASE(8, 16) GBM3D_WIE_CASE(8, 8) GBM3D_WIE_CASE(8, 32)

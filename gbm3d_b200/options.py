@@ -10,10 +10,12 @@ Host-side mirror of the reference's utility layer (toby-sanders/GBM3D):
   myPSNR                 utilities/myPSNR.m:7-12
 
 Options are plain dicts with the reference's field names.  Two fields exist
-only here: ``refStride`` (reference-block stride; absent or None means the
-block size, which is the reference's tiling) and ``staleWeights`` (mirror
-GBM3D.m's reuse of step-1 weight slices when step 2 has fewer spins; default
-True).
+only here: ``refStride`` / ``refStrideWie`` (reference-block stride of step 1
+/ step 2; absent or None means the block size, which is the reference's
+tiling) and ``staleWeights`` (mirror GBM3D.m's reuse of step-1 weight slices
+when step 2 has fewer spins; default True).  ``wname`` exists in the
+reference but GBM3D.m ignores it (it always uses bior1.5 x Haar); here
+``wname='haar'`` selects a 3D Haar bank for step 1.
 """
 from __future__ import annotations
 
@@ -69,11 +71,22 @@ def resolve_opts(opts: dict | None) -> dict:
     if opts is None:
         opts = {"profile": "default"}
     if "profile" in opts:
-        extra = {k: opts[k] for k in ("refStride", "staleWeights") if k in opts}
+        extra = {k: opts[k] for k in ("refStride", "refStrideWie", "staleWeights") if k in opts}
         o = setBM3Dopts(opts["profile"])
         o.update(extra)
         opts = o
     return checkBM3Dopts(opts)
+
+
+def strides(opts: dict) -> tuple[int, int]:
+    """(step-1, step-2) reference strides; None or absent means the block size."""
+    s1, s2 = opts.get("refStride"), opts.get("refStrideWie")
+    return (int(s1) if s1 else int(opts["blockSize"]), int(s2) if s2 else int(opts["blockSizeWie"]))
+
+
+def grid_count(L: int, d: int, s: int) -> int:
+    """References along an axis of L pixels at stride s: floor((L-d)/s)+1."""
+    return (L - d) // s + 1
 
 
 def getTau(levels: int, mode: int = 1) -> np.ndarray:

@@ -48,7 +48,9 @@ typedef struct gbm3d_ctx gbm3d_ctx;
 
 /* Option struct with the reference's field names (utilities/setBM3Dopts.m:17-86,
  * utilities/checkBM3Dopts.m:10-24).  filtType: 0 = 'ht', 1 = 'median'.
- * refStride: reference-block spacing; 0 means blockSize (the reference's tiling).
+ * refStride / refStrideWie: reference-block spacing of step 1 / step 2; 0 means
+ * blockSize / blockSizeWie (the reference's tiling).  Not in the reference; with
+ * stride s the references sit at 0, s, 2s, ... and M = floor((m-d)/s)+1.
  * staleWeights: 1 mirrors GBM3D.m:26-27,82 (step 2 reuses the step-1 weight
  * slices it does not overwrite). */
 typedef struct gbm3d_opts {
@@ -59,6 +61,8 @@ typedef struct gbm3d_opts {
   int nMatchSpins, matchSpins[8];
   int nMatchSpinsWie, matchSpinsWie[8];
   int staleWeights;
+  int refStrideWie;
+  int wavelet; /* step-1 bank of gbm3d_denoise: 0 = bior1.5 x Haar (GBM3D.m:40), 1 = 3D Haar */
 } gbm3d_opts;
 
 /* Separable 3D wavelet bank: 1D analysis (a_) and synthesis (s_) filters for the
@@ -92,8 +96,10 @@ void gbm3d_bior_filters(gbm3d_filters* out);
 /* ---- the reference's hot-path functions -------------------------------------- */
 
 /* [S,Volume] = matchBlocksCPU(I,sigma,opts)           source/matchBlocksCPU.m:1-116
- * I: m x n double.  S: K x M x N, M=floor(m/d), N=floor(n/d).  S_count: M x N or
- * NULL.  Volume: m x n x K single, or NULL to skip the gather. */
+ * I: m x n double.  S: K x M x N, M=floor((m-d)/s)+1, N=floor((n-d)/s)+1 with
+ * s = refStride (M = floor(m/d) for s = d).  S_count: M x N or NULL.  Volume:
+ * m x n x K single for s = d, (M*d) x (N*d) x K otherwise, or NULL to skip
+ * the gather. */
 int gbm3d_matchBlocksCPU(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
                          const gbm3d_opts* opts, uint32_t* S, int32_t* S_count, float* Volume);
 
@@ -109,7 +115,7 @@ int gbm3d_matchBlocksGPU(gbm3d_ctx* ctx, const double* I, int m, int n, double s
 /* [U,W] = denoiseAndAggregateGPU(Volume,S,tau,Psi,Psi2,opts)   source/denoiseAndAggregateGPU.m:1-92
  * Volume: (M*d) x (N*d) x K single; S: K x M x N; S_count may be NULL;
  * tau: levels x 7 double; filters: the separable factors of Psi/Psi2.
- * U, W: (M*d) x (N*d) double. */
+ * U, W: ((M-1)*s+d) x ((N-1)*s+d) double, s = refStride (M*d x N*d for s = d). */
 int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* ctx, const float* Volume, const uint32_t* S,
                                  const int32_t* S_count, int M, int N, const double* tau,
                                  const gbm3d_filters* filters, const gbm3d_opts* opts,
@@ -117,12 +123,13 @@ int gbm3d_denoiseAndAggregateGPU(gbm3d_ctx* ctx, const float* Volume, const uint
 
 /* [S,V1,V2] = matchBlocksWie(I,In,sigma,opts)            source/matchBlocksWie.m:1-92
  * I (pilot) and In (noisy): m x n double.  V1, V2: d x d x K x M x N single
- * (either may be NULL). */
+ * (either may be NULL), M=floor((m-d)/s)+1 with s = refStrideWie. */
 int gbm3d_matchBlocksWie(gbm3d_ctx* ctx, const double* I, const double* In, int m, int n,
                          double sigma, const gbm3d_opts* opts, uint32_t* S, float* V1, float* V2);
 
 /* [U,W] = denoiseAndAggregateWieFast(V1,V2,S,sigma,opts)  source/denoiseAndAggregateWieFast.m:1-100
- * sigma: one double, or d x d doubles when sigma_is_matrix (broadcast over slots). */
+ * sigma: one double, or d x d doubles when sigma_is_matrix (broadcast over slots).
+ * U, W: ((M-1)*s+d) x ((N-1)*s+d) double, s = refStrideWie. */
 int gbm3d_denoiseAndAggregateWieFast(gbm3d_ctx* ctx, const float* V1, const float* V2,
                                      const uint32_t* S, int M, int N, const double* sigma,
                                      int sigma_is_matrix, const gbm3d_opts* opts,

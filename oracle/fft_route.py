@@ -44,30 +44,34 @@ def _block_norms(X, d, shape):
     return np.real(np.fft.ifft2(np.conj(np.fft.fft2(g)) * np.fft.fft2(X ** 2)))
 
 
-def match_blocks(I, d, d2, K, In=None):
+def match_blocks(I, d, d2, K, In=None, st=None):
     """matchBlocksCPU.m:21-116 (top-K branch) / matchBlocksWie.m:21-92.
 
     Returns S (K, M, N) uint32, Volume (m, n, K) and, with In, V1/V2 (d,d,K,M,N).
+    st: reference stride (default d, the reference's tiling); with st != d the
+    references sit at i*st, M = (m-d)//st + 1 and Volume is (M d, N d, K).
     """
     I = np.asarray(I, dtype=np.float64)
     m, n = I.shape
-    M, N = m // d, n // d
+    st = st or d
+    M, N = (m - d) // st + 1, (n - d) // st + 1
     h = d2 // 2
     Ipad = _search_pad(I, d2)
     Ipad2 = _search_pad(np.asarray(In, dtype=np.float64), d2) if In is not None else None
     bn = _block_norms(I, d, (m, n))
     bnp = _block_norms(Ipad, d, (m + d2, n + d2))
     S = np.zeros((K, M, N), dtype=np.uint32)
-    Vol = np.zeros((m, n, K))
+    Vol = np.zeros((m, n, K) if st == d else (M * d, N * d, K))
     V1 = np.zeros((d, d, K, M, N)) if In is not None else None
     V2 = np.zeros_like(V1) if In is not None else None
     for i in range(M):
         for j in range(N):
-            xR = I[i * d:(i + 1) * d, j * d:(j + 1) * d]
-            It = Ipad[i * d:i * d + d + d2, j * d:j * d + d + d2]
+            y0, x0 = i * st, j * st
+            xR = I[y0:y0 + d, x0:x0 + d]
+            It = Ipad[y0:y0 + d + d2, x0:x0 + d + d2]
             cc = np.real(np.fft.ifft2(np.conj(np.fft.fft2(_pad_to(xR, (d + d2, d + d2)))) * np.fft.fft2(It)))
-            nr = bn[i * d, j * d]
-            D = (nr + bnp[i * d:i * d + d2, j * d:j * d + d2] - 2 * cc[:d2, :d2]) / nr
+            nr = bn[y0, x0]
+            D = (nr + bnp[y0:y0 + d2, x0:x0 + d2] - 2 * cc[:d2, :d2]) / nr
             idx = np.argsort(D.ravel(order="F"), kind="stable")[:K]  # mink
             s = (idx + 1).astype(np.uint32)
             s[0] = d2 * d2 // 2 + h + 1
@@ -77,7 +81,7 @@ def match_blocks(I, d, d2, K, In=None):
                 Vol[i * d:(i + 1) * d, j * d:(j + 1) * d, k] = It[a:a + d, b:b + d]
                 if In is not None:
                     V1[:, :, k, i, j] = It[a:a + d, b:b + d]
-                    V2[:, :, k, i, j] = Ipad2[i * d:i * d + d + d2, j * d:j * d + d + d2][a:a + d, b:b + d]
+                    V2[:, :, k, i, j] = Ipad2[y0:y0 + d + d2, x0:x0 + d + d2][a:a + d, b:b + d]
     return S, Vol, V1, V2
 
 
@@ -127,9 +131,11 @@ def sine_window(d, lo, hi):
     return np.outer(v, v)
 
 
-def denoise_ht(Volume, S, tau, Psi, Psi2, d, d2, levels, cycle_spin):
-    """denoiseAndAggregateGPU.m:11-92 (filtType 'ht')."""
+def denoise_ht(Volume, S, tau, Psi, Psi2, d, d2, levels, cycle_spin, st=None):
+    """denoiseAndAggregateGPU.m:11-92 (filtType 'ht'); st: reference stride
+    (Volume is (M d, N d, K); output ((M-1) st + d, (N-1) st + d))."""
     K, M, N = S.shape
+    st = st or d
     m, n = M * d, N * d
     Vrec = np.zeros((m, n, K, cycle_spin))
     for spin in range(cycle_spin):
@@ -140,7 +146,8 @@ def denoise_ht(Volume, S, tau, Psi, Psi2, d, d2, levels, cycle_spin):
                 C[i, j] = C[i, j] * (np.abs(C[i, j]) > tau[i, j])
         Vrec[..., spin] = _circshift(wav_rec3(Psi2, levels, C), (-spin, -spin, -spin))
     Vavg = np.maximum(Vrec.mean(axis=3), 0)
-    U = np.zeros((m + d2, n + d2))
+    mo, no = (M - 1) * st + d, (N - 1) * st + d
+    U = np.zeros((mo + d2, no + d2))
     W = np.zeros_like(U)
     mask = sine_window(d, 0.1, 0.9)
     for y in range(M):
@@ -148,11 +155,11 @@ def denoise_ht(Volume, S, tau, Psi, Psi2, d, d2, levels, cycle_spin):
             blocks = Vavg[y * d:(y + 1) * d, x * d:(x + 1) * d, :K]
             wt = 1.0 / (agg_weight(blocks) + np.finfo(float).eps)
             for i in range(K):
-                a, b = (int(S[i, y, x]) - 1) % d2 + y * d, (int(S[i, y, x]) - 1) // d2 + x * d
+                a, b = (int(S[i, y, x]) - 1) % d2 + y * st, (int(S[i, y, x]) - 1) // d2 + x * st
                 U[a:a + d, b:b + d] += wt * blocks[:, :, i] * mask
                 W[a:a + d, b:b + d] += wt * mask
     h = d2 // 2
-    return U[h:m + h, h:n + h], W[h:m + h, h:n + h]
+    return U[h:mo + h, h:no + h], W[h:mo + h, h:no + h]
 
 
 def _dec1d(Psi, Phi, levels, U):
@@ -206,10 +213,11 @@ def dct_matrix(d):
     return T
 
 
-def denoise_wiener(V1, V2, S, sigma, d2, variant=0):
+def denoise_wiener(V1, V2, S, sigma, d2, variant=0, st=None):
     """denoiseAndAggregateWieFast.m:23-100 (variant 0) / denoiseAndAggregateWie.m (variant 1)."""
     d, _, K, M, N = V1.shape
-    m, n = M * d, N * d
+    st = st or d
+    m, n = (M - 1) * st + d, (N - 1) * st + d
     levels = 2 if K < 16 else 3
     cc = np.sqrt(2.0) / 2
     Psi, Phi = np.array([-cc, cc]), np.array([cc, cc])
@@ -236,11 +244,24 @@ def denoise_wiener(V1, V2, S, sigma, d2, variant=0):
         for x in range(N):
             wt = w / np.linalg.norm(filt[:, :, :, y, x].ravel()) ** 2
             for i in range(K):
-                a, b = (int(S[i, y, x]) - 1) % d2 + y * d, (int(S[i, y, x]) - 1) // d2 + x * d
+                a, b = (int(S[i, y, x]) - 1) % d2 + y * st, (int(S[i, y, x]) - 1) // d2 + x * st
                 U[a:a + d, b:b + d] += wt * B[:, :, i, y, x]
                 W[a:a + d, b:b + d] += wt
     h = d2 // 2
     return U[h:m + h, h:n + h], W[h:m + h, h:n + h]
+
+
+def padded_size(L, opts):
+    """GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
+    smallest size at which both steps' references end exactly at the border."""
+    d, dw = opts["blockSize"], opts["blockSizeWie"]
+    st1, st2 = opts.get("refStride") or d, opts.get("refStrideWie") or dw
+    if st1 == d and (not opts["Wiener"] or (st2 == dw and d % dw == 0)):
+        return -(-L // d) * d
+    p = max(L, d, dw)
+    while (p - d) % st1 or (opts["Wiener"] and (p - dw) % st2):
+        p += 1
+    return p
 
 
 def gbm3d(I, sigma, opts, Psi, Psi2, tau_unit):
@@ -248,7 +269,8 @@ def gbm3d(I, sigma, opts, Psi, Psi2, tau_unit):
     I = np.asarray(I, dtype=np.float64)
     m, n = I.shape
     d, dw, d2, K = opts["blockSize"], opts["blockSizeWie"], opts["matchSize"], opts["numMax"]
-    Mp, Np = -(-m // d) * d, -(-n // d) * d
+    st1, st2 = opts.get("refStride") or d, opts.get("refStrideWie") or dw
+    Mp, Np = padded_size(m, opts), padded_size(n, opts)
     Ip = np.zeros((Mp, Np))
     Ip[:m, :n] = I
     Ip[m:, :n] = np.flipud(I[m - (Mp - m):m, :n])
@@ -259,8 +281,8 @@ def gbm3d(I, sigma, opts, Psi, Psi2, tau_unit):
     U1s = np.zeros((Mp, Np, nS))
     Ws = np.zeros((Mp, Np, max(nS, nW)))
     for ii, s in enumerate(opts["matchSpins"]):
-        S, Vol, _, _ = match_blocks(_circshift(Ip, (s, s)), d, d2, K)
-        u, w = denoise_ht(Vol, S, tau, Psi, Psi2, d, d2, opts["levels"], opts["cycleSpin"])
+        S, Vol, _, _ = match_blocks(_circshift(Ip, (s, s)), d, d2, K, st=st1)
+        u, w = denoise_ht(Vol, S, tau, Psi, Psi2, d, d2, opts["levels"], opts["cycleSpin"], st=st1)
         U1s[..., ii] = _circshift(u, (-s, -s))
         Ws[..., ii] = _circshift(w, (-s, -s))
     U1 = U1s.sum(axis=2) / Ws[..., :nS].sum(axis=2)
@@ -268,8 +290,8 @@ def gbm3d(I, sigma, opts, Psi, Psi2, tau_unit):
         return U1[:m, :n], U1[:m, :n]
     Us = np.zeros((Mp, Np, max(nS, nW)))
     for ii, s in enumerate(opts["matchSpinsWie"]):
-        S, _, V1, V2 = match_blocks(_circshift(U1, (s, s)), dw, d2, K, In=_circshift(Ip, (s, s)))
-        u, w = denoise_wiener(V1, V2, S, sigma, d2)
+        S, _, V1, V2 = match_blocks(_circshift(U1, (s, s)), dw, d2, K, In=_circshift(Ip, (s, s)), st=st2)
+        u, w = denoise_wiener(V1, V2, S, sigma, d2, st=st2)
         Us[..., ii] = _circshift(u, (-s, -s))
         Ws[..., ii] = _circshift(w, (-s, -s))
     U = Us.sum(axis=2) / Ws.sum(axis=2)

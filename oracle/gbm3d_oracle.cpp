@@ -141,6 +141,7 @@ typedef struct {
   int staleWeights;  // GBM3D.m:26-27,82 slice-reuse behaviour (1 = mirror it)
   int filtType;      // 0 'ht', 1 'median' (denoiseAndAggregateGPU.m:135,165)
   int refStride, refStrideWie;  // reference spacing per step; 0 = block size (the reference)
+  int wavelet;                  // step-1 bank: 0 = bior1.5 x Haar (GBM3D.m:40), 1 = 3D Haar
 } orc_opts;
 
 }  // extern "C"
@@ -773,6 +774,20 @@ void bior_filters(orc_filters* f) {
   f->s_lo_z[0] = Cc; f->s_lo_z[1] = Cc; f->s_hi_z[0] = -Cc; f->s_hi_z[1] = Cc;
 }
 
+// 3D Haar bank: the two-tap Haar pair on the spatial axes as well as the slot axis.
+void haar_filters(orc_filters* f) {
+  std::memset(f, 0, sizeof(*f));
+  const double Cc = std::sqrt(2.0) / 2;
+  f->len_xy = 2;
+  f->len_z = 2;
+  double* lo[4] = {f->a_lo_xy, f->s_lo_xy, f->a_lo_z, f->s_lo_z};
+  double* hi[4] = {f->a_hi_xy, f->s_hi_xy, f->a_hi_z, f->s_hi_z};
+  for (int q = 0; q < 4; ++q) {
+    lo[q][0] = Cc; lo[q][1] = Cc;
+    hi[q][0] = -Cc; hi[q][1] = Cc;
+  }
+}
+
 // GBM3D.m:15-83
 template <class T>
 void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, double* Uout, double* U1out) {
@@ -794,7 +809,8 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
   get_tau(o->levels, o->tauMode, tau.data());
   for (auto& t : tau) t *= sigma;
   orc_filters f;
-  bior_filters(&f);
+  if (o->wavelet == 1) haar_filters(&f);
+  else bior_filters(&f);
   const int nS = o->nSpins, nW = o->nSpinsWie, nslice = std::max(nS, nW);
   std::vector<double> Us((size_t)nslice * px, 0.0), Ws((size_t)nslice * px, 0.0), U1s((size_t)nS * px, 0.0);
   std::vector<double> sh(px), u(px), w(px);

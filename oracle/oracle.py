@@ -52,7 +52,7 @@ class orc_opts(C.Structure):
         ("nSpins", C.c_int), ("spins", C.c_int * 8),
         ("nSpinsWie", C.c_int), ("spinsWie", C.c_int * 8),
         ("staleWeights", C.c_int), ("filtType", C.c_int),
-        ("refStride", C.c_int), ("refStrideWie", C.c_int),
+        ("refStride", C.c_int), ("refStrideWie", C.c_int), ("wavelet", C.c_int),
     ]
 
 
@@ -245,6 +245,7 @@ def make_opts(o: dict) -> orc_opts:
     c.filtType = 1 if o.get("filtType", "ht") == "median" else 0
     c.refStride = int(o.get("refStride") or 0)
     c.refStrideWie = int(o.get("refStrideWie") or 0)
+    c.wavelet = 1 if o.get("wname", "bior") == "haar" else 0
     return c
 
 

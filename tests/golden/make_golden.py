@@ -10,6 +10,7 @@ inputs and, per stage, the outputs of the reference function with that name.
 """
 from __future__ import annotations
 
+import json
 import os
 import sys
 
@@ -35,31 +36,40 @@ def banks(fac):
     return P, P2
 
 
+# patch 8, reference stride 3, group 16, search +-12 (matchSize 24)
+STRIDE3 = dict(blockSize=8, blockSizeWie=8, matchSize=24, refStride=3, refStrideWie=3)
+
 CASES = [
-    # name, m, n, sigma, seed, profile, wavelet
-    ("default_64x96_s25", 64, 96, 25.0, 3, "default", "bior"),
-    ("default_70x90_s10", 70, 90, 10.0, 5, "default", "bior"),
-    ("fast_64x64_s50", 64, 64, 50.0, 7, "fast", "bior"),
-    ("haar_64x64_s25", 64, 64, 25.0, 11, "default", "haar"),
+    # name, m, n, sigma, seed, profile, wavelet, option overrides
+    ("default_64x96_s25", 64, 96, 25.0, 3, "default", "bior", {}),
+    ("default_70x90_s10", 70, 90, 10.0, 5, "default", "bior", {}),
+    ("fast_64x64_s50", 64, 64, 50.0, 7, "fast", "bior", {}),
+    ("haar_64x64_s25", 64, 64, 25.0, 11, "default", "haar", {}),
+    ("stride3_50x58_s25", 50, 58, 25.0, 31, "default", "bior", STRIDE3),
+    ("stride3haar_40x48_s10", 40, 48, 10.0, 32, "default", "haar", STRIDE3),
 ]
 
 
-def make(name, m, n, sigma, seed, profile, wav):
+def make(name, m, n, sigma, seed, profile, wav, over):
     clean, noisy = synth.noisy_image(m, n, sigma, seed=seed)
     opts = options.resolve_opts({"profile": profile})
+    opts.update(over)
     fac = options.bior_factors() if wav == "bior" else options.haar_factors()
     P, P2 = banks(fac)
     tau_unit = options.getTau(opts["levels"], opts["tauMode"])
     d, dw, d2, K = opts["blockSize"], opts["blockSizeWie"], opts["matchSize"], opts["numMax"]
+    st1, st2 = opts.get("refStride") or d, opts.get("refStrideWie") or dw
     out = dict(clean=clean, noisy=noisy, sigma=sigma, profile=profile, wavelet=wav)
-    # stage tests on the unpadded image size multiple of d
-    Mp, Np = -(-m // d) * d, -(-n // d) * d
+    if over:
+        out["opts"] = json.dumps(over, sort_keys=True)
+    # stage tests on the image padded as the pipeline pads it
+    Mp, Np = F.padded_size(m, opts), F.padded_size(n, opts)
     Ip = options.myMirrorPadImage(noisy, Mp, Np)
-    S1, Vol, _, _ = F.match_blocks(Ip, d, d2, K)
-    U1, W1 = F.denoise_ht(Vol, S1, sigma * tau_unit, P, P2, d, d2, opts["levels"], opts["cycleSpin"])
+    S1, Vol, _, _ = F.match_blocks(Ip, d, d2, K, st=st1)
+    U1, W1 = F.denoise_ht(Vol, S1, sigma * tau_unit, P, P2, d, d2, opts["levels"], opts["cycleSpin"], st=st1)
     pilot = U1 / W1
-    S2, _, V1, V2 = F.match_blocks(pilot, dw, d2, K, In=Ip)
-    U2, W2 = F.denoise_wiener(V1, V2, S2, sigma, d2)
+    S2, _, V1, V2 = F.match_blocks(pilot, dw, d2, K, In=Ip, st=st2)
+    U2, W2 = F.denoise_wiener(V1, V2, S2, sigma, d2, st=st2)
     out.update(padded=Ip, S1=S1, U1=U1, W1=W1, pilot=pilot, S2=S2, U2=U2, W2=W2)
     if wav == "bior":
         U, Ustep1 = F.gbm3d(noisy, sigma, opts, P, P2, tau_unit)
@@ -87,8 +97,12 @@ def check_sym4_data():
 
 
 if __name__ == "__main__":
+    only = sys.argv[1:]  # optional case names; default: all
     for c in CASES:
-        make(*c)
+        if not only or c[0] in only:
+            make(*c)
+    if only:
+        sys.exit(0)
     make_global("global_64x64_s25", 64, 64, 25.0, 21)
     make_global("global_48x64_s01", 48, 64, 0.1, 22)
     check_sym4_data()

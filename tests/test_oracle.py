@@ -6,6 +6,7 @@ same functions by direct arithmetic.  Agreement to ~1e-9 relative in FP64 with
 identical match sets pins the two restatements to each other.
 """
 import glob
+import json
 import os
 
 import numpy as np
@@ -28,11 +29,19 @@ def _filters(O, wav):
     return O.bior_filters() if wav == "bior" else O.haar_filters()
 
 
+def _opts(g):
+    """The fixture's profile plus its option overrides (stride cases)."""
+    o = options.resolve_opts({"profile": str(g["profile"])})
+    if "opts" in g:
+        o.update(json.loads(str(g["opts"])))
+    return o
+
+
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
 def test_oracle_matches_golden_stages(oracle, path):
     g = _load(path)
     O = oracle
-    opts = options.resolve_opts({"profile": str(g["profile"])})
+    opts = _opts(g)
     sigma = float(g["sigma"])
     f = _filters(O, str(g["wavelet"]))
     S1, Vol, cnt = O.matchBlocksCPU(g["padded"], sigma, opts, prec=64)
@@ -52,7 +61,7 @@ def test_oracle_matches_golden_stages(oracle, path):
                          ids=[os.path.basename(p)[:-4] for p in GOLDEN if "haar" not in p])
 def test_oracle_matches_golden_pipeline(oracle, path):
     g = _load(path)
-    opts = options.resolve_opts({"profile": str(g["profile"])})
+    opts = _opts(g)
     U, U1 = oracle.GBM3D(g["noisy"], float(g["sigma"]), opts, prec=64)
     assert max_abs(U1, g["Ustep1"]) <= 1e-9
     assert max_abs(U, g["U"]) <= 1e-9
