@@ -71,6 +71,7 @@ _SIGS = {
     "gbm3d_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "gbm3d_stage_times": (C.c_int, [_P, _P, C.c_int]),
     "gbm3d_last_launch_count": (C.c_int, [_P]),
+    "gbm3d_kernel_time": (C.c_int, [_P, C.c_char_p, _P]),
     "gbm3d_matchBlocks_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P, _P]),
 }
 
@@ -139,6 +140,12 @@ class Context:
 
     def launch_count(self) -> int:
         return int(lib().gbm3d_last_launch_count(self.h))
+
+    def kernel_time(self, name: str) -> tuple[int, float]:
+        """(launches, total ms) of one kernel family in the last timed call."""
+        t = C.c_float(0.0)
+        n = lib().gbm3d_kernel_time(self.h, name.encode(), C.byref(t))
+        return int(n), float(t.value)
 
 
 _ctx: dict[int, Context] = {}

@@ -33,6 +33,11 @@ struct gbm3d_ctx {
   bool timing = false;
   std::vector<cudaEvent_t> evpool;           // events reused across calls
   std::vector<std::pair<int, int>> records;  // (stage, index of start event; end = +1)
+  // per-launch timing: kpool[0] marks the call's start, kpool[i] is recorded
+  // right after launch i (krec[i-1] names it), so on the in-order stream the
+  // launch's device time is elapsed(kpool[i-1], kpool[i])
+  std::vector<cudaEvent_t> kpool;
+  std::vector<std::string> krec;
   int launches = 0;
   int* flag = nullptr;  // device status word (non-finite input)
 };
@@ -74,9 +79,22 @@ T* buf(gbm3d_ctx* c, const char* name, size_t count) {
   return reinterpret_cast<T*>(p);
 }
 
+void kevent(gbm3d_ctx* c, size_t idx) {
+  while (c->kpool.size() <= idx) {
+    cudaEvent_t e;
+    ck(c, cudaEventCreate(&e), "cudaEventCreate");
+    c->kpool.push_back(e);
+  }
+  ck(c, cudaEventRecord(c->kpool[idx], c->st), "cudaEventRecord");
+}
+
 void launched(gbm3d_ctx* c, cudaError_t e, const char* what) {
   ck(c, e, what);
   ++c->launches;
+  if (c->timing) {
+    c->krec.push_back(what);
+    kevent(c, c->krec.size());
+  }
 }
 
 // Stage timer: records a start/end event pair on the stream when timing is on.
@@ -509,6 +527,8 @@ int guarded(gbm3d_ctx* c, F&& f) {
     ck(c, cudaSetDevice(c->device), "cudaSetDevice");
     c->launches = 0;
     c->records.clear();
+    c->krec.clear();
+    if (c->timing) kevent(c, 0);
     f();
     return GBM3D_OK;
   } catch (const Fail& e) {
@@ -710,6 +730,23 @@ int gbm3d_stage_times(const gbm3d_ctx* c, float* ms, int n) {
 }
 
 int gbm3d_last_launch_count(const gbm3d_ctx* c) { return c ? c->launches : 0; }
+
+int gbm3d_kernel_time(const gbm3d_ctx* c, const char* name, float* total_ms) {
+  if (!c || !name || !total_ms || !c->timing) return -1;
+  float acc = 0.f;
+  int n = 0;
+  for (size_t i = 0; i < c->krec.size(); ++i) {
+    if (c->krec[i] != name) continue;
+    float t = 0.f;
+    if (cudaEventSynchronize(c->kpool[i + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&t, c->kpool[i], c->kpool[i + 1]) != cudaSuccess)
+      return -1;
+    acc += t;
+    ++n;
+  }
+  *total_ms = acc;
+  return n;
+}
 
 void gbm3d_default_opts(const char* profile, gbm3d_opts* o) {
   if (!o) return;

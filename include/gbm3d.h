@@ -163,6 +163,13 @@ int gbm3d_stage_times(const gbm3d_ctx* ctx, float* ms, int n);
 /* Number of kernels the last pipeline call launched. */
 int gbm3d_last_launch_count(const gbm3d_ctx* ctx);
 
+/* With timing on: device time (ms) summed over the last call's launches of
+ * the kernel family `name` ("match", "wav_analysis", "wav_synthesis",
+ * "aggregate", "wiener", "ht_weights", "make_pad", "accum", "ratio", "prep",
+ * ...), measured between CUDA events recorded after consecutive launches on
+ * the context stream.  Returns the number of such launches, or -1. */
+int gbm3d_kernel_time(const gbm3d_ctx* ctx, const char* name, float* total_ms);
+
 /* Step-1 block matching that allocates nothing.  No counterpart in the
  * reference: it exists for callers that may not allocate device memory while
  * they run (servers and video pipelines that reserve all GPU memory at
