@@ -792,6 +792,79 @@ void gbm3d_bior_filters(gbm3d_filters* f) {
   if (f) bior(f);
 }
 
+// Psi / Psi2 (Ly x Lx x Lz x 8, column-major; band order LLL, HLL, LHL, LLH,
+// HHL, HLH, LHH, HHH over (y, x, z), getWaveFilters3Dbior.m:39-58) back to
+// separable 1D factors.  Known banks (bior1.5 x Haar, 3D Haar) are recognised
+// to 1e-5 and returned exactly; any other separable bank is split at its
+// largest |LLL| entry (a, a, c): lo = LLL(:,a,c)/LLL(a,a,c), vlo = LLL(a,a,:),
+// hi = HLL(:,a,c)/vlo(c), vhi = LLH(a,a,:), and must rebuild Psi to 1e-4.
+static void bank_of(const gbm3d_filters& f, int which, std::vector<double>& B) {
+  const int L = f.len_xy, Lz = f.len_z;
+  const double* xy[2] = {which ? f.s_lo_xy : f.a_lo_xy, which ? f.s_hi_xy : f.a_hi_xy};
+  const double* z[2] = {which ? f.s_lo_z : f.a_lo_z, which ? f.s_hi_z : f.a_hi_z};
+  static const int ord[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+  B.assign((size_t)L * L * Lz * 8, 0.0);
+  for (int b = 0; b < 8; ++b)
+    for (int zz = 0; zz < Lz; ++zz)
+      for (int x = 0; x < L; ++x)
+        for (int y = 0; y < L; ++y)
+          B[y + (size_t)L * (x + (size_t)L * (zz + (size_t)Lz * b))] = xy[ord[b][0]][y] * xy[ord[b][1]][x] * z[ord[b][2]][zz];
+}
+
+static double bank_err(const gbm3d_filters& f, const float* Psi, const float* Psi2) {
+  std::vector<double> B;
+  double e = 0.0;
+  for (int w = 0; w < 2; ++w) {
+    bank_of(f, w, B);
+    const float* P = w ? Psi2 : Psi;
+    for (size_t i = 0; i < B.size(); ++i) e = std::max(e, std::fabs(B[i] - (double)P[i]));
+  }
+  return e;
+}
+
+int gbm3d_filters_from_bank(const float* Psi, const float* Psi2, int L, int Lz, gbm3d_filters* out) {
+  if (!Psi || !Psi2 || !out || L < 1 || L > 16 || Lz < 1 || Lz > 16) return GBM3D_ERR_ARG;
+  gbm3d_filters f;
+  bior(&f);
+  if (f.len_xy == L && f.len_z == Lz && bank_err(f, Psi, Psi2) <= 1e-5) { *out = f; return GBM3D_OK; }
+  haar3d(&f);
+  if (f.len_xy == L && f.len_z == Lz && bank_err(f, Psi, Psi2) <= 1e-5) { *out = f; return GBM3D_OK; }
+  std::memset(&f, 0, sizeof(f));
+  f.len_xy = L;
+  f.len_z = Lz;
+  const size_t band = (size_t)L * L * Lz;
+  for (int w = 0; w < 2; ++w) {
+    const float* P = w ? Psi2 : Psi;
+    int a = 0, c = 0;
+    double best = -1.0;
+    for (int zz = 0; zz < Lz; ++zz)
+      for (int x = 0; x < L; ++x)
+        for (int y = 0; y < L; ++y) {
+          const double v = std::fabs((double)P[y + (size_t)L * (x + (size_t)L * zz)]);
+          if (v > best) { best = v; a = y; c = zz; }
+        }
+    auto at = [&](int b, int y, int x, int zz) { return (double)P[y + (size_t)L * (x + (size_t)L * zz) + band * b]; };
+    const double piv = at(0, a, a, c);
+    if (piv == 0.0) return GBM3D_ERR_ARG;
+    double* lo = w ? f.s_lo_xy : f.a_lo_xy;
+    double* hi = w ? f.s_hi_xy : f.a_hi_xy;
+    double* vlo = w ? f.s_lo_z : f.a_lo_z;
+    double* vhi = w ? f.s_hi_z : f.a_hi_z;
+    for (int zz = 0; zz < Lz; ++zz) {
+      vlo[zz] = at(0, a, a, zz);
+      vhi[zz] = at(3, a, a, zz);
+    }
+    if (vlo[c] == 0.0) return GBM3D_ERR_ARG;
+    for (int y = 0; y < L; ++y) {
+      lo[y] = at(0, y, a, c) / piv;
+      hi[y] = at(1, y, a, c) / vlo[c];
+    }
+  }
+  if (bank_err(f, Psi, Psi2) > 1e-4) return GBM3D_ERR_ARG;  // not separable
+  *out = f;
+  return GBM3D_OK;
+}
+
 int gbm3d_matchBlocksCPU(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
                          uint32_t* S, int32_t* S_count, float* Volume) {
   return guarded(c, [&] {

@@ -93,6 +93,12 @@ void gbm3d_default_opts(const char* profile, gbm3d_opts* out);
 void gbm3d_get_tau(int levels, int mode, double* tau /* levels x 7 */);
 void gbm3d_bior_filters(gbm3d_filters* out);
 
+/* Separable factors of a Psi/Psi2 pair (single, Ly x Lx x Lz x 8 column-major,
+ * the arguments denoiseAndAggregateGPU.m receives).  Host-only, no device
+ * needed.  Returns GBM3D_ERR_ARG for a bank that is not an outer product of
+ * 1D filters (every bank of the reference is). */
+int gbm3d_filters_from_bank(const float* Psi, const float* Psi2, int len_xy, int len_z, gbm3d_filters* out);
+
 /* ---- the reference's hot-path functions -------------------------------------- */
 
 /* [S,Volume] = matchBlocksCPU(I,sigma,opts)           source/matchBlocksCPU.m:1-116
