@@ -139,14 +139,17 @@ def test_filters_from_bank_host_only():
 # ---- on the GPU ---------------------------------------------------------------------
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kw", [{}, {"numMin": 4}, {"blockSize": 8, "refStride": 3, "matchSize": 24}])
-def test_matchBlocksCPU_gateway(gw, kw):
+@pytest.mark.parametrize("sigma,kw", [(10.0, {}), (0.01, {"numMin": 4}),
+                                      (10.0, {"blockSize": 8, "refStride": 3, "matchSize": 24})])
+def test_matchBlocksCPU_gateway(gw, sigma, kw):
+    """sigma 0.01 with numMin 4: the tolerance 0.005 sigma^2 d^2 admits only the
+    reference itself, so every cell is cut to numMin entries."""
     from gbm3d_b200 import api
     _, noisy = synth.noisy_image(64, 80, 10.0, seed=41)
     o, mo = _opts(**kw)
-    C, V = gw["matchBlocksCPU"](noisy, 10.0, mo, nargout=2)
+    C, V = gw["matchBlocksCPU"](noisy, sigma, mo, nargout=2)
     S, cnt = _cell_to_set(C, o["numMax"])
-    Sa, Va = api.matchBlocksCPU(noisy, 10.0, o)
+    Sa, Va = api.matchBlocksCPU(noisy, sigma, o)
     assert np.array_equal(cnt, Sa.count) and np.array_equal(S, np.asarray(Sa)) and np.array_equal(V, Va)
     if o["numMin"] < o["numMax"]:
         assert (cnt < o["numMax"]).any(), "the tolerance branch should shorten some cells"
