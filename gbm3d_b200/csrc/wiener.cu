@@ -77,11 +77,13 @@ __device__ __forceinline__ void haar_rec(float* v, float cc) {
 template <int D, int K>
 __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   constexpr int DD = D * D, GS = DD * K;
-  // shared layout of one group: element (r, c) of slot k at k*PG + r + CS*c.
-  // Column stride d+1 and page stride d(d+1) keep every access pattern below
-  // (rows of a page, columns of a page, one coefficient across slots) free
-  // of bank conflicts.
-  constexpr int CS = D + 1, PG = D * CS, GSP = PG * K;
+  // shared layout of one group: element (r, c) of slot page k at k*PG + r + D*c
+  // (column-major pages).  The page stride D*D + D puts the 32/D pages a warp
+  // touches at once on distinct bank groups, so row accesses (lane = (page,
+  // row)), coefficient accesses (lane = element) and 16-byte column reads are
+  // free of bank conflicts.
+  constexpr int PG = DD + D, GSP = PG * K;
+  constexpr int RPG = 32 / D;  // pages per 32-task round
   extern __shared__ float sm[];
   float* Tm = sm;
   float* Ti = sm + DD;
@@ -99,6 +101,14 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   const int g = blockIdx.x * 4 + warp;
   if (g >= A.M * A.N) return;
   const float cc = 0.70710678118654752440f;
+  // every task a lane runs has row r = lane % D (rounds of 32 tasks hold whole pages)
+  const int r = lane % D, kq = lane / D;
+  float Trow[D], Tirow[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    Trow[j] = Tm[r + j * D];
+    Tirow[j] = Ti[r + j * D];
+  }
 
   // ---- load the two groups -----------------------------------------------
   if (A.padP) {
@@ -109,35 +119,42 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       const int a = e % A.d2, b = e / A.d2;
       const size_t o = (size_t)(i * A.s + a) + (size_t)(j * A.s + b) * A.P;
       for (int t = lane; t < DD; t += 32) {
-        const int r = t % D, c = t / D;
-        b1[k * PG + r + CS * c] = A.padP[o + r + (size_t)c * A.P];
-        b2[k * PG + r + CS * c] = A.padN[o + r + (size_t)c * A.P];
+        const int rr = t % D, c = t / D;
+        b1[k * PG + t] = A.padP[o + rr + (size_t)c * A.P];
+        b2[k * PG + t] = A.padN[o + rr + (size_t)c * A.P];
       }
     }
   } else {
     const float* v1 = A.V1 + (size_t)g * GS;
     const float* v2 = A.V2 + (size_t)g * GS;
     for (int t = lane; t < GS; t += 32) {
-      const int k = t / DD, r = t % D, c = (t % DD) / D;
-      b1[k * PG + r + CS * c] = v1[t];
-      b2[k * PG + r + CS * c] = v2[t];
+      const int k = t / DD, e = t % DD;
+      b1[k * PG + e] = v1[t];
+      b2[k * PG + e] = v2[t];
     }
   }
   __syncwarp();
 
-  // ---- forward DCT of each slot page, in place: task (k, r) -> row r of T X T'.
-  // K*D is a multiple of 32 and 32 a multiple of D, so each round holds whole
-  // pages: all their rows are read before any is written back.
+  // ---- forward DCT of each slot page, in place: lane (k, r) makes row r of
+  // T X T'.  P[n] = sum_j T(r,j) X(j,n), then Y(r,l) = sum_n P[n] T(l,n), each
+  // a serial fmaf chain from 0 in ascending j / n.  A round holds whole pages,
+  // so all their rows are read before any is written.
   auto fwd = [&](float* X) {
-    for (int t0 = 0; t0 < K * D; t0 += 32) {
-      const int k = (t0 + lane) / D, r = (t0 + lane) % D;
-      const float* x = X + k * PG;
+#pragma unroll 1
+    for (int k0 = 0; k0 < K; k0 += RPG) {
+      const float* x = X + (k0 + kq) * PG;
       float P[D];
 #pragma unroll
       for (int n = 0; n < D; ++n) {
+        float col[D];
+#pragma unroll
+        for (int q = 0; q < D; q += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(x + n * D + q);
+          col[q] = v.x; col[q + 1] = v.y; col[q + 2] = v.z; col[q + 3] = v.w;
+        }
         float acc = 0.f;
 #pragma unroll
-        for (int jj = 0; jj < D; ++jj) acc = fmaf(Tm[r + jj * D], x[jj + CS * n], acc);
+        for (int jj = 0; jj < D; ++jj) acc = fmaf(Trow[jj], col[jj], acc);
         P[n] = acc;
       }
       float Y[D];
@@ -145,12 +162,12 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       for (int l = 0; l < D; ++l) {
         float acc = 0.f;
 #pragma unroll
-        for (int n = 0; n < D; ++n) acc = fmaf(P[n], Tm[l + n * D], acc);
+        for (int n = 0; n < D; ++n) acc = fmaf(P[n], A.T[l + n * D], acc);
         Y[l] = acc;
       }
       __syncwarp();
 #pragma unroll
-      for (int l = 0; l < D; ++l) X[k * PG + r + CS * l] = Y[l];
+      for (int l = 0; l < D; ++l) X[(k0 + kq) * PG + r + D * l] = Y[l];
       __syncwarp();
     }
   };
@@ -159,12 +176,11 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
 
   // ---- Haar along slots, Wiener gain, inverse Haar (lane per coefficient) ----
   for (int e = lane; e < DD; e += 32) {
-    const int off = e % D + CS * (e / D);
     float v1[K], v2[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      v1[k] = b1[k * PG + off];
-      v2[k] = b2[k * PG + off];
+      v1[k] = b1[k * PG + e];
+      v2[k] = b2[k * PG + e];
     }
     haar_dec<K>(v1, cc);
     haar_dec<K>(v2, cc);
@@ -174,20 +190,19 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       const float p = v1[k] * v1[k];
       float f = p / (p + sg);
       if (e == 0 && k >= 14) f = 1.f;
-      b1[k * PG + off] = f;
+      b1[k * PG + e] = f;
       v2[k] = v2[k] * f;
     }
     haar_rec<K>(v2, cc);
 #pragma unroll
-    for (int k = 0; k < K; ++k) b2[k * PG + off] = v2[k];
+    for (int k = 0; k < K; ++k) b2[k * PG + e] = v2[k];
   }
   __syncwarp();
 
   // ---- n2 = norm(col(filt))^2: lane l adds elements o = l, l+32, ... ----------
   float s = 0.f;
   for (int o = lane; o < GS; o += 32) {
-    const int k = o / DD, e = o % DD;
-    const float f = b1[k * PG + e % D + CS * (e / D)];
+    const float f = b1[(o / DD) * PG + o % DD];
     s = s + f * f;
   }
 #pragma unroll
@@ -203,31 +218,40 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   }
   __syncwarp();
 
-  // ---- inverse DCT: P = Y Ti' (rows, into b1), X = Ti P (columns, to global) ----
-  for (int task = lane; task < K * D; task += 32) {
-    const int k = task / D, r = task % D;
+  // ---- inverse DCT, lane (k, r): P(r,l) = sum_n Y(r,n) Ti(l,n) into b1 (the
+  // gains are no longer needed), then X(r,l) = sum_j Ti(r,j) P(j,l) to global.
+  float* og = A.out + (size_t)g * GS;
+#pragma unroll 1
+  for (int k0 = 0; k0 < K; k0 += RPG) {
+    const int k = k0 + kq;
     const float* y = b2 + k * PG;
-    float Prow[D];
+    float Yr[D];
+#pragma unroll
+    for (int n = 0; n < D; ++n) Yr[n] = y[r + D * n];
 #pragma unroll
     for (int l = 0; l < D; ++l) {
       float acc = 0.f;
 #pragma unroll
-      for (int n = 0; n < D; ++n) acc = fmaf(y[r + CS * n], Ti[l + n * D], acc);
-      Prow[l] = acc;
+      for (int n = 0; n < D; ++n) acc = fmaf(Yr[n], A.Ti[l + n * D], acc);
+      b1[k * PG + r + D * l] = acc;
     }
-#pragma unroll
-    for (int l = 0; l < D; ++l) b1[k * PG + r + CS * l] = Prow[l];
   }
   __syncwarp();
-  float* og = A.out + (size_t)g * GS;
-  for (int task = lane; task < K * D; task += 32) {
-    const int k = task / D, l = task % D;
-    const float* p = b1 + k * PG + CS * l;
+#pragma unroll 1
+  for (int k0 = 0; k0 < K; k0 += RPG) {
+    const int k = k0 + kq;
+    const float* p = b1 + k * PG;
 #pragma unroll
-    for (int r = 0; r < D; ++r) {
+    for (int l = 0; l < D; ++l) {
+      float col[D];
+#pragma unroll
+      for (int q = 0; q < D; q += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p + l * D + q);
+        col[q] = v.x; col[q + 1] = v.y; col[q + 2] = v.z; col[q + 3] = v.w;
+      }
       float acc = 0.f;
 #pragma unroll
-      for (int jj = 0; jj < D; ++jj) acc = fmaf(Ti[r + jj * D], p[jj], acc);
+      for (int jj = 0; jj < D; ++jj) acc = fmaf(Tirow[jj], col[jj], acc);
       float v = acc > 0.f ? acc : 0.f;
       if (A.clamp_one && v > 1.f) v = 1.f;
       og[k * DD + r + l * D] = wvs[r + l * D] * v;  // weight.*blocks(:,:,i) (:84-90)
@@ -239,7 +263,7 @@ bool wiener_supported(int d, int K) { return (d == 4 || d == 8 || d == 16) && (K
 
 template <int D, int K>
 static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
-  const size_t sm = (size_t)(3 * D * D + 4 * 2 * D * (D + 1) * K + 4 * D * D) * sizeof(float);
+  const size_t sm = (size_t)(3 * D * D + 4 * 2 * (D * D + D) * K + 4 * D * D) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wiener<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
