@@ -1067,6 +1067,24 @@ int gbm3d_denoiseAndAggregateWie(gbm3d_ctx* c, const float* V1, const float* V2,
   return wiener_entry(c, V1, V2, S, M, N, &sigma, 0, o, U, W, 1);
 }
 
+int gbm3d_tc_selfcheck(gbm3d_ctx* c, const uint16_t* A, const uint16_t* B, float* C) {
+  return guarded(c, [&] {
+    if (!A || !B || !C) argfail(c, "missing argument");
+    uint16_t* dA = buf<uint16_t>(c, "tc.A", 128 * 64);
+    uint16_t* dB = buf<uint16_t>(c, "tc.B", 256 * 64);
+    float* dC = buf<float>(c, "tc.C", 128 * 256);
+    ck(c, cudaMemcpyAsync(dA, A, 128 * 64 * 2, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemcpyAsync(dB, B, 256 * 64 * 2, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    launched(c, launch_tc_gemm_check(dA, dB, dC, c->flag, c->st), "tc_gemm_check");
+    ck(c, cudaMemcpyAsync(C, dC, 128 * 256 * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    if (flag) argfail(c, "tensor-core MMA did not complete in time", GBM3D_ERR_CUDA);
+  });
+}
+
 int gbm3d_denoise_device(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
                          double* U, double* U1) {
   return guarded(c, [&] {

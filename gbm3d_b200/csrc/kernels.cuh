@@ -113,4 +113,7 @@ cudaError_t launch_match_global(int d, const GlobalMatchArgs& A, cudaStream_t st
 // in-place sym4 prefilter; work holds 8 * m * n floats
 cudaError_t launch_sym4_prefilter(float* I, int m, int n, float tau, float* work, cudaStream_t st);
 
+// ---- tensor-core self-check (tc_check.cu) -------------------------------------------
+cudaError_t launch_tc_gemm_check(const uint16_t* A, const uint16_t* B, float* C, int* err, cudaStream_t st);
+
 }  // namespace gbm3d

@@ -176,6 +176,12 @@ int gbm3d_last_launch_count(const gbm3d_ctx* ctx);
  * the context stream.  Returns the number of such launches, or -1. */
 int gbm3d_kernel_time(const gbm3d_ctx* ctx, const char* name, float* total_ms);
 
+/* Tensor-core self-check: C (128 x 256 fp32, row-major) = A B^T for A 128 x 64
+ * and B 256 x 64 row-major bf16 (raw 16-bit patterns), computed by one
+ * tcgen05 MMA sequence with the operand layouts the matcher and the pilot
+ * network use.  Host pointers. */
+int gbm3d_tc_selfcheck(gbm3d_ctx* ctx, const uint16_t* A, const uint16_t* B, float* C);
+
 /* Step-1 block matching that allocates nothing.  No counterpart in the
  * reference: it exists for callers that may not allocate device memory while
  * they run (servers and video pipelines that reserve all GPU memory at
