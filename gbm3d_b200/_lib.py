@@ -33,6 +33,7 @@ class gbm3d_opts(C.Structure):
         ("nMatchSpins", C.c_int), ("matchSpins", C.c_int * 8),
         ("nMatchSpinsWie", C.c_int), ("matchSpinsWie", C.c_int * 8),
         ("staleWeights", C.c_int), ("refStrideWie", C.c_int), ("wavelet", C.c_int),
+        ("form", C.c_int),
     ]
 
 

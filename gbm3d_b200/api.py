@@ -79,6 +79,10 @@ def c_opts(opts: dict) -> gbm3d_opts:
     if wn not in ("bior", "haar"):
         raise GBM3DError(5, f"wname '{wn}': the pipeline's banks are 'bior' (bior1.5 x Haar) and 'haar'")
     c.wavelet = 1 if wn == "haar" else 0
+    form = o.get("form", "plain")
+    if form not in ("plain", "precision"):
+        raise GBM3DError(5, f"form '{form}': 'plain' or 'precision'")
+    c.form = 1 if form == "precision" else 0
     return c
 
 

@@ -33,7 +33,7 @@ constexpr int BIAS = 1 << 12;  // offset added to tile-relative block origins be
 //   step 1: value (wg * Vavg) * mask, weight wg * mask   (denoiseAndAggregateGPU.m:200-201)
 //   step 2: value and weight precomputed by the Wiener kernel (:84-90 of
 //           denoiseAndAggregateWieFast.m), the same single-precision products
-template <int D, int D2, bool WIE>
+template <int D, int D2, bool WIE, bool KAHAN>
 __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   extern __shared__ int smi[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -67,6 +67,18 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   const int vlane = WIE ? pr + pc * D : pr + mv * pc;
   const int wlane = pr + pc * D;
   float u = 0.f, w = 0.f;
+  float cu = 0.f, cw = 0.f;  // Kahan compensations
+  // acc += x, rounded to single (the reference's order), or compensated
+  auto add = [&](float& acc, float& comp, float x) {
+    if (KAHAN) {
+      const float y = x - comp;
+      const float t = acc + y;
+      comp = (t - acc) - y;
+      acc = t;
+    } else {
+      acc = acc + x;
+    }
+  };
   auto walk = [&](int count) {
     for (int e0 = 0; e0 < count; e0 += 4) {
       int4 en[4];
@@ -86,12 +98,12 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
       for (int t = 0; t < 4; ++t) {
         if (cov[t]) {
           if (WIE) {
-            u = u + val[t];
-            w = w + wv[t];
+            add(u, cu, val[t]);
+            add(w, cw, wv[t]);
           } else {
             const float wg = __int_as_float(en[t].z);
-            u = u + (wg * val[t]) * wv[t];
-            w = w + wg * wv[t];
+            add(u, cu, (wg * val[t]) * wv[t]);
+            add(w, cw, wg * wv[t]);
           }
         }
       }
@@ -156,13 +168,14 @@ __global__ void __launch_bounds__(128) k_aggregate_px(AggArgs A) {
   }
 }
 
-template <int D, int D2, bool WIE>
+template <int D, int D2, bool WIE, bool KAHAN = false>
 static cudaError_t launch_px(const AggArgs& A, cudaStream_t st) {
   const size_t sm = (size_t)((D * D + 3) & ~3) * sizeof(float) + (size_t)4 * LCAP * sizeof(int4);
-  cudaError_t e = cudaFuncSetAttribute(k_aggregate_px<D, D2, WIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_aggregate_px<D, D2, WIE, KAHAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = ((A.m + TR - 1) / TR) * ((A.n + TC - 1) / TC);
-  k_aggregate_px<D, D2, WIE><<<(tiles + 3) / 4, 128, sm, st>>>(A);
+  k_aggregate_px<D, D2, WIE, KAHAN><<<(tiles + 3) / 4, 128, sm, st>>>(A);
   return cudaGetLastError();
 }
 
@@ -171,6 +184,13 @@ cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st) {
   if ((size_t)A.m * A.n * A.K >= ((size_t)1 << 31) || (size_t)A.M * A.N * A.K * A.d * A.d >= ((size_t)1 << 31) ||
       A.s < 1 || A.s > A.d)
     return cudaErrorInvalidValue;
+  if (A.kahan) {  // precision form: patch 8
+#define GBM3D_AGGK_CASE(DD2) \
+  if (A.d == 8 && A.d2 == DD2) return A.wiener ? launch_px<8, DD2, true, true>(A, st) : launch_px<8, DD2, false, true>(A, st);
+    GBM3D_AGGK_CASE(16) GBM3D_AGGK_CASE(24) GBM3D_AGGK_CASE(32)
+#undef GBM3D_AGGK_CASE
+    return cudaErrorInvalidValue;
+  }
 #define GBM3D_AGG_CASE(DD, DD2)                                                                 \
   if (A.d == DD && A.d2 == DD2)                                                                 \
     return A.wiener ? launch_px<DD, DD2, true>(A, st) : launch_px<DD, DD2, false>(A, st);

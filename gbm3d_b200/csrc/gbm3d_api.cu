@@ -39,6 +39,7 @@ struct gbm3d_ctx {
   std::vector<cudaEvent_t> kpool;
   std::vector<std::string> krec;
   int launches = 0;
+  int form = 0;         // 0 plain, 1 precision form (set from the options of the current call)
   int* flag = nullptr;  // device status word (non-finite input)
 };
 
@@ -62,6 +63,13 @@ void ck(gbm3d_ctx* c, cudaError_t e, const char* what) {
 void argfail(gbm3d_ctx* c, const std::string& s, int code = GBM3D_ERR_ARG) {
   set_err(c, s);
   throw Fail{code};
+}
+
+// Device status word: bit 0 non-finite input (k_prep), bit 1 a tensor-core
+// MMA that did not complete within its wait limit (the kernel gave up).
+void report_flag(gbm3d_ctx* c, int flag) {
+  if (flag & 1) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+  if (flag & 2) argfail(c, "tensor-core MMA did not complete in time", GBM3D_ERR_CUDA);
 }
 
 template <class T>
@@ -314,6 +322,8 @@ void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
     argfail(c, "refStrideWie must be in 1..blockSizeWie (0: blockSizeWie)");
   if (o->filtType != 0 && o->filtType != 1) argfail(c, "unrecognized filtering");  // denoiseAndAggregateGPU.m:54
   if (o->wavelet != 0 && o->wavelet != 1) argfail(c, "wavelet must be 0 (bior1.5 x Haar) or 1 (3D Haar)");
+  if (o->form != 0 && o->form != 1) argfail(c, "form must be 0 (plain) or 1 (precision)");
+  c->form = o->form;
 }
 
 void check_match(gbm3d_ctx* c, int d, int d2, int K) {
@@ -355,7 +365,7 @@ void check_match_set(gbm3d_ctx* c, const uint32_t* S, const int32_t* cnt, size_t
 // the reference's layout) and (M d) x (N d) x K otherwise.
 void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, int spin, int d, int d2,
                int K, int numMin, double sigma, uint32_t* S, int32_t* cnt, float* volume, float* V1,
-               float* V2, const char* tag, int s) {
+               float* V2, const char* tag, int s, int form) {
   const int P = pitch4(m + d2);
   const std::string t(tag);
   float* pad = buf<float>(c, (t + ".pad").c_str(), (size_t)P * (n + d2));
@@ -383,6 +393,18 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
   A.n = s == d ? n : A.N * d;
   A.V1 = V1;
   A.V2 = V2;
+  A.err = c->flag;
+  if (form == 1) {
+    // precision form: the V1/V2 gathers of matchBlocksWie are not produced by
+    // the tensor-core matcher, so that entry point keeps the plain search
+    if (!match_tc_supported(d, d2, s, K, A.tol_branch != 0))
+      argfail(c, "precision form needs blockSize 8, numMin = numMax <= 16 and refStride <= 4",
+              GBM3D_ERR_UNSUPPORTED);
+    if (!V1 && !V2 && !img2) {
+      launched(c, launch_match_tc(d, d2, A, c->st), "match_tc");
+      return;
+    }
+  }
   launched(c, launch_match(d, d2, A, c->st), "match");
 }
 
@@ -459,6 +481,7 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
   std::vector<double> mk(d * d);
   sine_window(d, 0.1, 0.9, mk.data());
   for (int e = 0; e < d * d; ++e) A.win[e] = (float)mk[e];
+  A.kahan = c->form == 1;
   A.s = s;
   A.m = (M - 1) * s + d;
   A.n = (N - 1) * s + d;
@@ -505,6 +528,7 @@ void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float*
   G.blocks = A.out;
   G.gw = A.wt;
   G.s = A.s;
+  G.kahan = c->form == 1;
   G.m = (M - 1) * A.s + d;
   G.n = (N - 1) * A.s + d;
   G.U = U;
@@ -526,6 +550,7 @@ int guarded(gbm3d_ctx* c, F&& f) {
   try {
     ck(c, cudaSetDevice(c->device), "cudaSetDevice");
     c->launches = 0;
+    c->form = 0;
     c->records.clear();
     c->krec.clear();
     if (c->timing) kevent(c, 0);
@@ -603,7 +628,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     const int s = o->matchSpins[ii];
     {
       StageTimer t(c, 1);
-      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1", st1);
+      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1", st1, o->form);
     }
     run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType, st1);
     k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
@@ -632,7 +657,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     const int s = o->matchSpinsWie[ii];
     {
       StageTimer t(c, 4);
-      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2", st2);
+      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2", st2, o->form);
     }
     float* padP = buf<float>(c, "m2.pad", 1);  // the pilot search image run_match just built
     float* padN = buf<float>(c, "m2.padN", (size_t)pitch4(Mp + d2) * (Np + d2));
@@ -890,14 +915,14 @@ int gbm3d_matchBlocksCPU(gbm3d_ctx* c, const double* I, int m, int n, double sig
       dV = buf<float>(c, "io.V", vn);
       ck(c, cudaMemsetAsync(dV, 0, vn * sizeof(float), c->st), "memset");
     }
-    run_match(c, If, nullptr, m, n, 0, d, d2, K, o->numMin, sigma, dS, dc, dV, nullptr, nullptr, "m1", s);
+    run_match(c, If, nullptr, m, n, 0, d, d2, K, o->numMin, sigma, dS, dc, dV, nullptr, nullptr, "m1", s, o->form);
     ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (S_count) ck(c, cudaMemcpyAsync(S_count, dc, (size_t)M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (Volume) ck(c, cudaMemcpyAsync(Volume, dV, vn * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
-    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+    report_flag(c, flag);
   });
 }
 
@@ -944,7 +969,7 @@ int gbm3d_matchBlocksGPU(gbm3d_ctx* c, const double* I, int m, int n, double sig
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
-    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+    report_flag(c, flag);
   });
 }
 
@@ -1007,14 +1032,14 @@ int gbm3d_matchBlocksWie(gbm3d_ctx* c, const double* I, const double* In, int m,
     uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
     float* d1 = V1 ? buf<float>(c, "io.V1", gs) : nullptr;
     float* d2p = V2 ? buf<float>(c, "io.V2", gs) : nullptr;
-    run_match(c, If, V2 ? Inf : nullptr, m, n, 0, d, d2, K, K, sigma, dS, nullptr, nullptr, d1, d2p, "m2", s);
+    run_match(c, If, V2 ? Inf : nullptr, m, n, 0, d, d2, K, K, sigma, dS, nullptr, nullptr, d1, d2p, "m2", s, o->form);
     ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (V1) ck(c, cudaMemcpyAsync(V1, d1, gs * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (V2) ck(c, cudaMemcpyAsync(V2, d2p, gs * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
-    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+    report_flag(c, flag);
   });
 }
 
@@ -1109,7 +1134,7 @@ int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, con
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
-    if (flag) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
+    report_flag(c, flag);
   });
 }
 

@@ -20,12 +20,17 @@ struct MatchArgs {
   int m, n;           // volume rows/cols: the image for s = d, (M d) x (N d) otherwise
   float* V1;          // d x d x K x M x N gathers (may be null)
   float* V2;
+  int* err;           // set to 1 by the tensor-core matcher when an MMA wait times out (may be null)
 };
 bool match_supported(int d, int d2);
 size_t match_smem_bytes(int d, int d2);
 cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st);
 cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
                             cudaStream_t st);
+// Precision form (match_tc.cu): bf16 tensor-core distances, exact FP32 re-rank
+// of the 32 best; top-K branch only (numMin = numMax), d = 8, stride <= 4.
+bool match_tc_supported(int d, int d2, int s, int K, bool tol_branch);
+cudaError_t launch_match_tc(int d, int d2, const MatchArgs& A, cudaStream_t st);
 
 // ---- step 1: global 3D wavelet hard thresholding (wavelet.cu) ----------------
 struct WaveletBank {
@@ -89,6 +94,7 @@ struct AggArgs {
   const int32_t* cnt;   // may be null (every group holds K)
   int M, N, d, d2, K;
   int s;                // reference stride (block of reference (i, j) lands at (i s + a, j s + b))
+  int kahan;            // 1: Kahan-compensated FP32 sums (precision form; d = 8 only)
   int wiener;           // 0: step-1 weights (scalar x mask); 1: step-2 (precomputed)
   const float* blocks;  // step 1: tile-space Vavg ((M d) x (N d) x K); step 2: weighted values, d x d x K per group
   const float* gw;      // step 1: weight per group; step 2: weight table, d x d per group

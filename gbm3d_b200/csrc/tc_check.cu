@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) k_tc_gemm_check(const uint16_t* __restric
     tc::commit(mbar);
   }
   const bool ok = tc::mbar_wait(mbar, 0, 2000000000LL);
-  if (!ok && tid == 0) atomicExch(err, 1);
+  if (!ok && tid == 0) atomicOr(err, 2);
   tc::fence_after_sync();
   if (ok) {
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);

@@ -63,6 +63,11 @@ typedef struct gbm3d_opts {
   int staleWeights;
   int refStrideWie;
   int wavelet; /* step-1 bank of gbm3d_denoise: 0 = bior1.5 x Haar (GBM3D.m:40), 1 = 3D Haar */
+  /* 0 plain (the reference's arithmetic, FP32); 1 precision form: block
+   * distances on the bf16 tensor cores with an exact FP32 re-rank of the 32
+   * best per reference, and Kahan-compensated FP32 aggregation.  Not in the
+   * reference. */
+  int form;
 } gbm3d_opts;
 
 /* Separable 3D wavelet bank: 1D analysis (a_) and synthesis (s_) filters for the
