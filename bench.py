@@ -117,6 +117,9 @@ def padded_side(o) -> int:
     s1, s2 = opt.strides(o)
     if s1 == d and (not o["Wiener"] or (s2 == dw and d % dw == 0)):
         return -(-SIZE // d) * d
+    import math
+    if o["Wiener"] and (d - dw) % math.gcd(s1, s2):
+        raise ValueError("no padded size lets both reference grids end at the border")
     p = max(SIZE, d, dw)
     while (p - d) % s1 or (o["Wiener"] and (p - dw) % s2):
         p += 1

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <numeric>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -583,7 +584,12 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   if (!(sigma >= 0) || !std::isfinite(sigma)) argfail(c, "sigma must be a finite non-negative scalar");
   const int st1 = stride1(o), st2 = stride2(o);
   // GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
-  // smallest size whose references of both steps end exactly at the border
+  // smallest size whose references of both steps end exactly at the border.
+  // Such a size exists iff d = dw modulo gcd(st1, st2); then the search below
+  // ends within lcm(st1, st2) steps.
+  if (o->Wiener && (d - dw) % std::gcd(st1, st2) != 0)
+    argfail(c, "no padded size lets both reference grids end at the border: blockSize - blockSizeWie must be "
+               "a multiple of gcd(refStride, refStrideWie)", GBM3D_ERR_UNSUPPORTED);
   auto padded = [&](int L) {
     if (st1 == d && (!o->Wiener || (st2 == dw && d % dw == 0))) return (L + d - 1) / d * d;
     int p = std::max(L, std::max(d, dw));

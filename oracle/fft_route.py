@@ -254,10 +254,13 @@ def denoise_wiener(V1, V2, S, sigma, d2, variant=0, st=None):
 def padded_size(L, opts):
     """GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
     smallest size at which both steps' references end exactly at the border."""
+    import math
     d, dw = opts["blockSize"], opts["blockSizeWie"]
     st1, st2 = opts.get("refStride") or d, opts.get("refStrideWie") or dw
     if st1 == d and (not opts["Wiener"] or (st2 == dw and d % dw == 0)):
         return -(-L // d) * d
+    if opts["Wiener"] and (d - dw) % math.gcd(st1, st2):
+        raise ValueError("no padded size lets both reference grids end at the border")
     p = max(L, d, dw)
     while (p - d) % st1 or (opts["Wiener"] and (p - dw) % st2):
         p += 1

@@ -37,6 +37,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <numeric>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -1163,6 +1164,10 @@ int orc_match_blocks_global(int prec, const double* I, int m, int n, double sigm
 // U = GBM3D(I,sigma,opts); U1out (may be null) receives out.U1.
 int orc_gbm3d(int prec, const double* I, int m, int n, double sigma, const orc_opts* o,
               double* U, double* U1) {
+  const int st1 = o->refStride > 0 ? o->refStride : o->blockSize;
+  const int st2 = o->refStrideWie > 0 ? o->refStrideWie : o->blockSizeWie;
+  // no padded size lets both reference grids end at the border
+  if (o->Wiener && (o->blockSize - o->blockSizeWie) % std::gcd(st1, st2) != 0) return 1;
   if (prec == 32) gbm3d<float>(I, m, n, sigma, o, U, U1);
   else gbm3d<double>(I, m, n, sigma, o, U, U1);
   return 0;

@@ -255,7 +255,8 @@ def GBM3D(I, sigma, opts, prec=32):
     U = np.zeros((m, n), order="F")
     U1 = np.zeros((m, n), order="F")
     oc = make_opts(opts)
-    lib().orc_gbm3d(prec, _p(I), m, n, C.c_double(sigma), C.byref(oc), _p(U), _p(U1))
+    if lib().orc_gbm3d(prec, _p(I), m, n, C.c_double(sigma), C.byref(oc), _p(U), _p(U1)) != 0:
+        raise ValueError("no padded size lets both reference grids end at the border")
     return U, U1
 
 

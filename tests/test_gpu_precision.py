@@ -81,6 +81,6 @@ def test_precision_form_rejects_unsupported(gpu):
     from gbm3d_b200 import GBM3DError
     _, noisy = synth.noisy_image(64, 64, 25.0, seed=1)
     with pytest.raises(GBM3DError):
-        gpu.GBM3D(noisy, 25.0, _opts("precision", blockSize=16))
+        gpu.GBM3D(noisy, 25.0, _opts("precision", blockSize=16, refStride=4, refStrideWie=4))
     with pytest.raises(GBM3DError):
         gpu.GBM3D(noisy, 25.0, _opts("precision", numMin=4))
