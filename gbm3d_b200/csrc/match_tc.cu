@@ -17,7 +17,10 @@
 // B^T (positions x 64), in chunks of 128 positions double-buffered in shared
 // memory and in two TMEM accumulators of 128 columns, so the next chunk's MMA
 // runs while the current one is read out.  Each thread keeps the 2K smallest
-// approximate distances of its own window.
+// approximate distances of its own window in a max-heap in shared memory: a
+// position is tested against the heap's root with one compare, and the rare
+// candidates that beat it are inserted in batches of 32 positions, so the
+// warp's lanes diverge only in the short sift-down loop.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "tc.cuh"
@@ -35,8 +38,8 @@ constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 
 struct TcGeom {
   int PR, PC, NP;   // candidate-position grid of a tile
-  int CH, CW;       // region (fp32 / bf16 image) rows (padded even) and columns
-  size_t off_img32, off_img16, off_nb2, off_A, off_B, off_misc, bytes;
+  int CH, CW;       // region (fp32 image) rows (padded even) and columns
+  size_t off_img32, off_nb2, off_A, off_B, off_heap, off_misc, bytes;
 };
 
 __host__ __device__ inline TcGeom tc_geom(int s, int d2) {
@@ -56,8 +59,8 @@ __host__ __device__ inline TcGeom tc_geom(int s, int d2) {
   g.off_A = take((size_t)128 * TKD * 2, 1024);
   g.off_B = take((size_t)2 * NC * TKD * 2, 1024);
   g.off_img32 = take((size_t)g.CH * g.CW * 4, 16);
-  g.off_img16 = take((size_t)g.CH * g.CW * 2, 16);
-  g.off_nb2 = take((size_t)((g.NP + NC - 1) / NC * NC) * 4, 16);
+  g.off_nb2 = take((size_t)2 * NC * 4, 16);             // ||b'||^2 of the two chunks in flight
+  g.off_heap = take((size_t)2 * CAND * 128 * 4, 16);    // per-thread heaps: values, then positions
   g.off_misc = take(64, 16);
   g.bytes = o;
   return g;
@@ -70,8 +73,9 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
   const int s = A.s;
   const TcGeom G = tc_geom(s, D2);
   float* img32 = reinterpret_cast<float*>(smem + G.off_img32);        // column-major CH x CW
-  uint16_t* img16 = reinterpret_cast<uint16_t*>(smem + G.off_img16);  // bf16 of (img32 - mean)
-  float* nb2 = reinterpret_cast<float*>(smem + G.off_nb2);            // ||b'||^2 per position
+  float* nb2 = reinterpret_cast<float*>(smem + G.off_nb2);            // ||b'||^2, chunk buffer b at b*NC
+  float* hv = reinterpret_cast<float*>(smem + G.off_heap);            // heap node q of thread t at q*128+t
+  int* hp = reinterpret_cast<int*>(hv + CAND * 128);
   unsigned char* sA = smem + G.off_A;
   unsigned char* sB = smem + G.off_B;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + G.off_misc);    // [2]
@@ -123,21 +127,8 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
   __syncthreads();
   const int ntot = fail_s[1] + fail_s[2] + fail_s[3] + fail_s[4];
   const float mean = ntot > 0 ? (red[0] + red[1] + red[2] + red[3]) / (float)ntot : 0.f;
-  for (int e = tid; e < G.CH * G.CW; e += 128) img16[e] = tc::bf16_bits(img32[e] - mean);
-  // ||b'||^2 of every position (fp32 of the centred values), 0 past the grid
   const int NPc = (G.NP + NC - 1) / NC * NC;
-  for (int p = tid; p < NPc; p += 128) {
-    float acc = 0.f;
-    if (p < G.NP) {
-      const int pr = p % G.PR, pc = p / G.PR;
-      for (int c = 0; c < TD; ++c)
-        for (int r = 0; r < TD; ++r) {
-          const float t = img32[(pr + r) + (pc + c) * G.CH] - mean;
-          acc = fmaf(t, t, acc);
-        }
-    }
-    nb2[p] = acc;
-  }
+  auto bf = [&](float x) -> uint32_t { return tc::bf16_bits(x - mean); };
   // ---- A: this thread's reference block (at window offset (H, H)) ------------
   {
     const int ry = s * li + H, rx = s * lj + H;
@@ -145,19 +136,19 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
     for (int r = 0; r < TD; ++r) {
       uint32_t w[4];
 #pragma unroll
-      for (int c = 0; c < TD; c += 2) {
-        const uint32_t lo = img16[(ry + r) + (rx + c) * G.CH], hi = img16[(ry + r) + (rx + c + 1) * G.CH];
-        w[c / 2] = lo | (hi << 16);
-      }
+      for (int c = 0; c < TD; c += 2)
+        w[c / 2] = bf(img32[(ry + r) + (rx + c) * G.CH]) | (bf(img32[(ry + r) + (rx + c + 1) * G.CH]) << 16);
       *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(tid, r * TD, TKD)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
   // B chunk: thread t builds the row of position chunk*NC + t (k = r*8 + c)
+  // and its squared norm ||b'||^2 (fp32 of the centred values; 0 past the grid)
   auto build_B = [&](int chunk, int buf) {
     const int p = chunk * NC + tid;
     unsigned char* base = sB + (size_t)buf * NC * TKD * 2;
     const int pr = p % G.PR, pc = p / G.PR;
     const bool in = p < G.NP;
+    float acc = 0.f;
 #pragma unroll
     for (int r = 0; r < TD; ++r) {
       uint32_t w[4];
@@ -165,23 +156,33 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
       for (int c = 0; c < TD; c += 2) {
         uint32_t lo = 0, hi = 0;
         if (in) {
-          lo = img16[(pr + r) + (pc + c) * G.CH];
-          hi = img16[(pr + r) + (pc + c + 1) * G.CH];
+          const float x0v = img32[(pr + r) + (pc + c) * G.CH] - mean;
+          const float x1v = img32[(pr + r) + (pc + c + 1) * G.CH] - mean;
+          acc = fmaf(x0v, x0v, acc);
+          acc = fmaf(x1v, x1v, acc);
+          lo = tc::bf16_bits(x0v);
+          hi = tc::bf16_bits(x1v);
         }
         w[c / 2] = lo | (hi << 16);
       }
       *reinterpret_cast<uint4*>(base + tc::kmajor_offset(tid, r * TD, TKD)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    nb2[buf * NC + tid] = acc;
   };
   const int nch = NPc / NC;
-  build_B(0, 0);
+  // chunks are visited from the middle of the position grid outwards: positions
+  // near the windows' centres tend to match best, so the heap thresholds drop
+  // early and few later positions need inserting.  Buffers follow the visit order.
+  const int mid = nch / 2;
+  auto chunk_of = [&](int k) { return k == 0 ? mid : ((k & 1) ? mid - (k + 1) / 2 : mid + k / 2); };
+  build_B(chunk_of(0), 0);
   tc::fence_proxy_async();
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *taddr_s;
   constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NC);
-  auto issue = [&](int chunk) {
+  auto issue = [&](int chunk) {  // chunk: position in the visit order (selects the buffers)
     const uint32_t a0 = tc::smem_u32(sA);
     const uint32_t b0 = tc::smem_u32(sB + (size_t)(chunk & 1) * NC * TKD * 2);
 #pragma unroll
@@ -192,22 +193,20 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
   };
   if (tid == 0) issue(0);
 
-  // running 2K smallest approximate distances of this thread's window
-  float cv[CAND];
-  int cp[CAND];
+  // running 2K smallest approximate distances of this thread's window: a
+  // max-heap (root = the largest kept = the admission threshold)
 #pragma unroll
   for (int q = 0; q < CAND; ++q) {
-    cv[q] = 3.0e38f;
-    cp[q] = -1;
+    hv[q * 128 + tid] = 3.0e38f;
+    hp[q * 128 + tid] = -1;
   }
   float thr = 3.0e38f;
-  int thr_i = 0;
   const int wr0 = s * li, wc0 = s * lj;  // window origin in position coordinates
   // columns of position space any reference of this warp can use
   const int wpc_lo = s * (warp * 32 / TI), wpc_hi = s * (warp * 32 / TI + 32 / TI - 1) + D2 - 1;
 
   for (int c = 0; c < nch; ++c) {
-    if (c + 1 < nch) build_B(c + 1, (c + 1) & 1);
+    if (c + 1 < nch) build_B(chunk_of(c + 1), (c + 1) & 1);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -217,39 +216,63 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
     const bool ok = tc::mbar_wait(&mbar[c & 1], (uint32_t)((c >> 1) & 1), WAIT_CYCLES);
     if (!ok) *fail_s = 1;
     tc::fence_after_sync();
-    const int p0 = c * NC;
+    const int p0 = chunk_of(c) * NC;
     const int pc_first = p0 / G.PR, pc_last = (p0 + NC - 1) / G.PR;
     if (ok && pc_last >= wpc_lo && pc_first <= wpc_hi) {  // warp-uniform skip of chunks outside every window
       const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((c & 1) * NC);
 #pragma unroll 1
       for (int q0 = 0; q0 < NC; q0 += 32) {
+        // positions P0 .. P0+31: rows r0.. of column c0, then (after a wrap) rows 0.. of c0+1
+        const int P0 = p0 + q0, r0 = P0 % G.PR, c0 = P0 / G.PR;
+        const int L1 = min(32, G.PR - r0);
+        auto bits = [](int lo, int hi) -> uint32_t {
+          if (hi <= lo) return 0u;
+          const int n = hi - lo;
+          return (n >= 32 ? 0xffffffffu : ((1u << n) - 1u)) << lo;
+        };
+        uint32_t inm = 0;
+        if ((unsigned)(c0 - wc0) < (unsigned)D2) inm |= bits(max(0, wr0 - r0), min(L1, wr0 + D2 - r0));
+        if ((unsigned)(c0 + 1 - wc0) < (unsigned)D2) inm |= bits(L1 + wr0, min(32, L1 + wr0 + D2));
+        if (!__any_sync(0xffffffffu, inm != 0)) continue;  // no reference of this warp sees these positions
         float v[32];
         tc::tmem_ld32(lane_base + q0, v);
-        int p = p0 + q0, pr = p % G.PR, pc = p / G.PR;
+        uint32_t qm = 0;
 #pragma unroll
         for (int u = 0; u < 32; ++u) {
-          const float dist = fmaf(-2.f, v[u], nb2[p]);
-          const bool in = (unsigned)(pr - wr0) < (unsigned)D2 && (unsigned)(pc - wc0) < (unsigned)D2 && p < G.NP;
-          if (in && dist < thr) {
+          v[u] = fmaf(-2.f, v[u], nb2[(c & 1) * NC + q0 + u]);  // approximate distance (less ||a'||^2)
+          qm |= (v[u] < thr ? 1u : 0u) << u;
+        }
+        qm &= inm;
+        // insert the qualifying positions one at a time (lanes with none idle)
+        while (__any_sync(0xffffffffu, qm != 0)) {
+          if (qm) {
+            const int u = __ffs(qm) - 1;
+            qm &= qm - 1;
+            float d = v[0];
 #pragma unroll
-            for (int q = 0; q < CAND; ++q)
-              if (q == thr_i) {
-                cv[q] = dist;
-                cp[q] = p;
+            for (int k = 1; k < 32; ++k) d = (u == k) ? v[k] : d;
+            if (d < thr) {  // replace the root, sift down
+              int q = 0;
+              while (true) {
+                int ch = 2 * q + 1;
+                if (ch >= CAND) break;
+                float cv = hv[ch * 128 + tid];
+                if (ch + 1 < CAND) {
+                  const float cv2 = hv[(ch + 1) * 128 + tid];
+                  if (cv2 > cv) {
+                    cv = cv2;
+                    ++ch;
+                  }
+                }
+                if (cv <= d) break;
+                hv[q * 128 + tid] = cv;
+                hp[q * 128 + tid] = hp[ch * 128 + tid];
+                q = ch;
               }
-            thr = cv[0];
-            thr_i = 0;
-#pragma unroll
-            for (int q = 1; q < CAND; ++q)
-              if (cv[q] > thr) {
-                thr = cv[q];
-                thr_i = q;
-              }
-          }
-          ++p;
-          if (++pr == G.PR) {
-            pr = 0;
-            ++pc;
+              hv[q * 128 + tid] = d;
+              hp[q * 128 + tid] = P0 + u;
+              thr = hv[tid];
+            }
           }
         }
       }
@@ -261,13 +284,11 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
   if (failed && tid == 0 && A.err) atomicOr(A.err, 2);
 
   // ---- exact FP32 re-rank (the plain matcher's operation order) ----------------
-  // The operand buffers are free now: candidates, exact keys and the selection
-  // go to shared memory (element q of thread t at q * 128 + t).
-  int* cpS = reinterpret_cast<int*>(sB);
-  uint32_t* keyS = reinterpret_cast<uint32_t*>(sB) + CAND * 128;
+  // The operand buffers are free now: exact keys and the selection go to
+  // shared memory (element q of thread t at q * 128 + t) beside the heap.
+  const int* cpS = hp;
+  uint32_t* keyS = reinterpret_cast<uint32_t*>(sB);
   uint32_t* selS = reinterpret_cast<uint32_t*>(sA);
-#pragma unroll
-  for (int q = 0; q < CAND; ++q) cpS[q * 128 + tid] = cp[q];
   if (valid && !failed) {
     const int ry = s * li + H, rx = s * lj + H;
     float xr[TKD];
