@@ -245,15 +245,20 @@ def GBM3D(I, sigma, opts: dict | None = None, ctx: Context | None = None):
     """
     ctx = ctx or context()
     o = _opt.resolve_opts(opts)
-    if np.ndim(sigma) != 0 and np.size(sigma) != 1:
-        raise GBM3DError(5, "coloured-noise (matrix) sigma is not supported by GBM3D here")
     I = np.asfortranarray(I, dtype=np.float64)
     m, n = I.shape
     U = np.zeros((m, n), order="F")
     U1 = np.zeros((m, n), order="F")
     co = c_opts(o)
-    ctx.check(lib().gbm3d_denoise(ctx.h, _p(I), m, n, float(np.asarray(sigma).reshape(-1)[0]), C.byref(co),
-                                  _p(U), _p(U1)))
+    sg = np.asarray(sigma, dtype=np.float64)
+    if sg.ndim >= 1 and sg.shape[0] > 1:
+        # coloured noise, sigma = sigma^2 * PSD (GBM3D.m:33-35)
+        tau = np.asfortranarray(_opt.getColoredTau(int(o["levels"]), sg))
+        swie = np.asfortranarray(_opt.getColoredWie(sg, int(o["blockSizeWie"])))
+        ctx.check(lib().gbm3d_denoise_colored(ctx.h, _p(I), m, n, _sigma_scalar(sg), _p(tau), _p(swie),
+                                              C.byref(co), _p(U), _p(U1)))
+        return U, {"U1": U1, "tau": tau, "sigmaWie": swie}
+    ctx.check(lib().gbm3d_denoise(ctx.h, _p(I), m, n, float(sg.reshape(-1)[0]), C.byref(co), _p(U), _p(U1)))
     return U, {"U1": U1}
 
 

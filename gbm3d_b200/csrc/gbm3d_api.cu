@@ -573,8 +573,11 @@ void opts_dims(const gbm3d_opts* o, int& d, int& dw, int& d2, int& K) {
 }
 
 // The whole GBM3D.m pipeline on device buffers.
+// tau_in (levels x 7) and sigwie_in (blockSizeWie^2) replace sigma * getTau
+// and the scalar Wiener sigma on the coloured-noise path (GBM3D.m:30-36);
+// sigma is then what the matchers use, mean(sqrt(sigmaPSD)).
 void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const gbm3d_opts* o, double* dU,
-              double* dU1) {
+              double* dU1, const double* tau_in = nullptr, const double* sigwie_in = nullptr) {
   check_opts(c, o);
   int d, dw, d2, K;
   opts_dims(o, d, dw, d2, K);
@@ -609,6 +612,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   std::vector<double> tau(o->levels * 7);
   tau_table(o->levels, o->tauMode, tau.data());
   for (auto& t : tau) t *= sigma;
+  if (tau_in) std::copy(tau_in, tau_in + o->levels * 7, tau.begin());
 
   StageTimer tall(c, 7);
   float* If = buf<float>(c, "p.If", px);
@@ -679,7 +683,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     A.K = K;
     A.s = st2;
     double sg = sigma;
-    fill_wiener_consts(A, dw, &sg, 0, 0);
+    fill_wiener_consts(A, dw, sigwie_in ? sigwie_in : &sg, sigwie_in ? 1 : 0, 0);
     run_wiener_agg(c, A, dw, d2, Us, Ws);
     k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
     launched(c, cudaGetLastError(), "accum");
@@ -1124,8 +1128,8 @@ int gbm3d_denoise_device(gbm3d_ctx* c, const double* I, int m, int n, double sig
   });
 }
 
-int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,
-                  double* U1) {
+static int denoise_host(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,
+                        double* U1, const double* tau, const double* sigwie) {
   return guarded(c, [&] {
     if (!I || !U) argfail(c, "missing argument");
     if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
@@ -1134,7 +1138,7 @@ int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, con
     double* dU = buf<double>(c, "h.U", px);
     double* dU1 = U1 ? buf<double>(c, "h.U1", px) : nullptr;
     ck(c, cudaMemcpyAsync(dI, I, px * 8, cudaMemcpyHostToDevice, c->st), "H2D");
-    pipeline(c, dI, m, n, sigma, o, dU, dU1);
+    pipeline(c, dI, m, n, sigma, o, dU, dU1, tau, sigwie);
     ck(c, cudaMemcpyAsync(U, dU, px * 8, cudaMemcpyDeviceToHost, c->st), "D2H");
     if (U1) ck(c, cudaMemcpyAsync(U1, dU1, px * 8, cudaMemcpyDeviceToHost, c->st), "D2H");
     int flag = 0;
@@ -1142,6 +1146,20 @@ int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, con
     ck(c, cudaStreamSynchronize(c->st), "sync");
     report_flag(c, flag);
   });
+}
+
+int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,
+                  double* U1) {
+  return denoise_host(c, I, m, n, sigma, o, U, U1, nullptr, nullptr);
+}
+
+int gbm3d_denoise_colored(gbm3d_ctx* c, const double* I, int m, int n, double sigma_match, const double* tau,
+                          const double* sigmaWie, const gbm3d_opts* o, double* U, double* U1) {
+  if (!tau || !sigmaWie) {
+    if (c) c->err = "tau and sigmaWie are required";
+    return GBM3D_ERR_ARG;
+  }
+  return denoise_host(c, I, m, n, sigma_match, o, U, U1, tau, sigmaWie);
 }
 
 }  // extern "C"

@@ -89,6 +89,97 @@ def grid_count(L: int, d: int, s: int) -> int:
     return (L - d) // s + 1
 
 
+def _bior_xy():
+    Ca, Cb, Cc = 0.016572815184060, 0.121533978016438, np.sqrt(2.0) / 2
+    lo = np.array([Ca, -Ca, -Cb, Cb, Cc, Cc, Cb, -Cb, -Ca, Ca])
+    hi = np.zeros(10)
+    hi[4], hi[5] = -Cc, Cc
+    return lo, hi
+
+
+def _fft2_sized(h, d1, d2):
+    """fft2(h, d1, d2): zero-pad (or crop) h to d1 x d2 first."""
+    z = np.zeros((d1, d2))
+    a, b = min(h.shape[0], d1), min(h.shape[1], d2)
+    z[:a, :b] = h[:a, :b]
+    return np.fft.fft2(z)
+
+
+def getColoredTau(levels: int, sigmaPSD, tau0: float = 6.0) -> np.ndarray:
+    """levels x 7 thresholds for coloured noise, sigmaPSD = sigma^2 * |F(filter)|^2
+    (utilities/getColoredTau.m:10-57): the 2D bior1.5 filters of the 7 detail
+    bands (the 3D band order with the slot axis dropped), replicated 2^(i-1)
+    times per axis at level i, and tau(i,j) = tau0 * sqrt(<PSD, |Psi_hat|^2> /
+    sum |Psi_hat|^2)."""
+    P = np.asarray(sigmaPSD, dtype=np.float64)
+    d1, d2 = P.shape
+    lo, hi = _bior_xy()
+    f = [np.outer(lo, lo), np.outer(hi, lo), np.outer(lo, hi), np.outer(lo, lo),
+         np.outer(hi, hi), np.outer(hi, lo), np.outer(lo, hi), np.outer(hi, hi)]
+    f = [x.astype(np.float32).astype(np.float64) for x in f]  # Psi is single in the reference
+    tau = np.zeros((levels, 7))
+    for i in range(levels):
+        k = 2 ** i
+        for j in range(7):
+            ph = np.kron(f[j + 1], np.ones((k, k)))  # imresize(.., 2^(i-1), 'nearest')
+            F = np.abs(_fft2_sized(ph, d1, d2)) ** 2
+            tau[i, j] = np.sqrt(np.sum(P * F) / np.sum(F))
+    return tau * tau0
+
+
+def gaussian_psf_hat(shape, omega: float) -> np.ndarray:
+    """Transfer function of a unit-sum circular Gaussian of standard deviation
+    omega centred on pixel (1,1) (the role of makeGausPSF(shape, omega) in
+    getColoredWie.m:6; that helper is not part of the reference repository,
+    so this form is an assumption)."""
+    m, n = shape
+    y = np.minimum(np.arange(m), m - np.arange(m))
+    x = np.minimum(np.arange(n), n - np.arange(n))
+    h = np.exp(-(y[:, None] ** 2 + x[None, :] ** 2) / (2.0 * omega ** 2))
+    return np.fft.fft2(h / h.sum())
+
+
+def _resize_bilinear_aa(a, out_len, axis):
+    """One axis of imresize(.., 'bilinear') with antialiasing when shrinking:
+    triangle kernel stretched by 1/scale, weights normalised, symmetric border."""
+    L = a.shape[axis]
+    scale = out_len / L
+    width = 2.0 / scale if scale < 1 else 2.0
+    u = np.arange(1, out_len + 1)
+    x = u / scale + 0.5 * (1 - 1 / scale)
+    left = np.floor(x - width / 2).astype(int)
+    P = int(np.ceil(width)) + 2
+    idx = left[:, None] + np.arange(P)[None, :]
+    dist = x[:, None] - idx
+    if scale < 1:
+        w = scale * np.maximum(0.0, 1 - np.abs(scale * dist))
+    else:
+        w = np.maximum(0.0, 1 - np.abs(dist))
+    w = w / w.sum(axis=1, keepdims=True)
+    aux = np.concatenate([np.arange(1, L + 1), np.arange(L, 0, -1)])
+    idx = aux[np.mod(idx - 1, 2 * L)] - 1
+    a = np.moveaxis(a, axis, 0)
+    out = np.einsum("up,up...->u...", w, a[idx])
+    return np.moveaxis(out, 0, axis)
+
+
+def getColoredWie(sigmaPSD, d: int) -> np.ndarray:
+    """d x d Wiener sigmas for coloured noise (utilities/getColoredWie.m:6-18):
+    the PSD smoothed by a Gaussian of width 3, resized to d x d (bilinear,
+    antialiased), then sigmaWie(j,i) = sqrt(sum(PSD .* |fft2(idct2(e_ji))|^2)) / d."""
+    P = np.asarray(sigmaPSD, dtype=np.float64)
+    P = np.real(np.fft.ifft2(gaussian_psf_hat(P.shape, 3.0) * np.fft.fft2(P)))
+    P = _resize_bilinear_aa(_resize_bilinear_aa(P, d, 0), d, 1)
+    T = np.sqrt(2.0 / d) * np.cos(np.pi * (2 * np.arange(d)[None, :] + 1) * np.arange(d)[:, None] / (2 * d))
+    T[0, :] = np.sqrt(1.0 / d)
+    out = np.zeros((d, d))
+    for i in range(d):
+        for j in range(d):
+            y = np.outer(T[j], T[i])  # idct2 of the impulse at (j, i)
+            out[j, i] = np.sqrt(np.sum(P * np.abs(np.fft.fft2(y)) ** 2)) / d
+    return out
+
+
 def getTau(levels: int, mode: int = 1) -> np.ndarray:
     """levels x 7 threshold multipliers (getTau.m:9-51)."""
     tau = np.zeros((levels, 7), order="F")

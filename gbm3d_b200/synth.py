@@ -48,3 +48,18 @@ def noisy_image(m: int, n: int, sigma: float, seed: int = 0, dtype=np.float64):
     rng = np.random.Generator(np.random.PCG64(seed + 1_000_003))
     noisy = clean + sigma * rng.standard_normal((m, n))
     return clean, np.asfortranarray(noisy.astype(dtype))
+
+
+def colored_noisy_image(m: int, n: int, sigma: float, omega: float = 1.0, seed: int = 0):
+    """(clean, noisy, sigmaPSD): white noise of std sigma filtered by a unit-sum
+    circular Gaussian of width omega (scripts/mainTestColoredNoise.m builds its
+    test noise this way), and its power spectrum sigma^2 |g_hat|^2, the matrix
+    sigma that GBM3D.m takes for coloured noise."""
+    from .options import gaussian_psf_hat
+    clean = clean_image(m, n, seed)
+    rng = np.random.Generator(np.random.PCG64(seed + 2_000_003))
+    ghat = gaussian_psf_hat((m, n), omega)
+    w = sigma * rng.standard_normal((m, n))
+    noise = np.real(np.fft.ifft2(np.fft.fft2(w) * ghat))
+    psd = sigma ** 2 * np.abs(ghat) ** 2
+    return clean, np.asfortranarray(clean + noise), np.asfortranarray(psd)

@@ -158,6 +158,14 @@ int gbm3d_denoiseAndAggregateWie(gbm3d_ctx* ctx, const float* V1, const float* V
 int gbm3d_denoise(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
                   const gbm3d_opts* opts, double* U, double* U1);
 
+/* [U,out] = GBM3D(I,sigmaPSD,opts) for coloured noise (GBM3D.m:33-35): the
+ * caller passes tau = getColoredTau(levels, sigmaPSD) (levels x 7),
+ * sigmaWie = getColoredWie(sigmaPSD, blockSizeWie) (blockSizeWie^2, column-
+ * major) and sigma_match = mean(sqrt(sigmaPSD(:))), the scalar the matchers
+ * use (matchBlocksCPU.m:21).  Host pointers, as gbm3d_denoise. */
+int gbm3d_denoise_colored(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma_match, const double* tau,
+                          const double* sigmaWie, const gbm3d_opts* opts, double* U, double* U1);
+
 /* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
  * the context stream (synchronise before reading U). */
 int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,

@@ -790,8 +790,21 @@ void haar_filters(orc_filters* f) {
 }
 
 // GBM3D.m:15-83
+// tau_in (levels x 7) and sigwie_in (dw x dw) replace sigma * getTau and the
+// scalar Wiener sigma on the coloured-noise path (GBM3D.m:30-36); sigma is then
+// mean(sqrt(sigmaPSD)) as the matchers use it (matchBlocksCPU.m:21).
+template <class T>
+void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, double* Uout, double* U1out,
+           const double* tau_in, const double* sigwie_in);
+
 template <class T>
 void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, double* Uout, double* U1out) {
+  gbm3d<T>(I0, m0, n0, sigma, o, Uout, U1out, nullptr, nullptr);
+}
+
+template <class T>
+void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, double* Uout, double* U1out,
+           const double* tau_in, const double* sigwie_in) {
   const int d = o->blockSize, dw = o->blockSizeWie, d2 = o->matchSize, K = o->numMax;
   const int st1 = o->refStride > 0 ? o->refStride : d, st2 = o->refStrideWie > 0 ? o->refStrideWie : dw;
   // GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
@@ -809,6 +822,7 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
   std::vector<double> tau(o->levels * 7);
   get_tau(o->levels, o->tauMode, tau.data());
   for (auto& t : tau) t *= sigma;
+  if (tau_in) std::copy(tau_in, tau_in + o->levels * 7, tau.begin());
   orc_filters f;
   if (o->wavelet == 1) haar_filters(&f);
   else bior_filters(&f);
@@ -864,7 +878,8 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
     MatchOut<T> mo{S.data(), nullptr, nullptr, V1.data(), V2.data()};
     match_blocks<T>(Ip.data(), In.data(), Mp, Np, dw, d2, K, K, 0.0, false, mo, st2);
     double sg = sigma;
-    denoise_wiener<T>(V1.data(), V2.data(), M, N, dw, d2, K, S.data(), &sg, 0, 0, u.data(), w.data(), st2);
+    denoise_wiener<T>(V1.data(), V2.data(), M, N, dw, d2, K, S.data(), sigwie_in ? sigwie_in : &sg,
+                      sigwie_in ? 1 : 0, 0, u.data(), w.data(), st2);
     circshift2(u.data(), Mp, Np, -s, &Us[ii * px]);
     circshift2(w.data(), Mp, Np, -s, &Ws[ii * px]);
   }
@@ -1170,6 +1185,16 @@ int orc_gbm3d(int prec, const double* I, int m, int n, double sigma, const orc_o
   if (o->Wiener && (o->blockSize - o->blockSizeWie) % std::gcd(st1, st2) != 0) return 1;
   if (prec == 32) gbm3d<float>(I, m, n, sigma, o, U, U1);
   else gbm3d<double>(I, m, n, sigma, o, U, U1);
+  return 0;
+}
+
+int orc_gbm3d_colored(int prec, const double* I, int m, int n, double sigma_match, const double* tau,
+                      const double* sigwie, const orc_opts* o, double* U, double* U1) {
+  const int st1 = o->refStride > 0 ? o->refStride : o->blockSize;
+  const int st2 = o->refStrideWie > 0 ? o->refStrideWie : o->blockSizeWie;
+  if (o->Wiener && (o->blockSize - o->blockSizeWie) % std::gcd(st1, st2) != 0) return 1;
+  if (prec == 32) gbm3d<float>(I, m, n, sigma_match, o, U, U1, tau, sigwie);
+  else gbm3d<double>(I, m, n, sigma_match, o, U, U1, tau, sigwie);
   return 0;
 }
 

@@ -260,6 +260,22 @@ def GBM3D(I, sigma, opts, prec=32):
     return U, U1
 
 
+def GBM3D_colored(I, sigma_match, tau, sigmaWie, opts, prec=32):
+    """GBM3D.m:33-35 for coloured noise: tau (levels x 7) and sigmaWie
+    (blockSizeWie^2) given, sigma_match = mean(sqrt(sigmaPSD(:)))."""
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n = I.shape
+    U = np.zeros((m, n), order="F")
+    U1 = np.zeros((m, n), order="F")
+    oc = make_opts(opts)
+    tau = np.asfortranarray(tau, dtype=np.float64)
+    sw = np.asfortranarray(sigmaWie, dtype=np.float64)
+    if lib().orc_gbm3d_colored(prec, _p(I), m, n, C.c_double(sigma_match), _p(tau), _p(sw), C.byref(oc),
+                               _p(U), _p(U1)) != 0:
+        raise ValueError("no padded size lets both reference grids end at the border")
+    return U, U1
+
+
 def matchBlocksGPU(I, sigma, opts, prec=32):
     """S = matchBlocksGPU(I, sigma, opts) (source/matchBlocksGPU.m:1): global
     circular search; S indexes the m x n image.  Returns S, counts and the

@@ -230,3 +230,14 @@ def test_GBM3D_distributed_cuda_matches_oracle_tiles(gpu):
     Uo, outo = D.GBM3D_distributed(noisy, 25.0, {"profile": "default"}, backend=oracle_backend())
     assert np.array_equal(out["U2"], outo["U2"]) and np.array_equal(U, Uo)
     assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255) + 5
+
+
+@pytest.mark.parametrize("m,n,sigma,omega,seed", [(64, 64, 25.0, 1.0, 31), (96, 80, 40.0, 2.0, 32)])
+def test_GBM3D_colored_noise(gpu, oracle, m, n, sigma, omega, seed):
+    """GBM3D.m:33-35: matrix sigma (sigma^2 * PSD) -> getColoredTau / getColoredWie."""
+    clean, noisy, psd = synth.colored_noisy_image(m, n, sigma, omega=omega, seed=seed)
+    o = _opts()
+    U, out = gpu.GBM3D(noisy, psd, o)
+    Uo, U1o = oracle.GBM3D_colored(noisy, float(np.mean(np.sqrt(psd))), out["tau"], out["sigmaWie"], o, prec=32)
+    assert np.array_equal(out["U1"], U1o) and np.array_equal(U, Uo)
+    assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255)

@@ -180,3 +180,38 @@ def test_median_filter_matches_scipy(oracle):
     rng = np.random.default_rng(0)
     V = rng.normal(size=(24, 20, 16))
     assert np.array_equal(oracle.medfilt3(V, prec=64), nd.median_filter(V, size=3, mode="nearest"))
+
+
+def test_colored_thresholds_white_psd():
+    """A flat PSD sigma^2 gives tau = 6 sigma in every band (getColoredTau.m:51-57)
+    and sigmaWie = sigma for every DCT coefficient (Parseval, getColoredWie.m:10-18)."""
+    for sigma in (5.0, 25.0):
+        psd = np.full((64, 48), sigma ** 2)
+        assert np.allclose(options.getColoredTau(3, psd), 6 * sigma, rtol=1e-12)
+        assert np.allclose(options.getColoredWie(psd, 8), sigma, rtol=1e-12)
+
+
+def test_colored_thresholds_follow_the_spectrum():
+    """Low-pass noise: coarse bands see more noise than fine ones; the Wiener
+    sigmas fall from the DC coefficient towards high frequencies."""
+    _, _, psd = synth.colored_noisy_image(64, 64, 25.0, omega=1.0, seed=3)
+    tau = options.getColoredTau(3, psd)
+    assert np.all(tau[2] > tau[0])
+    sw = options.getColoredWie(psd, 8)
+    assert sw[0, 0] > sw[7, 7] and np.all(sw > 0)
+
+
+def test_resize_identity_and_constant():
+    a = np.random.default_rng(0).normal(size=(12, 9))
+    assert np.allclose(options._resize_bilinear_aa(a, 12, 0), a)
+    assert np.allclose(options._resize_bilinear_aa(np.full((40, 3), 2.5), 8, 0), 2.5)
+
+
+def test_colored_pipeline_oracle_denoises(oracle):
+    clean, noisy, psd = synth.colored_noisy_image(64, 64, 25.0, omega=1.0, seed=4)
+    o = options.resolve_opts({"profile": "default"})
+    tau = options.getColoredTau(o["levels"], psd)
+    sw = options.getColoredWie(psd, o["blockSizeWie"])
+    U, _ = oracle.GBM3D_colored(noisy, float(np.mean(np.sqrt(psd))), tau, sw, o, prec=64)
+    # strongly correlated noise (std 7 after the blur) is the hard case: a smaller gain
+    assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255) + 1
