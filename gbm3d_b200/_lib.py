@@ -75,6 +75,12 @@ _SIGS = {
     "gbm3d_kernel_time": (C.c_int, [_P, C.c_char_p, _P]),
     "gbm3d_filters_from_bank": (C.c_int, [_P, _P, C.c_int, C.c_int, C.POINTER(gbm3d_filters)]),
     "gbm3d_tc_selfcheck": (C.c_int, [_P, _P, _P, _P]),
+    "gbm3d_pilot_param_count": (C.c_int, []),
+    "gbm3d_pilot_set_params": (C.c_int, [_P, _P]),
+    "gbm3d_pilot_get_params": (C.c_int, [_P, _P]),
+    "gbm3d_pilot_forward": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P]),
+    "gbm3d_pilot_train_step": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_float, _P]),
+    "gbm3d_pilot_gradients": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "gbm3d_denoise_colored": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, _P, _P, C.POINTER(gbm3d_opts), _P,
                                         _P]),
     "gbm3d_matchBlocks_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P, _P]),

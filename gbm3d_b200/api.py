@@ -80,9 +80,9 @@ def c_opts(opts: dict) -> gbm3d_opts:
         raise GBM3DError(5, f"wname '{wn}': the pipeline's banks are 'bior' (bior1.5 x Haar) and 'haar'")
     c.wavelet = 1 if wn == "haar" else 0
     form = o.get("form", "plain")
-    if form not in ("plain", "precision"):
-        raise GBM3DError(5, f"form '{form}': 'plain' or 'precision'")
-    c.form = 1 if form == "precision" else 0
+    if form not in ("plain", "precision", "learned"):
+        raise GBM3DError(5, f"form '{form}': 'plain', 'precision' or 'learned'")
+    c.form = {"plain": 0, "precision": 1, "learned": 2}[form]
     return c
 
 

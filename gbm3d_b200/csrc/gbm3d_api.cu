@@ -40,7 +40,10 @@ struct gbm3d_ctx {
   std::vector<cudaEvent_t> kpool;
   std::vector<std::string> krec;
   int launches = 0;
-  int form = 0;         // 0 plain, 1 precision form (set from the options of the current call)
+  int form = 0;         // 0 plain, 1 precision form, 2 learned pilot (set from the current call's options)
+  bool pilot_ready = false;  // pilot parameters loaded (gbm3d_pilot_set_params)
+  int pilot_step = 0;        // Adam steps taken
+  int sms = 148;
   int* flag = nullptr;  // device status word (non-finite input)
 };
 
@@ -323,7 +326,8 @@ void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
     argfail(c, "refStrideWie must be in 1..blockSizeWie (0: blockSizeWie)");
   if (o->filtType != 0 && o->filtType != 1) argfail(c, "unrecognized filtering");  // denoiseAndAggregateGPU.m:54
   if (o->wavelet != 0 && o->wavelet != 1) argfail(c, "wavelet must be 0 (bior1.5 x Haar) or 1 (3D Haar)");
-  if (o->form != 0 && o->form != 1) argfail(c, "form must be 0 (plain) or 1 (precision)");
+  if (o->form < 0 || o->form > 2) argfail(c, "form must be 0 (plain), 1 (precision) or 2 (learned pilot)");
+  if (o->form == 2 && !c->pilot_ready) argfail(c, "learned pilot: no parameters loaded (gbm3d_pilot_set_params)");
   c->form = o->form;
 }
 
@@ -573,6 +577,46 @@ void opts_dims(const gbm3d_opts* o, int& d, int& dw, int& d2, int& K) {
 }
 
 // The whole GBM3D.m pipeline on device buffers.
+// ---- learned pilot state -----------------------------------------------------------
+
+PilotNet pilot_net(gbm3d_ctx* c) {
+  PilotNet P{};
+  P.master = buf<float>(c, "pl.master", pilot_param_count());
+  static const int co[PILOT_LAYERS] = {48, 48, 48, 48, 48, 48, 48, 16}, ci[PILOT_LAYERS] = {16, 48, 48, 48, 48, 48, 48, 48};
+  for (int l = 0; l < PILOT_LAYERS; ++l) {
+    P.wfwd[l] = buf<uint16_t>(c, ("pl.wf" + std::to_string(l)).c_str(), (size_t)9 * co[l] * ci[l]);
+    P.wbwd[l] = buf<uint16_t>(c, ("pl.wb" + std::to_string(l)).c_str(), (size_t)9 * co[l] * ci[l]);
+  }
+  return P;
+}
+
+// NHWC activation buffers: acts[0] 16 channels, acts[1..7] 48 channels
+void pilot_acts(gbm3d_ctx* c, size_t px, uint16_t** acts) {
+  acts[0] = buf<uint16_t>(c, "pl.a0", px * 16);
+  for (int l = 1; l < PILOT_LAYERS; ++l) acts[l] = buf<uint16_t>(c, ("pl.a" + std::to_string(l)).c_str(), px * 48);
+}
+
+void check_pilot_dims(gbm3d_ctx* c, int nimg, int H, int W) {
+  if (!c->pilot_ready) argfail(c, "learned pilot: no parameters loaded (gbm3d_pilot_set_params)");
+  if (nimg < 1 || H < 1 || W < 1 || (size_t)nimg * H * W > ((size_t)1 << 31)) argfail(c, "pilot: image sizes out of range");
+}
+
+// pilot (fp32, [image][row][column]) of nimg noisy images of H x W, sigma per image (device)
+void run_pilot(gbm3d_ctx* c, const float* img, const float* sig, int nimg, int H, int W, float* out) {
+  const size_t px = (size_t)nimg * H * W;
+  uint16_t* acts[PILOT_LAYERS];
+  pilot_acts(c, px, acts);
+  launched(c, pilot_pack_input(img, sig, nimg, H, W, acts[0], c->st), "pilot_pack");
+  launched(c, pilot_forward(pilot_net(c), img, nimg, H, W, acts, out, c->flag, c->sms, c->st), "pilot_conv");
+}
+
+__global__ void k_crop_f2d(const float* __restrict__ v, int Mp, double* __restrict__ out, int m, int n) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, col = blockIdx.y;
+  if (r < m && col < n) out[r + (size_t)col * m] = (double)v[r + (size_t)col * Mp];
+}
+
+__global__ void k_fill_f(float* __restrict__ p, float v) { p[0] = v; }
+
 // tau_in (levels x 7) and sigwie_in (blockSizeWie^2) replace sigma * getTau
 // and the scalar Wiener sigma on the coloured-noise path (GBM3D.m:30-36);
 // sigma is then what the matchers use, mean(sqrt(sigmaPSD)).
@@ -623,17 +667,39 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     launched(c, cudaGetLastError(), "prep");
   }
 
+  float* Us = buf<float>(c, "p.Us", px);
+  float* Ws = buf<float>(c, "p.Ws", px);
+  double* Ua = buf<double>(c, "p.Ua", px);
+  double* Wa = buf<double>(c, "p.Wa", px);
+  double* U1d = buf<double>(c, "p.U1d", px);
+  float* U1f = buf<float>(c, "p.U1f", px);
+  const bool stale = o->form != 2 && o->Wiener && o->staleWeights && nW < nS;
+  float* Wstale = stale ? buf<float>(c, "p.Wstale", px * (nS - nW)) : nullptr;
+  if (o->form == 2) {
+    // learned pilot in place of step 1: the padded image, column-major Mp x Np,
+    // is the network's [Np rows][Mp columns] image
+    float* sg = buf<float>(c, "pl.sig1", 1);
+    k_fill_f<<<1, 1, 0, c->st>>>(sg, (float)sigma);
+    launched(c, cudaGetLastError(), "fill");
+    {
+      StageTimer t(c, 2);
+      run_pilot(c, If, sg, 1, Np, Mp, U1f);
+    }
+    if (dU1) {
+      k_crop_f2d<<<grid2(m, n), 256, 0, c->st>>>(U1f, Mp, dU1, m, n);
+      launched(c, cudaGetLastError(), "crop");
+    }
+    if (!o->Wiener) {
+      k_crop_f2d<<<grid2(m, n), 256, 0, c->st>>>(U1f, Mp, dU, m, n);
+      launched(c, cudaGetLastError(), "crop");
+      return;
+    }
+  } else {
   // step 1: hard-thresholding estimate over the match spins
   const int M1 = grid_count(Mp, d, st1), N1 = grid_count(Np, d, st1);
   uint32_t* S1 = buf<uint32_t>(c, "p.S1", (size_t)K * M1 * N1);
   int32_t* cnt1 = buf<int32_t>(c, "p.cnt1", (size_t)M1 * N1);
   float* vol = buf<float>(c, "p.vol", (size_t)M1 * d * N1 * d * K);
-  float* Us = buf<float>(c, "p.Us", px);
-  float* Ws = buf<float>(c, "p.Ws", px);
-  double* Ua = buf<double>(c, "p.Ua", px);
-  double* Wa = buf<double>(c, "p.Wa", px);
-  const bool stale = o->Wiener && o->staleWeights && nW < nS;
-  float* Wstale = stale ? buf<float>(c, "p.Wstale", px * (nS - nW)) : nullptr;
   for (int ii = 0; ii < nS; ++ii) {
     const int s = o->matchSpins[ii];
     {
@@ -650,14 +716,13 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
       launched(c, cudaGetLastError(), "shift_copy");
     }
   }
-  double* U1d = buf<double>(c, "p.U1d", px);
-  float* U1f = buf<float>(c, "p.U1f", px);
   k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua, Wa, Mp, Np, U1d, U1f, dU1, m, n);
   launched(c, cudaGetLastError(), "ratio");
   if (!o->Wiener) {
     k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua, Wa, Mp, Np, nullptr, nullptr, dU, m, n);
     launched(c, cudaGetLastError(), "ratio");
     return;
+  }
   }
 
   // step 2: empirical Wiener estimate over the Wiener match spins
@@ -720,6 +785,7 @@ int gbm3d_ctx_create(int device, gbm3d_ctx** out) {
     return GBM3D_ERR_CUDA;
   }
   c->st = c->own;
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   *out = c;
   return GBM3D_OK;
 }
@@ -730,6 +796,7 @@ void gbm3d_ctx_destroy(gbm3d_ctx* c) {
   cudaStreamSynchronize(c->st);
   for (auto& kv : c->bufs) cudaFree(kv.second.first);
   for (auto& e : c->evpool) cudaEventDestroy(e);
+  for (auto& e : c->kpool) cudaEventDestroy(e);
   if (c->flag) cudaFree(c->flag);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -1151,6 +1218,103 @@ static int denoise_host(gbm3d_ctx* c, const double* I, int m, int n, double sigm
 int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,
                   double* U1) {
   return denoise_host(c, I, m, n, sigma, o, U, U1, nullptr, nullptr);
+}
+
+// ---- learned pilot ---------------------------------------------------------------------
+
+int gbm3d_pilot_param_count(void) { return pilot_param_count(); }
+
+int gbm3d_pilot_set_params(gbm3d_ctx* c, const float* params) {
+  return guarded(c, [&] {
+    if (!params) argfail(c, "missing argument");
+    const int np = pilot_param_count();
+    PilotNet P = pilot_net(c);
+    float* m1 = buf<float>(c, "pl.m1", np);
+    float* m2 = buf<float>(c, "pl.m2", np);
+    ck(c, cudaMemcpyAsync(const_cast<float*>(P.master), params, (size_t)np * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(m1, 0, (size_t)np * 4, c->st), "memset");
+    ck(c, cudaMemsetAsync(m2, 0, (size_t)np * 4, c->st), "memset");
+    launched(c, pilot_pack_weights(P.master, P.wfwd, P.wbwd, c->st), "pilot_weights");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    c->pilot_ready = true;
+    c->pilot_step = 0;
+  });
+}
+
+int gbm3d_pilot_get_params(gbm3d_ctx* c, float* params) {
+  return guarded(c, [&] {
+    if (!params) argfail(c, "missing argument");
+    if (!c->pilot_ready) argfail(c, "learned pilot: no parameters loaded (gbm3d_pilot_set_params)");
+    PilotNet P = pilot_net(c);
+    ck(c, cudaMemcpyAsync(params, P.master, (size_t)pilot_param_count() * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+  });
+}
+
+int gbm3d_pilot_forward(gbm3d_ctx* c, const float* img, const float* sigma, int nimg, int H, int W, float* pilot) {
+  return guarded(c, [&] {
+    if (!img || !sigma || !pilot) argfail(c, "missing argument");
+    check_pilot_dims(c, nimg, H, W);
+    run_pilot(c, img, sigma, nimg, H, W, pilot);
+  });
+}
+
+// forward + loss + backward; with lr > 0 also one Adam step.  grad (host, may be
+// null) receives the parameter gradients, loss (host, may be null) the loss.
+static int pilot_train(gbm3d_ctx* c, const float* img, const float* target, const float* sigma, int nimg, int H,
+                       int W, float lr, float* grad_host, float* loss) {
+  return guarded(c, [&] {
+    if (!img || !target || !sigma) argfail(c, "missing argument");
+    check_pilot_dims(c, nimg, H, W);
+    const size_t px = (size_t)nimg * H * W;
+    const int np = pilot_param_count();
+    PilotNet P = pilot_net(c);
+    uint16_t* acts[PILOT_LAYERS];
+    pilot_acts(c, px, acts);
+    float* out = buf<float>(c, "pl.out", px);
+    uint16_t* dy16 = buf<uint16_t>(c, "pl.dy16", px * 16);
+    uint16_t* gA = buf<uint16_t>(c, "pl.gA", px * 48);
+    uint16_t* gB = buf<uint16_t>(c, "pl.gB", px * 48);
+    const int nparts = 2 * c->sms;
+    float* part = buf<float>(c, "pl.part", (size_t)nparts * (9 * 48 * 48 + 48));
+    float* grad = buf<float>(c, "pl.grad", np);
+    float* lpart = buf<float>(c, "pl.lpart", 256);
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    launched(c, pilot_pack_input(img, sigma, nimg, H, W, acts[0], c->st), "pilot_pack");
+    launched(c, pilot_forward(P, img, nimg, H, W, acts, out, c->flag, c->sms, c->st), "pilot_conv");
+    launched(c, pilot_backward(P, out, target, nimg, H, W, acts, dy16, gA, gB, part, nparts, grad, lpart, c->flag,
+                               c->sms, c->st), "pilot_backward");
+    if (lr > 0.f) {
+      c->pilot_step += 1;
+      launched(c, pilot_adam(const_cast<float*>(P.master), grad, buf<float>(c, "pl.m1", np), buf<float>(c, "pl.m2", np),
+                             np, lr, c->pilot_step, c->st), "pilot_adam");
+      launched(c, pilot_pack_weights(P.master, P.wfwd, P.wbwd, c->st), "pilot_weights");
+    }
+    float lp[256];
+    ck(c, cudaMemcpyAsync(lp, lpart, sizeof(lp), cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (grad_host) ck(c, cudaMemcpyAsync(grad_host, grad, (size_t)np * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    report_flag(c, flag);
+    double s = 0.0;
+    for (int i = 0; i < 256; ++i) s += lp[i];
+    if (loss) *loss = (float)(s / (double)px);
+  });
+}
+
+int gbm3d_pilot_train_step(gbm3d_ctx* c, const float* img, const float* target, const float* sigma, int nimg, int H,
+                           int W, float lr, float* loss) {
+  if (!(lr > 0.f)) {
+    if (c) c->err = "lr must be positive";
+    return GBM3D_ERR_ARG;
+  }
+  return pilot_train(c, img, target, sigma, nimg, H, W, lr, nullptr, loss);
+}
+
+int gbm3d_pilot_gradients(gbm3d_ctx* c, const float* img, const float* target, const float* sigma, int nimg, int H,
+                          int W, float* grad, float* loss) {
+  return pilot_train(c, img, target, sigma, nimg, H, W, 0.f, grad, loss);
 }
 
 int gbm3d_denoise_colored(gbm3d_ctx* c, const double* I, int m, int n, double sigma_match, const double* tau,

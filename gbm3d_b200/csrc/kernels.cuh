@@ -119,6 +119,25 @@ cudaError_t launch_match_global(int d, const GlobalMatchArgs& A, cudaStream_t st
 // in-place sym4 prefilter; work holds 8 * m * n floats
 cudaError_t launch_sym4_prefilter(float* I, int m, int n, float tau, float* work, cudaStream_t st);
 
+// ---- learned pilot (pilot.cu) ----------------------------------------------------------
+constexpr int PILOT_LAYERS = 8;
+struct PilotNet {
+  const float* master;           // fp32 parameters: per layer W [9][co][ci] then b [co]
+  uint16_t* wfwd[PILOT_LAYERS];  // bf16 [9][COUT][CIN], channels padded to 16 / 48
+  uint16_t* wbwd[PILOT_LAYERS];  // bf16 data-gradient weights (flipped taps, transposed channels)
+};
+int pilot_param_count();
+int pilot_param_offset(int layer);
+cudaError_t pilot_pack_weights(const float* master, uint16_t* const* wfwd, uint16_t* const* wbwd, cudaStream_t st);
+cudaError_t pilot_pack_input(const float* img, const float* sig, int nimg, int H, int W, uint16_t* out,
+                             cudaStream_t st);
+cudaError_t pilot_forward(const PilotNet& P, const float* img, int nimg, int H, int W, uint16_t* const* acts,
+                          float* pilot, int* err, int sms, cudaStream_t st);
+cudaError_t pilot_backward(const PilotNet& P, const float* pilot, const float* target, int nimg, int H, int W,
+                           uint16_t* const* acts, uint16_t* dy16, uint16_t* gA, uint16_t* gB, float* part,
+                           int nparts, float* grad, float* loss_part, int* err, int sms, cudaStream_t st);
+cudaError_t pilot_adam(float* w, const float* g, float* m1, float* m2, int n, float lr, int step, cudaStream_t st);
+
 // ---- tensor-core self-check (tc_check.cu) -------------------------------------------
 cudaError_t launch_tc_gemm_check(const uint16_t* A, const uint16_t* B, float* C, int* err, cudaStream_t st);
 

@@ -65,8 +65,9 @@ typedef struct gbm3d_opts {
   int wavelet; /* step-1 bank of gbm3d_denoise: 0 = bior1.5 x Haar (GBM3D.m:40), 1 = 3D Haar */
   /* 0 plain (the reference's arithmetic, FP32); 1 precision form: block
    * distances on the bf16 tensor cores with an exact FP32 re-rank of the 32
-   * best per reference, and Kahan-compensated FP32 aggregation.  Not in the
-   * reference. */
+   * best per reference, and Kahan-compensated FP32 aggregation; 2 learned
+   * pilot: the step-1 estimate comes from the pilot network (gbm3d_pilot_*).
+   * Not in the reference. */
   int form;
 } gbm3d_opts;
 
@@ -165,6 +166,26 @@ int gbm3d_denoise(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
  * use (matchBlocksCPU.m:21).  Host pointers, as gbm3d_denoise. */
 int gbm3d_denoise_colored(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma_match, const double* tau,
                           const double* sigmaWie, const gbm3d_opts* opts, double* U, double* U1);
+
+/* ---- learned pilot (opts.form = 2) -------------------------------------------------
+ * A residual CNN (8 layers of 3x3 convolutions, 48 channels, bf16 weights and
+ * activations, fp32 accumulation on the tensor cores) that produces the step-1
+ * estimate from the noisy image and sigma; step 2 (Wiener) then runs as usual.
+ * Not in the reference.  Parameters: fp32 vector of gbm3d_pilot_param_count()
+ * values, per layer W [9][out][in] (tap = 3*dy + dx) then the bias [out];
+ * inputs 2 (noisy/255, sigma/255), outputs 48, 48, ..., 1.  Images for the
+ * pilot calls are fp32 device arrays [image][row][column]; sigma one float per
+ * image (device).  A column-major m x n image is the [n][m] image here. */
+int gbm3d_pilot_param_count(void);
+int gbm3d_pilot_set_params(gbm3d_ctx* ctx, const float* params /* host */);
+int gbm3d_pilot_get_params(gbm3d_ctx* ctx, float* params /* host */);
+int gbm3d_pilot_forward(gbm3d_ctx* ctx, const float* img, const float* sigma, int nimg, int H, int W, float* pilot);
+/* One Adam step (lr > 0) on mean((pilot - target)^2); *loss (host) gets the loss. */
+int gbm3d_pilot_train_step(gbm3d_ctx* ctx, const float* img, const float* target, const float* sigma, int nimg,
+                           int H, int W, float lr, float* loss);
+/* Loss gradients (host, gbm3d_pilot_param_count() floats) without an update. */
+int gbm3d_pilot_gradients(gbm3d_ctx* ctx, const float* img, const float* target, const float* sigma, int nimg,
+                          int H, int W, float* grad, float* loss);
 
 /* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
  * the context stream (synchronise before reading U). */
