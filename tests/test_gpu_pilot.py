@@ -15,8 +15,7 @@ import sys
 import numpy as np
 import pytest
 
-sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle"))
-import pilot_ref as R  # noqa: E402
+from oracle import pilot_ref as R  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 

@@ -9,8 +9,7 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle"))
-import pilot_ref as R  # noqa: E402
+from oracle import pilot_ref as R  # noqa: E402
 
 
 def test_param_layout():
