@@ -75,6 +75,7 @@ _SIGS = {
     "gbm3d_kernel_time": (C.c_int, [_P, C.c_char_p, _P]),
     "gbm3d_filters_from_bank": (C.c_int, [_P, _P, C.c_int, C.c_int, C.POINTER(gbm3d_filters)]),
     "gbm3d_tc_selfcheck": (C.c_int, [_P, _P, _P, _P]),
+    "gbm3d_ctx_synchronize": (C.c_int, [_P]),
     "gbm3d_pilot_param_count": (C.c_int, []),
     "gbm3d_pilot_set_params": (C.c_int, [_P, _P]),
     "gbm3d_pilot_get_params": (C.c_int, [_P, _P]),
@@ -122,6 +123,7 @@ class Context:
         if rc != GBM3D_OK:
             raise GBM3DError(rc, f"cannot create a context on CUDA device {device}")
         self.h = h
+        self.device = device
 
     def check(self, rc: int) -> None:
         if rc != GBM3D_OK:

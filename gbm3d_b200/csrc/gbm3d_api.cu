@@ -833,6 +833,15 @@ int gbm3d_stage_times(const gbm3d_ctx* c, float* ms, int n) {
 
 int gbm3d_last_launch_count(const gbm3d_ctx* c) { return c ? c->launches : 0; }
 
+int gbm3d_ctx_synchronize(gbm3d_ctx* c) {
+  if (!c) return GBM3D_ERR_ARG;
+  if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
+    c->err = "stream synchronisation failed";
+    return GBM3D_ERR_CUDA;
+  }
+  return GBM3D_OK;
+}
+
 int gbm3d_kernel_time(const gbm3d_ctx* c, const char* name, float* total_ms) {
   if (!c || !name || !total_ms || !c->timing) return -1;
   float acc = 0.f;

@@ -18,6 +18,7 @@ more than 0.1 dB below the plain step's, the image takes the plain path.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import ctypes as C
 import math
 import os
@@ -40,6 +41,23 @@ def dense_opts(**kw) -> dict:
     o.update(blockSize=8, blockSizeWie=8, matchSize=32, numMax=16, numMin=16, refStride=3, refStrideWie=3)
     o.update(kw)
     return o
+
+
+@contextlib.contextmanager
+def shared_stream(ctx=None):
+    """Run torch's work and the library's on one explicit stream, so device
+    buffers torch fills are ready when the library reads them (and back)."""
+    import torch
+    ctx = ctx or context()
+    torch.cuda.synchronize()  # work torch queued earlier (on any stream) is done
+    s = torch.cuda.Stream(torch.device("cuda", ctx.device))
+    ctx.set_stream(s.cuda_stream)
+    try:
+        with torch.cuda.stream(s):
+            yield s
+    finally:
+        s.synchronize()
+        ctx.set_stream(None)
 
 
 def param_count() -> int:
@@ -80,11 +98,15 @@ def load(path: str = WEIGHTS, ctx=None) -> np.ndarray:
 
 
 def forward_device(img, sig, out, ctx=None) -> None:
-    """img, out: torch float32 [N, H, W] on the device; sig: torch float32 [N]."""
+    """img, out: torch float32 [N, H, W] on the device; sig: torch float32 [N].
+    Runs on torch's current stream and returns when the output is ready."""
+    import torch
     ctx = ctx or context()
     N, H, W = img.shape
+    torch.cuda.current_stream().synchronize()
     ctx.check(lib().gbm3d_pilot_forward(ctx.h, C.c_void_p(img.data_ptr()), C.c_void_p(sig.data_ptr()), N, H, W,
                                         C.c_void_p(out.data_ptr())))
+    ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
 
 
 def pilot_image(I, sigma, ctx=None) -> np.ndarray:
@@ -148,6 +170,15 @@ def train(steps: int = 3000, batch: int = 32, lr: float = 1e-3, n_crops: int = 2
     losses = []
     loss = C.c_float(0.0)
     t0 = time.time()
+    with shared_stream(ctx):
+        _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, loss, t0, log)
+    return get_params(ctx), losses
+
+
+def _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, loss, t0, log):
+    import torch
+    dev = xb.device
+    batch = xb.shape[0]
     for step in range(steps):
         idx = torch.randint(0, noisy.shape[0], (batch,), generator=gen).to(dev)
         torch.index_select(noisy, 0, idx, out=xb)
@@ -161,7 +192,6 @@ def train(steps: int = 3000, batch: int = 32, lr: float = 1e-3, n_crops: int = 2
         if log and (step % 200 == 0 or step == steps - 1):
             log(f"step {step}: loss {np.mean(losses[-50:]):.3f} (RMSE {math.sqrt(np.mean(losses[-50:])):.3f}), "
                 f"{time.time() - t0:.1f}s")
-    return get_params(ctx), losses
 
 
 # ---- fallback gate --------------------------------------------------------------------------
@@ -207,9 +237,38 @@ def GBM3D_learned(I, sigma, opts=None, ctx=None, use_gate: bool = True):
     return U, out
 
 
+def evaluate(size: int = 1024, sigmas=(15.0, 25.0, 50.0), seed: int = 900, ctx=None, log=print) -> list[dict]:
+    """PSNR (vs the clean image) of the plain 2-step method, the learned-pilot
+    method and the learned network's untrained initialisation, per sigma."""
+    ctx = ctx or context()
+    trained = get_params(ctx)
+    rows = []
+    for k, sigma in enumerate(sigmas):
+        clean, noisy = synth.noisy_image(size, size, sigma, seed=seed + k)
+        o = dense_opts()
+        Up, outp = api.GBM3D(noisy, sigma, dict(o, form="plain"), ctx=ctx)
+        Ul, outl = GBM3D_learned(noisy, sigma, o, ctx=ctx)
+        set_params(init_params(0), ctx)
+        Uu, _ = api.GBM3D(noisy, sigma, dict(o, form="learned"), ctx=ctx)
+        set_params(trained, ctx)
+        row = {"sigma": sigma, "psnr_noisy": options.myPSNR(clean, noisy, 255),
+               "psnr_plain": options.myPSNR(clean, Up, 255), "psnr_learned": options.myPSNR(clean, Ul, 255),
+               "psnr_untrained": options.myPSNR(clean, Uu, 255),
+               "psnr_step1_plain": options.myPSNR(clean, outp["U1"], 255),
+               "psnr_step1_learned": options.myPSNR(clean, outl["U1"], 255),
+               "path": outl["path"], "gate": outl["gate"]}
+        rows.append(row)
+        if log:
+            log(row)
+    return rows
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
+    ev = sub.add_parser("eval")
+    ev.add_argument("--size", type=int, default=1024)
+    ev.add_argument("--weights", default=WEIGHTS)
     t = sub.add_parser("train")
     t.add_argument("--steps", type=int, default=3000)
     t.add_argument("--batch", type=int, default=32)
@@ -220,6 +279,10 @@ def main():
     a = ap.parse_args()
     from . import build
     build.build()
+    if a.cmd == "eval":
+        load(a.weights)
+        evaluate(a.size)
+        return
     params, losses = train(a.steps, a.batch, a.lr, a.crops, seed=a.seed)
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     np.save(a.out, params)

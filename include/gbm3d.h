@@ -87,6 +87,8 @@ int gbm3d_ctx_create(int device, gbm3d_ctx** out);
 void gbm3d_ctx_destroy(gbm3d_ctx* ctx);
 /* Run subsequent work on this cudaStream_t (NULL = the context's own stream). */
 int gbm3d_ctx_set_stream(gbm3d_ctx* ctx, void* cuda_stream);
+/* Wait until the context's stream has finished all queued work. */
+int gbm3d_ctx_synchronize(gbm3d_ctx* ctx);
 const char* gbm3d_last_error(const gbm3d_ctx* ctx);
 int gbm3d_version(void);
 

@@ -60,11 +60,14 @@ def test_pilot_gradients_match_reference(gpu):
     sig = rng.uniform(5, 50, N)
     p = _params(2)
     pilot.set_params(p)
+    import torch
     ctx = context()
     g = np.zeros(pilot.param_count(), dtype=np.float32)
     loss = C.c_float(0)
-    ctx.check(lib().gbm3d_pilot_gradients(ctx.h, C.c_void_p(_dev(img).data_ptr()), C.c_void_p(_dev(tgt).data_ptr()),
-                                          C.c_void_p(_dev(sig).data_ptr()), N, H, W, g.ctypes.data_as(C.c_void_p),
+    di, dt, ds = _dev(img), _dev(tgt), _dev(sig)
+    torch.cuda.synchronize()  # the inputs are on the device before the library's stream reads them
+    ctx.check(lib().gbm3d_pilot_gradients(ctx.h, C.c_void_p(di.data_ptr()), C.c_void_p(dt.data_ptr()),
+                                          C.c_void_p(ds.data_ptr()), N, H, W, g.ctypes.data_as(C.c_void_p),
                                           C.byref(loss)))
     ref, lref = R.gradients(p, img, sig, tgt)
     assert abs(loss.value - lref) <= 1e-2 * lref
