@@ -269,3 +269,46 @@ def GBM3D_device(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dic
     co = c_opts(_opt.resolve_opts(opts))
     ctx.check(lib().gbm3d_denoise_device(ctx.h, C.c_void_p(I_ptr), m, n, float(sigma), C.byref(co),
                                          C.c_void_p(U_ptr), C.c_void_p(U1_ptr or 0)))
+
+
+def GBM3D_batch(images, sigmas, opts: dict | None = None, use_graph: bool = True, ctx: Context | None = None,
+                outputs=None):
+    """Batched form: denoise a list of device images (torch float64 tensors of
+    shape (n, m), i.e. column-major m x n arrays) with one option set in one
+    call; with use_graph the launch sequence is captured once into a CUDA graph
+    and replayed when the same batch is denoised again.  Returns the outputs
+    (allocated like the inputs unless given) once the work has finished."""
+    import torch
+    ctx = ctx or context()
+    o = _opt.resolve_opts(opts)
+    k = len(images)
+    outs = outputs if outputs is not None else [torch.empty_like(x) for x in images]
+    Ip = (C.c_void_p * k)(*[x.data_ptr() for x in images])
+    Up = (C.c_void_p * k)(*[u.data_ptr() for u in outs])
+    ms = (C.c_int * k)(*[int(x.shape[1]) for x in images])
+    ns = (C.c_int * k)(*[int(x.shape[0]) for x in images])
+    sg = (C.c_double * k)(*[float(s) for s in sigmas])
+    co = c_opts(o)
+    torch.cuda.synchronize()
+    ctx.check(lib().gbm3d_denoise_batch(ctx.h, k, Ip, ms, ns, sg, C.byref(co), Up, 1 if use_graph else 0))
+    ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
+    return outs
+
+
+def GBM3D_rgb(I, sigma, opts: dict | None = None, ctx: Context | None = None):
+    """Colour GBM3D of an m x n x 3 RGB image (host array): opponent colour
+    space, luma-driven block matching, every channel filtered with luma's
+    match sets (gbm3d_denoise_rgb_device)."""
+    import torch
+    ctx = ctx or context()
+    o = _opt.resolve_opts(opts)
+    I = np.asarray(I, dtype=np.float64)
+    m, n, _ = I.shape
+    planes = [torch.from_numpy(np.asfortranarray(I[:, :, k]).ravel(order="F").copy()).cuda() for k in range(3)]
+    outs = [torch.empty_like(p) for p in planes]
+    co = c_opts(o)
+    torch.cuda.synchronize()
+    ctx.check(lib().gbm3d_denoise_rgb_device(ctx.h, *[C.c_void_p(p.data_ptr()) for p in planes], m, n, float(sigma),
+                                             C.byref(co), *[C.c_void_p(u.data_ptr()) for u in outs]))
+    ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
+    return np.stack([u.cpu().numpy().reshape(m, n, order="F") for u in outs], axis=2)

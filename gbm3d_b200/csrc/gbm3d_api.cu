@@ -42,6 +42,9 @@ struct gbm3d_ctx {
   int launches = 0;
   int form = 0;         // 0 plain, 1 precision form, 2 learned pilot (set from the current call's options)
   bool pilot_ready = false;  // pilot parameters loaded (gbm3d_pilot_set_params)
+  // the last batch captured as one CUDA graph, and the geometry it was captured for
+  std::string graph_key;
+  cudaGraphExec_t graph_exec = nullptr;
   int pilot_step = 0;        // Adam steps taken
   int sms = 148;
   int* flag = nullptr;  // device status word (non-finite input)
@@ -313,6 +316,25 @@ __global__ void k_ratio(const double* __restrict__ a, const double* __restrict__
 }
 
 dim3 grid2(int rows, int cols) { return dim3((rows + 255) / 256, cols); }
+
+// Opponent colour transform (Y, U, V) = A (R, G, B) with
+// A = [1/3 1/3 1/3; 1/2 0 -1/2; 1/4 -1/2 1/4], and its inverse
+// R = Y + U + 2V/3, G = Y - 4V/3, B = Y - U + 2V/3.
+__global__ void k_opp(const double* __restrict__ R, const double* __restrict__ G, const double* __restrict__ B,
+                      size_t n, double* __restrict__ Y, double* __restrict__ U, double* __restrict__ V, int inverse) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double a = R[i], b = G[i], c = B[i];
+    if (!inverse) {
+      Y[i] = (a + b + c) / 3.0;
+      U[i] = (a - c) / 2.0;
+      V[i] = (a - 2.0 * b + c) / 4.0;
+    } else {  // (a, b, c) = (Y, U, V)
+      Y[i] = a + b + 2.0 * c / 3.0;
+      U[i] = a - 4.0 * c / 3.0;
+      V[i] = a - b + 2.0 * c / 3.0;
+    }
+  }
+}
 
 // ---- validation ------------------------------------------------------------------
 
@@ -797,6 +819,7 @@ void gbm3d_ctx_destroy(gbm3d_ctx* c) {
   for (auto& kv : c->bufs) cudaFree(kv.second.first);
   for (auto& e : c->evpool) cudaEventDestroy(e);
   for (auto& e : c->kpool) cudaEventDestroy(e);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->flag) cudaFree(c->flag);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -1193,6 +1216,214 @@ int gbm3d_tc_selfcheck(gbm3d_ctx* c, const uint16_t* A, const uint16_t* B, float
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
     if (flag) argfail(c, "tensor-core MMA did not complete in time", GBM3D_ERR_CUDA);
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Colour GBM3D in the opponent space: block matching on the luma channel
+// only, and every channel filtered (hard threshold, then Wiener) and
+// aggregated with luma's match sets, each with its own noise level
+// sigma_c = sigma |row c of A|.  dI / dU: three device planes (R, G, B),
+// float64 column-major m x n.
+void pipeline_rgb(gbm3d_ctx* c, const double* const* dI, int m, int n, double sigma, const gbm3d_opts* o,
+                  double* const* dU) {
+  check_opts(c, o);
+  if (o->form == 2) argfail(c, "the learned pilot is trained on grey images", GBM3D_ERR_UNSUPPORTED);
+  if (!o->Wiener) argfail(c, "the colour form runs both steps", GBM3D_ERR_UNSUPPORTED);
+  int d, dw, d2, K;
+  opts_dims(o, d, dw, d2, K);
+  check_match(c, d, d2, K);
+  check_match(c, dw, d2, K);
+  if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
+  const int st1 = stride1(o), st2 = stride2(o);
+  if ((d - dw) % std::gcd(st1, st2) != 0)
+    argfail(c, "no padded size lets both reference grids end at the border", GBM3D_ERR_UNSUPPORTED);
+  auto padded = [&](int L) {
+    if (st1 == d && st2 == dw && d % dw == 0) return (L + d - 1) / d * d;
+    int p = std::max(L, std::max(d, dw));
+    while ((p - d) % st1 != 0 || (p - dw) % st2 != 0) ++p;
+    return p;
+  };
+  const int Mp = padded(m), Np = padded(n);
+  if (Mp - m > m || Np - n > n) argfail(c, "image smaller than the padding it needs");
+  if (Mp < d2 || Np < d2) argfail(c, "image smaller than matchSize");
+  const int nS = o->nMatchSpins, nW = o->nMatchSpinsWie;
+  if (nS < 1 || nS > 8 || nW < 1 || nW > 8) argfail(c, "match spin count out of range");
+  const size_t px = (size_t)Mp * Np, pm = (size_t)m * n;
+  const double csig[3] = {sigma * std::sqrt(1.0 / 3.0), sigma * std::sqrt(0.5), sigma * std::sqrt(0.375)};
+  gbm3d_filters f;
+  if (o->wavelet == 1) haar3d(&f);
+  else bior(&f);
+  const WaveletBank bk = make_bank(c, &f);
+  std::vector<double> tau1(o->levels * 7);
+  tau_table(o->levels, o->tauMode, tau1.data());
+  const int P = pitch4(Mp + d2);
+
+  // opponent planes, mirror padded to single
+  double* opp[3];
+  float* If[3];
+  for (int ch = 0; ch < 3; ++ch) {
+    opp[ch] = buf<double>(c, ("rgb.opp" + std::to_string(ch)).c_str(), pm);
+    If[ch] = buf<float>(c, ("rgb.If" + std::to_string(ch)).c_str(), px);
+  }
+  ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+  k_opp<<<592, 256, 0, c->st>>>(dI[0], dI[1], dI[2], pm, opp[0], opp[1], opp[2], 0);
+  launched(c, cudaGetLastError(), "opp");
+  for (int ch = 0; ch < 3; ++ch) {
+    k_prep<<<grid2(Mp, Np), 256, 0, c->st>>>(opp[ch], m, n, If[ch], Mp, Np, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+  }
+  float* Us = buf<float>(c, "p.Us", px);
+  float* Ws = buf<float>(c, "p.Ws", px);
+  double *Ua[3], *Wa[3];
+  float* U1f[3];
+  for (int ch = 0; ch < 3; ++ch) {
+    Ua[ch] = buf<double>(c, ("rgb.Ua" + std::to_string(ch)).c_str(), px);
+    Wa[ch] = buf<double>(c, ("rgb.Wa" + std::to_string(ch)).c_str(), px);
+    U1f[ch] = buf<float>(c, ("rgb.U1f" + std::to_string(ch)).c_str(), px);
+  }
+  float* pad = buf<float>(c, "rgb.pad", (size_t)P * (Np + d2));
+  float* pad2 = buf<float>(c, "rgb.pad2", (size_t)P * (Np + d2));
+
+  // step 1: luma matching, per-channel 3D hard thresholding
+  const int M1 = grid_count(Mp, d, st1), N1 = grid_count(Np, d, st1);
+  uint32_t* S1 = buf<uint32_t>(c, "p.S1", (size_t)K * M1 * N1);
+  int32_t* cnt1 = buf<int32_t>(c, "p.cnt1", (size_t)M1 * N1);
+  float* vol = buf<float>(c, "p.vol", (size_t)M1 * d * N1 * d * K);
+  for (int ii = 0; ii < nS; ++ii) {
+    const int s = o->matchSpins[ii];
+    for (int ch = 0; ch < 3; ++ch) {
+      if (ch == 0) {
+        StageTimer t(c, 1);
+        run_match(c, If[0], nullptr, Mp, Np, s, d, d2, K, o->numMin, csig[0], S1, cnt1, vol, nullptr, nullptr, "m1",
+                  st1, o->form);
+      } else {
+        launched(c, launch_make_pad(If[ch], Mp, Np, d2, s, pad, P, c->st), "make_pad");
+        launched(c, launch_gather_volume(pad, P, M1, N1, st1, d, d2, K, S1, cnt1, vol, c->st), "gather");
+      }
+      std::vector<double> tau(tau1);
+      for (auto& t : tau) t *= csig[ch];
+      run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType, st1);
+      k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua[ch], ii == 0);
+      launched(c, cudaGetLastError(), "accum");
+      k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa[ch], ii == 0);
+      launched(c, cudaGetLastError(), "accum");
+    }
+  }
+  for (int ch = 0; ch < 3; ++ch) {
+    k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua[ch], Wa[ch], Mp, Np, nullptr, U1f[ch], nullptr, m, n);
+    launched(c, cudaGetLastError(), "ratio");
+  }
+
+  // step 2: matching on the luma pilot, per-channel Wiener filtering
+  const int M2 = grid_count(Mp, dw, st2), N2 = grid_count(Np, dw, st2);
+  uint32_t* S2 = buf<uint32_t>(c, "p.S2", (size_t)K * M2 * N2);
+  for (int ii = 0; ii < nW; ++ii) {
+    const int s = o->matchSpinsWie[ii];
+    {
+      StageTimer t(c, 4);
+      run_match(c, U1f[0], nullptr, Mp, Np, s, dw, d2, K, K, csig[0], S2, nullptr, nullptr, nullptr, nullptr, "m2",
+                st2, o->form);
+    }
+    for (int ch = 0; ch < 3; ++ch) {
+      launched(c, launch_make_pad(U1f[ch], Mp, Np, d2, s, pad, P, c->st), "make_pad");
+      launched(c, launch_make_pad(If[ch], Mp, Np, d2, s, pad2, P, c->st), "make_pad");
+      WienerArgs A{};
+      A.padP = pad;
+      A.padN = pad2;
+      A.P = P;
+      A.d2 = d2;
+      A.S = S2;
+      A.M = M2;
+      A.N = N2;
+      A.K = K;
+      A.s = st2;
+      fill_wiener_consts(A, dw, &csig[ch], 0, 0);
+      run_wiener_agg(c, A, dw, d2, Us, Ws);
+      k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua[ch], ii == 0);
+      launched(c, cudaGetLastError(), "accum");
+      k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa[ch], ii == 0);
+      launched(c, cudaGetLastError(), "accum");
+    }
+  }
+  for (int ch = 0; ch < 3; ++ch) {
+    k_ratio<<<grid2(Mp, Np), 256, 0, c->st>>>(Ua[ch], Wa[ch], Mp, Np, nullptr, nullptr, opp[ch], m, n);
+    launched(c, cudaGetLastError(), "ratio");
+  }
+  k_opp<<<592, 256, 0, c->st>>>(opp[0], opp[1], opp[2], pm, dU[0], dU[1], dU[2], 1);
+  launched(c, cudaGetLastError(), "opp");
+}
+
+}  // namespace
+
+extern "C" {
+
+int gbm3d_denoise_rgb_device(gbm3d_ctx* c, const double* R, const double* G, const double* B, int m, int n,
+                             double sigma, const gbm3d_opts* o, double* UR, double* UG, double* UB) {
+  return guarded(c, [&] {
+    if (!R || !G || !B || !UR || !UG || !UB) argfail(c, "missing argument");
+    const double* in[3] = {R, G, B};
+    double* out[3] = {UR, UG, UB};
+    pipeline_rgb(c, in, m, n, sigma, o, out);
+  });
+}
+
+int gbm3d_denoise_batch(gbm3d_ctx* c, int nimg, const double* const* I, const int* m, const int* n,
+                        const double* sigma, const gbm3d_opts* o, double* const* U, int use_graph) {
+  return guarded(c, [&] {
+    if (nimg < 1 || !I || !m || !n || !sigma || !U || !o) argfail(c, "missing argument");
+    for (int k = 0; k < nimg; ++k)
+      if (!I[k] || !U[k]) argfail(c, "missing image or output pointer");
+    // largest images first: the workspace reaches its final size on the first ones
+    std::vector<int> ord(nimg);
+    for (int k = 0; k < nimg; ++k) ord[k] = k;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return (long)m[a] * n[a] > (long)m[b] * n[b]; });
+    auto run_all = [&] {
+      for (int k : ord) pipeline(c, I[k], m[k], n[k], sigma[k], o, U[k], nullptr);
+    };
+    if (!use_graph) {
+      run_all();
+      return;
+    }
+    std::string key(reinterpret_cast<const char*>(o), sizeof(*o));
+    for (int k = 0; k < nimg; ++k) {
+      const void* p[2] = {I[k], U[k]};
+      key.append(reinterpret_cast<const char*>(p), sizeof(p));
+      key.append(reinterpret_cast<const char*>(&m[k]), sizeof(int));
+      key.append(reinterpret_cast<const char*>(&n[k]), sizeof(int));
+      key.append(reinterpret_cast<const char*>(&sigma[k]), sizeof(double));
+    }
+    if (c->graph_exec && c->graph_key == key) {  // same batch geometry: replay
+      ck(c, cudaGraphLaunch(c->graph_exec, c->st), "cudaGraphLaunch");
+      c->launches = 1;
+      return;
+    }
+    // eager run (sizes every workspace buffer and produces this call's result),
+    // then the same launch sequence captured once for later calls
+    run_all();
+    const bool tm = c->timing;
+    c->timing = false;
+    ck(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    cudaGraph_t g = nullptr;
+    try {
+      run_all();
+    } catch (...) {
+      cudaStreamEndCapture(c->st, &g);
+      if (g) cudaGraphDestroy(g);
+      c->timing = tm;
+      throw;
+    }
+    c->timing = tm;
+    ck(c, cudaStreamEndCapture(c->st, &g), "cudaStreamEndCapture");
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    ck(c, e, "cudaGraphInstantiate");
+    c->graph_key = key;
   });
 }
 

@@ -27,6 +27,8 @@ size_t match_smem_bytes(int d, int d2);
 cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st);
 cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
                             cudaStream_t st);
+cudaError_t launch_gather_volume(const float* pad, int P, int M, int N, int s, int d, int d2, int K, const uint32_t* S,
+                                 const int32_t* cnt, float* vol, cudaStream_t st);
 // Precision form (match_tc.cu): bf16 tensor-core distances, exact FP32 re-rank
 // of the 32 best; top-K branch only (numMin = numMax), d = 8, stride <= 4.
 bool match_tc_supported(int d, int d2, int s, int K, bool tol_branch);

@@ -335,6 +335,34 @@ cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st) {
   return cudaErrorInvalidValue;
 }
 
+// Gather the blocks a match set selects from another image's search image:
+// the colour form matches on luma and filters every channel with those sets.
+// vol is tile-space (vm = M d rows), block (i, j) slot k at rows i d, cols j d.
+__global__ void k_gather_volume(const float* __restrict__ pad, int P, int M, int N, int s, int d, int d2, int K,
+                                const uint32_t* __restrict__ S, const int32_t* __restrict__ cnt,
+                                float* __restrict__ vol, int vm, int vn) {
+  const size_t total = (size_t)M * N * K * d * d;
+  const int h = d2 / 2;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t % d), c = (int)((t / d) % d);
+    const size_t gk = t / ((size_t)d * d);
+    const int k = (int)(gk % K);
+    const size_t g = gk / K;
+    const int i = (int)(g % M), j = (int)(g / M);
+    int e = (int)S[g * K + k] - 1;
+    if ((cnt && k >= cnt[g]) || (unsigned)e >= (unsigned)(d2 * d2)) e = h + h * d2;
+    const int a = e % d2, b = e / d2;
+    vol[(size_t)(i * d + r) + (size_t)vm * (j * d + c) + (size_t)vm * vn * k] =
+        pad[(size_t)(i * s + a + r) + (size_t)(j * s + b + c) * P];
+  }
+}
+
+cudaError_t launch_gather_volume(const float* pad, int P, int M, int N, int s, int d, int d2, int K, const uint32_t* S,
+                                 const int32_t* cnt, float* vol, cudaStream_t st) {
+  k_gather_volume<<<1184, 256, 0, st>>>(pad, P, M, N, s, d, d2, K, S, cnt, vol, M * d, N * d);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
                             cudaStream_t st) {
   const int R = m + d2, Q = n + d2;

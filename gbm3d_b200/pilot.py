@@ -156,8 +156,10 @@ def make_dataset(n_crops: int = 20000, crop: int = 128, size: int = 1024, seed: 
 
 
 def train(steps: int = 3000, batch: int = 32, lr: float = 1e-3, n_crops: int = 20000, crop: int = 128,
-          seed: int = 0, ctx=None, data=None, log=print, params=None) -> tuple[np.ndarray, list]:
-    """Adam on mean((pilot - step1)^2) with the library's kernels; cosine-decayed lr."""
+          seed: int = 0, ctx=None, data=None, log=print, params=None,
+          max_seconds: float | None = None) -> tuple[np.ndarray, list]:
+    """Adam on mean((pilot - step1)^2) with the library's kernels; cosine-decayed
+    lr.  max_seconds bounds the wall time (the schedule then ends early)."""
     import torch
     ctx = ctx or context()
     dev = torch.device("cuda", ctx.device)
@@ -171,11 +173,11 @@ def train(steps: int = 3000, batch: int = 32, lr: float = 1e-3, n_crops: int = 2
     loss = C.c_float(0.0)
     t0 = time.time()
     with shared_stream(ctx):
-        _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, loss, t0, log)
+        _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, loss, t0, log, max_seconds)
     return get_params(ctx), losses
 
 
-def _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, loss, t0, log):
+def _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, loss, t0, log, max_seconds=None):
     import torch
     dev = xb.device
     batch = xb.shape[0]
@@ -189,6 +191,10 @@ def _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, los
                                                C.c_void_p(sb.data_ptr()), batch, xb.shape[1], xb.shape[2],
                                                C.c_float(max(lr_t, 1e-6)), C.byref(loss)))
         losses.append(float(loss.value))
+        if max_seconds is not None and time.time() - t0 > max_seconds:
+            if log:
+                log(f"stopping at step {step}: {max_seconds}s budget")
+            break
         if log and (step % 200 == 0 or step == steps - 1):
             log(f"step {step}: loss {np.mean(losses[-50:]):.3f} (RMSE {math.sqrt(np.mean(losses[-50:])):.3f}), "
                 f"{time.time() - t0:.1f}s")
@@ -276,6 +282,7 @@ def main():
     t.add_argument("--crops", type=int, default=20000)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--out", default=WEIGHTS)
+    t.add_argument("--max-seconds", type=float, default=None)
     a = ap.parse_args()
     from . import build
     build.build()
@@ -283,7 +290,7 @@ def main():
         load(a.weights)
         evaluate(a.size)
         return
-    params, losses = train(a.steps, a.batch, a.lr, a.crops, seed=a.seed)
+    params, losses = train(a.steps, a.batch, a.lr, a.crops, seed=a.seed, max_seconds=a.max_seconds)
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     np.save(a.out, params)
     print(f"saved {a.out}: final loss {np.mean(losses[-100:]):.4f}")

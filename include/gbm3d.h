@@ -189,6 +189,24 @@ int gbm3d_pilot_train_step(gbm3d_ctx* ctx, const float* img, const float* target
 int gbm3d_pilot_gradients(gbm3d_ctx* ctx, const float* img, const float* target, const float* sigma, int nimg,
                           int H, int W, float* grad, float* loss);
 
+/* Colour GBM3D (device planes R, G, B; float64 column-major m x n): the
+ * opponent transform Y = (R+G+B)/3, U = (R-B)/2, V = (R-2G+B)/4, block
+ * matching on Y only, every channel filtered and aggregated with Y's match
+ * sets at its own noise level (sigma/sqrt(3), sigma/sqrt(2), sigma*sqrt(3/8)),
+ * and the inverse transform.  Asynchronous on the context stream.  Not in the
+ * reference. */
+int gbm3d_denoise_rgb_device(gbm3d_ctx* ctx, const double* R, const double* G, const double* B, int m, int n,
+                             double sigma, const gbm3d_opts* opts, double* UR, double* UG, double* UB);
+
+/* Batched form: nimg images of any sizes (device pointers, float64
+ * column-major, sigma per image) denoised with one option set.  With
+ * use_graph, the first call runs the batch and captures its whole launch
+ * sequence into one CUDA graph; a later call with the same pointers, sizes,
+ * sigmas and options replays it with a single graph launch.  Asynchronous on
+ * the context stream.  Not in the reference. */
+int gbm3d_denoise_batch(gbm3d_ctx* ctx, int nimg, const double* const* I, const int* m, const int* n,
+                        const double* sigma, const gbm3d_opts* opts, double* const* U, int use_graph);
+
 /* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
  * the context stream (synchronise before reading U). */
 int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
