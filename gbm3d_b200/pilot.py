@@ -11,8 +11,11 @@ memory.
 
 The fallback gate: per image, on a sampled central tile, the step-1 quality of
 the network and of the plain step 1 is estimated without the clean image by
-Monte-Carlo SURE (Stein's unbiased risk estimate with a random-probe
-divergence, Ramani, Blu & Unser 2008); when the network's estimated PSNR is
+recorruption (Pang et al., "Recorrupted-to-Recorrupted", 2021): with z ~ N(0,1),
+y1 = y + sigma z and y2 = y - sigma z carry independent noise, so
+mean((f(y1) - y2)^2) - 2 sigma^2 is an unbiased estimate of f's error at noise
+level sqrt(2) sigma.  Both methods see the same y1, y2, so the common noise in
+the two estimates cancels in their ratio; when the network's estimated PSNR is
 more than 0.1 dB below the plain step's, the image takes the plain path.
 """
 from __future__ import annotations
@@ -202,17 +205,12 @@ def _train_loop(ctx, steps, lr, noisy, target, sig, gen, xb, tb, sb, losses, los
 
 # ---- fallback gate --------------------------------------------------------------------------
 
-def _sure_psnr(fn, y, sigma, eps, probe):
-    """Estimated PSNR of fn(y) against the unknown clean image (Monte-Carlo SURE)."""
-    f = fn(y)
-    f2 = fn(y + eps * probe)
-    n = y.size
-    div = float(np.sum(probe * (f2 - f))) / eps
-    mse = float(np.mean((f - y) ** 2)) - sigma ** 2 + 2.0 * sigma ** 2 * div / n
-    return 10.0 * math.log10(255.0 ** 2 / max(mse, 1e-12))
+def _r2r_mse(fn, y1, y2, sigma):
+    """Estimated error (vs the unknown clean image) of fn at noise level sqrt(2) sigma."""
+    return float(np.mean((fn(y1) - y2) ** 2)) - 2.0 * sigma ** 2
 
 
-def gate(I, sigma, opts=None, tile: int = 256, threshold_db: float = 0.1, seed: int = 0, ctx=None) -> dict:
+def gate(I, sigma, opts=None, tile: int = 512, threshold_db: float = 0.1, seed: int = 0, ctx=None) -> dict:
     """Per-image decision: take the network's pilot unless its estimated step-1
     PSNR on a central tile is more than threshold_db below the plain step's."""
     o = dict(opts or dense_opts())
@@ -220,13 +218,14 @@ def gate(I, sigma, opts=None, tile: int = 256, threshold_db: float = 0.1, seed: 
     t = min(tile, m, n)
     r0, c0 = (m - t) // 2, (n - t) // 2
     y = np.asfortranarray(I[r0:r0 + t, c0:c0 + t], dtype=np.float64)
-    probe = np.random.default_rng(seed).choice([-1.0, 1.0], size=y.shape)
-    eps = max(0.01 * sigma, 1e-3)
+    z = np.random.default_rng(seed).standard_normal(y.shape)
+    y1, y2 = np.asfortranarray(y + sigma * z), y - sigma * z
+    s1 = math.sqrt(2.0) * sigma
     o1 = dict(o, Wiener=False, form="plain")
-    plain = _sure_psnr(lambda z: api.GBM3D(z, sigma, o1, ctx=ctx)[0], y, sigma, eps, probe)
-    net = _sure_psnr(lambda z: pilot_image(z, sigma, ctx), y, sigma, eps, probe)
-    return {"psnr_plain_est": plain, "psnr_pilot_est": net, "gap_db": plain - net,
-            "fallback": (plain - net) > threshold_db}
+    e_plain = _r2r_mse(lambda v: api.GBM3D(v, s1, o1, ctx=ctx)[0], y1, y2, sigma)
+    e_net = _r2r_mse(lambda v: pilot_image(v, s1, ctx), y1, y2, sigma)
+    gap = 10.0 * math.log10(max(e_net, 1e-12) / max(e_plain, 1e-12))
+    return {"mse_plain_est": e_plain, "mse_pilot_est": e_net, "gap_db": gap, "fallback": gap > threshold_db}
 
 
 def GBM3D_learned(I, sigma, opts=None, ctx=None, use_gate: bool = True):
@@ -254,14 +253,16 @@ def evaluate(size: int = 1024, sigmas=(15.0, 25.0, 50.0), seed: int = 900, ctx=N
         o = dense_opts()
         Up, outp = api.GBM3D(noisy, sigma, dict(o, form="plain"), ctx=ctx)
         Ul, outl = GBM3D_learned(noisy, sigma, o, ctx=ctx)
+        Un, outn = api.GBM3D(noisy, sigma, dict(o, form="learned"), ctx=ctx)
         set_params(init_params(0), ctx)
         Uu, _ = api.GBM3D(noisy, sigma, dict(o, form="learned"), ctx=ctx)
         set_params(trained, ctx)
         row = {"sigma": sigma, "psnr_noisy": options.myPSNR(clean, noisy, 255),
-               "psnr_plain": options.myPSNR(clean, Up, 255), "psnr_learned": options.myPSNR(clean, Ul, 255),
+               "psnr_plain": options.myPSNR(clean, Up, 255), "psnr_learned": options.myPSNR(clean, Un, 255),
+               "psnr_gated": options.myPSNR(clean, Ul, 255),
                "psnr_untrained": options.myPSNR(clean, Uu, 255),
                "psnr_step1_plain": options.myPSNR(clean, outp["U1"], 255),
-               "psnr_step1_learned": options.myPSNR(clean, outl["U1"], 255),
+               "psnr_step1_learned": options.myPSNR(clean, outn["U1"], 255),
                "path": outl["path"], "gate": outl["gate"]}
         rows.append(row)
         if log:
