@@ -49,7 +49,7 @@ WORKLOADS = {
 WL = "dense"
 STAGES = ["glue", "match1", "wavelet1", "agg1", "match2", "wiener2", "agg2", "total"]
 # arithmetic of each form: plain FP32; precision: bf16 tensor-core distances (+ exact FP32 re-rank)
-FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32"}
+FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32"}
 FAMILIES = ["match", "match_tc", "wav_analysis", "wav_synthesis", "aggregate", "wiener", "ht_weights", "make_pad",
             "accum", "ratio", "prep", "medfilt3"]
 
@@ -311,9 +311,27 @@ def run_ours(args):
                 "psnr": float(_opt.myPSNR(clean, U, 255))}
 
     o_plain = opts()
-    forms = ["plain", "precision"] if args.form == "auto" else sorted({"plain", args.form})
+    from gbm3d_b200 import pilot
+    have_pilot = os.path.exists(pilot.WEIGHTS)
+    if have_pilot:
+        pilot.load(ctx=ctx)
+    forms = (["plain", "precision"] + (["learned"] if have_pilot else [])) if args.form == "auto" \
+        else sorted({"plain", args.form})
     res = {f: measure(dict(o_plain, form=f), True) for f in forms}
     plain = res["plain"]
+    if "learned" in res:
+        # the learned form decides per image (on a 512^2 tile, host-orchestrated)
+        # whether to take the network's pilot; its time is added to the step, and
+        # a fallback means the plain path's time and result
+        t0 = time.perf_counter()
+        g = pilot.gate(noisy, SIGMA, o_plain, ctx=ctx)
+        gate_ms = (time.perf_counter() - t0) * 1e3
+        r = res["learned"]
+        if g["fallback"]:
+            r.update({k: plain[k] for k in ("stages", "ktimes", "launches", "psnr")})
+            r["ms"] = plain["ms"]
+        r["ms"] += gate_ms
+        r["gate"] = dict(g, ms=gate_ms)
     # the chosen form: the fastest one within 0.05 dB PSNR of the plain path
     ok = [f for f in forms if res[f]["psnr"] >= plain["psnr"] - 0.05]
     form = min(ok, key=lambda f: res[f]["ms"]) if args.form == "auto" else args.form
@@ -361,6 +379,7 @@ def run_ours(args):
             "config": _config({"form": form}),
             "forms": {f: {"value": world * mpix / (r["ms"] / 1e3), "unit": "MPix/s", "ms_per_step": r["ms"],
                           "psnr_db": r["psnr"], "stages_ms": dict(zip(STAGES, r["stages"])),
+                          "gate": r.get("gate"),
                           "kernels_ms": {k: {"launches": n, "ms": t} for k, (n, t) in r["ktimes"].items()}}
                       for f, r in res.items()},
             "plain": {"value": world * mpix / (plain["ms"] / 1e3), "unit": "MPix/s", "ms_per_step": plain["ms"],
