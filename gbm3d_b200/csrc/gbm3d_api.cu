@@ -319,19 +319,23 @@ dim3 grid2(int rows, int cols) { return dim3((rows + 255) / 256, cols); }
 
 // Opponent colour transform (Y, U, V) = A (R, G, B) with
 // A = [1/3 1/3 1/3; 1/2 0 -1/2; 1/4 -1/2 1/4], and its inverse
-// R = Y + U + 2V/3, G = Y - 4V/3, B = Y - U + 2V/3.
+// R = Y + U + 2V/3, G = Y - 4V/3, B = Y - U + 2V/3.  The chroma channels are
+// carried with an offset of 128 so that they stay non-negative through the
+// clamps at 0 of both steps (the offset only moves the coarse approximation,
+// which is never thresholded).
 __global__ void k_opp(const double* __restrict__ R, const double* __restrict__ G, const double* __restrict__ B,
                       size_t n, double* __restrict__ Y, double* __restrict__ U, double* __restrict__ V, int inverse) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const double a = R[i], b = G[i], c = B[i];
     if (!inverse) {
       Y[i] = (a + b + c) / 3.0;
-      U[i] = (a - c) / 2.0;
-      V[i] = (a - 2.0 * b + c) / 4.0;
-    } else {  // (a, b, c) = (Y, U, V)
-      Y[i] = a + b + 2.0 * c / 3.0;
-      U[i] = a - 4.0 * c / 3.0;
-      V[i] = a - b + 2.0 * c / 3.0;
+      U[i] = (a - c) / 2.0 + 128.0;
+      V[i] = (a - 2.0 * b + c) / 4.0 + 128.0;
+    } else {  // (a, b, c) = (Y, U + 128, V + 128)
+      const double u = b - 128.0, v = c - 128.0;
+      Y[i] = a + u + 2.0 * v / 3.0;
+      U[i] = a - 4.0 * v / 3.0;
+      V[i] = a - u + 2.0 * v / 3.0;
     }
   }
 }

@@ -190,7 +190,8 @@ int gbm3d_pilot_gradients(gbm3d_ctx* ctx, const float* img, const float* target,
                           int H, int W, float* grad, float* loss);
 
 /* Colour GBM3D (device planes R, G, B; float64 column-major m x n): the
- * opponent transform Y = (R+G+B)/3, U = (R-B)/2, V = (R-2G+B)/4, block
+ * opponent transform Y = (R+G+B)/3, U = (R-B)/2, V = (R-2G+B)/4 (chroma
+ * carried with an offset of 128 through the clamps at 0), block
  * matching on Y only, every channel filtered and aggregated with Y's match
  * sets at its own noise level (sigma/sqrt(3), sigma/sqrt(2), sigma*sqrt(3/8)),
  * and the inverse transform.  Asynchronous on the context stream.  Not in the

@@ -372,3 +372,96 @@ def match_blocks_global(I, sigma, d, K):
             D = (nr + bn - 2 * cc) / nr
             S[:, i, j] = np.argsort(D.ravel(order="F"), kind="stable")[:K] + 1
     return S, I
+
+
+def match_blocks_video(I, d, K):
+    """matchBlocksV.m:21-116 (top-K branch): I is m x n x F (F odd); FFT route
+    for the distances of every d x d offset in every frame of the 2d x 2d
+    window.  Returns S (K, M, N) and Volume (m, n, K)."""
+    I = np.asarray(I, dtype=np.float64)
+    m, n, F = I.shape
+    ref = (F - 1) // 2
+    M, N = m // d, n // d
+    T = np.zeros((2 * m, 2 * n, F))
+    T[:m, :n], T[:m, n:], T[m:, :n], T[m:, n:] = I, I, I, I
+    Ipad = np.roll(T[: m + d, : n + d], (d // 2, d // 2), axis=(0, 1))
+    g = np.zeros((m, n))
+    g[:d, :d] = 1
+    bn = np.real(np.fft.ifft2(np.conj(np.fft.fft2(g))[..., None] * np.fft.fft2(I ** 2, axes=(0, 1)), axes=(0, 1)))
+    gp = np.zeros((m + d, n + d))
+    gp[:d, :d] = 1
+    bnp = np.real(np.fft.ifft2(np.conj(np.fft.fft2(gp))[..., None] * np.fft.fft2(Ipad ** 2, axes=(0, 1)),
+                               axes=(0, 1)))
+    S = np.zeros((K, M, N), dtype=np.uint32)
+    Vol = np.zeros((m, n, K))
+    for i in range(M):
+        for j in range(N):
+            xR = I[i * d:(i + 1) * d, j * d:(j + 1) * d, ref]
+            It = Ipad[i * d:(i + 2) * d, j * d:(j + 2) * d, :]
+            xz = np.zeros((2 * d, 2 * d))
+            xz[:d, :d] = xR
+            cc = np.real(np.fft.ifft2(np.conj(np.fft.fft2(xz))[..., None] * np.fft.fft2(It, axes=(0, 1)), axes=(0, 1)))
+            nr = bn[i * d, j * d, ref]
+            D = (nr + bnp[i * d:(i + 1) * d, j * d:(j + 1) * d, :] - 2 * cc[:d, :d, :]) / nr
+            idx = np.argsort(D.ravel(order="F"), kind="stable")[:K]
+            s = (idx + 1).astype(np.uint32)
+            s[0] = d * d * F // 2 + d // 2 + 1
+            S[:, i, j] = s
+            for k in range(K):
+                e = int(s[k]) - 1
+                a, b, c = e % d, (e // d) % d, e // (d * d)
+                Vol[i * d:(i + 1) * d, j * d:(j + 1) * d, k] = It[a:a + d, b:b + d, c]
+    return S, Vol
+
+
+def denoise_video(Volume, S, tau, Psi, Psi2, d, F, levels, cycle_spin):
+    """denoiseAndAggregateV.m:11-90."""
+    K, M, N = S.shape
+    m, n = M * d, N * d
+    Vrec = np.zeros((m, n, K, cycle_spin))
+    for spin in range(cycle_spin):
+        V = _circshift(Volume, (spin, spin, spin))
+        C = wav_dec3(Psi, levels, V)
+        for i in range(levels):
+            for j in range(7):
+                C[i, j] = C[i, j] * (np.abs(C[i, j]) > tau[i, j])
+        Vrec[..., spin] = _circshift(wav_rec3(Psi2, levels, C), (-spin, -spin, -spin))
+    Vavg = np.minimum(np.maximum(Vrec.mean(axis=3), 0), 1)
+    U = np.zeros((m + d, n + d, F))
+    W = np.zeros_like(U)
+    for y in range(M):
+        for x in range(N):
+            blocks = Vavg[y * d:(y + 1) * d, x * d:(x + 1) * d, :K]
+            wt = 1.0 / agg_weight(blocks)
+            for i in range(K):
+                e = int(S[i, y, x]) - 1
+                a, b, c = e % d + y * d - d // 2, (e // d) % d + x * d - d // 2, e // (d * d)
+                if a >= 0 and b >= 0:
+                    U[a:a + d, b:b + d, c] += wt * blocks[:, :, i]
+                    W[a:a + d, b:b + d, c] += wt
+    return U[:m, :n], W[:m, :n]
+
+
+def vbm3d(I, sigma, d, K, levels, cycle_spin, tau_unit, spins, nF, Psi, Psi2):
+    """VBM3D.m:20-63 (frames already in the reference's [0,1] scale)."""
+    I = np.asarray(I, dtype=np.float64)
+    m, n, Kf = I.shape
+    Mp, Np = -(-m // d) * d, -(-n // d) * d
+    I2 = np.zeros((Mp, Np, Kf))
+    I2[:m, :n] = I
+    I2[m:, :n] = np.flipud(I[m - (Mp - m):m, :n])
+    I2[:m, n:] = np.fliplr(I[:m, n - (Np - n):n])
+    I2[m:, n:] = np.fliplr(np.flipud(I[m - (Mp - m):m, n - (Np - n):n]))
+    hw = (nF - 1) // 2
+    Y = np.zeros((Mp, Np, Kf, len(spins)))
+    for ii, s in enumerate(spins):
+        nn = np.zeros((Mp, Np, Kf))
+        for jj in range(hw, Kf - hw):
+            ind = slice(jj - hw, jj + hw + 1)
+            I3 = np.roll(I2[:, :, ind], (s, s), axis=(0, 1))
+            S, Vol = match_blocks_video(I3, d, K)
+            U, W = denoise_video(Vol, S, sigma * tau_unit, Psi, Psi2, d, nF, levels, cycle_spin)
+            Y[:, :, ind, ii] += U
+            nn[:, :, ind] += W
+        Y[:, :, :, ii] = np.roll(Y[:, :, :, ii] / nn, (-s, -s), axis=(0, 1))
+    return Y[:m, :n, hw:Kf - hw].mean(axis=3)

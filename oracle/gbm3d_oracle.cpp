@@ -900,6 +900,174 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
 
 
 // ---------------------------------------------------------------------------
+// Video — VBM3D.m:20-63, matchBlocksV.m:21-116 (top-K branch),
+// denoiseAndAggregateV.m:11-90
+// ---------------------------------------------------------------------------
+
+// Block matching over a window of F frames (F odd): references tile the
+// centre frame at stride d; candidates are the d x d offsets of the 2d x 2d
+// window of every frame (search image per frame built like matchBlocksCPU's
+// with d2 = d).  Ranked by (exact SSD, index a + b d + c d^2) like mink;
+// S(1) is forced to d^2 F/2 + d/2 + 1.  Volume: image-shaped m x n x K.
+template <class T>
+void match_video(const T* I, int m, int n, int F, int d, int K, uint32_t* S, T* Volume) {
+  const int h = d / 2, M = m / d, N = n / d, ref = (F - 1) / 2;
+  const size_t mn = (size_t)m * n;
+  auto pix = [&](int R, int C, int f) { return I[pad_index(R, m, h) + (size_t)m * pad_index(C, n, h) + mn * f]; };
+#pragma omp parallel for collapse(2) schedule(dynamic)
+  for (int j = 0; j < N; ++j)
+    for (int i = 0; i < M; ++i) {
+      const int g = i + M * j, nc = d * d * F;
+      std::vector<T> x((size_t)d * d);
+      for (int r = 0; r < d; ++r)
+        for (int c = 0; c < d; ++c) x[r * d + c] = pix(i * d + h + r, j * d + h + c, ref);
+      std::vector<std::pair<T, uint32_t>> key(nc);
+      for (int f = 0; f < F; ++f)
+        for (int b = 0; b < d; ++b)
+          for (int a = 0; a < d; ++a) {
+            T acc = T(0);
+            for (int r = 0; r < d; ++r)
+              for (int c = 0; c < d; ++c) {
+                const T t = x[r * d + c] - pix(i * d + a + r, j * d + b + c, f);
+                acc = fmaT(t, t, acc);
+              }
+            const uint32_t idx = (uint32_t)(a + b * d + f * d * d);
+            key[idx] = {acc, idx};
+          }
+      std::stable_sort(key.begin(), key.end(),
+                       [](const std::pair<T, uint32_t>& u, const std::pair<T, uint32_t>& v) { return u.first < v.first; });
+      for (int k = 0; k < K; ++k) S[(size_t)g * K + k] = key[k].second + 1;
+      S[(size_t)g * K] = (uint32_t)(d * d * F / 2 + d / 2 + 1);  // matchBlocksV.m:103
+      for (int k = 0; k < K; ++k) {
+        const int e = (int)S[(size_t)g * K + k] - 1;
+        const int a = e % d, b = (e / d) % d, f = e / (d * d);
+        for (int c = 0; c < d; ++c)
+          for (int r = 0; r < d; ++r)
+            Volume[(size_t)(i * d + r) + (size_t)m * (j * d + c) + mn * k] = pix(i * d + a + r, j * d + b + c, f);
+      }
+    }
+}
+
+// denoiseAndAggregateV.m:24-90: cycle-spun 3D wavelet hard threshold of the
+// volume, Vavg = min(max(mean, 0), 1), weight 1/TV(blocks) (the same
+// getBM3DAggWeights(3,1) measure as step 1), and aggregation without a window:
+// block k of reference (y, x) lands in frame c at rows a + y d - d/2, columns
+// b + x d - d/2 (discarded when it starts before row or column 0); sums are
+// double, each term fl(w * block).  U, Wt: m x n x F.
+template <class T>
+void denoise_video(const T* Volume, int M, int N, int d, int F, int K, const uint32_t* S, int levels, int cycleSpin,
+                   const double* tau, const orc_filters* f, double* U, double* Wt) {
+  const int m = M * d, n = N * d, h = d / 2;
+  const size_t vol = (size_t)m * n * K;
+  Bank1D<T> bxy = make_bank<T>(f->len_xy, f->a_lo_xy, f->a_hi_xy, f->s_lo_xy, f->s_hi_xy);
+  Bank1D<T> bz = make_bank<T>(f->len_z, f->a_lo_z, f->a_hi_z, f->s_lo_z, f->s_hi_z);
+  std::vector<T> sum(vol, T(0)), V(vol);
+  for (int spin = 0; spin < cycleSpin; ++spin) {
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < K; ++z)
+      for (int x = 0; x < n; ++x)
+        for (int y = 0; y < m; ++y)
+          V[y + (size_t)m * (x + (size_t)n * z)] =
+              Volume[pmod(y - spin, m) + (size_t)m * (pmod(x - spin, n) + (size_t)n * pmod(z - spin, K))];
+    wavelet_ht(V, m, n, K, levels, tau, bxy, bz);
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < K; ++z)
+      for (int x = 0; x < n; ++x)
+        for (int y = 0; y < m; ++y) {
+          size_t o = y + (size_t)m * (x + (size_t)n * z);
+          T v = V[pmod(y + spin, m) + (size_t)m * (pmod(x + spin, n) + (size_t)n * pmod(z + spin, K))];
+          sum[o] = spin == 0 ? v : sum[o] + v;
+        }
+  }
+  const T cs = (T)cycleSpin;
+#pragma omp parallel for
+  for (size_t o = 0; o < vol; ++o) {
+    T v = sum[o] / cs;
+    v = v > T(0) ? v : T(0);
+    sum[o] = v < T(1) ? v : T(1);
+  }
+  const size_t px = (size_t)m * n;
+  std::vector<double> Up((size_t)(m + d) * (n + d) * F, 0.0), Wp(Up.size(), 0.0);
+  const int P = m + d, Q = n + d;
+  for (int y = 0; y < M; ++y)
+    for (int x = 0; x < N; ++x) {
+      const int g = y + M * x;
+      const T w = ht_weight<T>(&sum[(size_t)y * d + (size_t)x * d * m], 1, m, px, d, K);
+      for (int k = 0; k < K; ++k) {
+        const int e = (int)S[(size_t)g * K + k] - 1;
+        const int a = e % d, b = (e / d) % d, fr = e / (d * d);
+        const int R0 = a + y * d - h, C0 = b + x * d - h;
+        if (R0 < 0 || C0 < 0) continue;
+        for (int c = 0; c < d; ++c)
+          for (int r = 0; r < d; ++r) {
+            const T blk = sum[(size_t)(y * d + r) + (size_t)m * (x * d + c) + px * k];
+            const size_t o = (size_t)(R0 + r) + (size_t)P * ((C0 + c) + (size_t)Q * fr);
+            Up[o] += (double)(w * blk);
+            Wp[o] += (double)w;
+          }
+      }
+    }
+  for (int fr = 0; fr < F; ++fr)
+    for (int c = 0; c < n; ++c)
+      for (int r = 0; r < m; ++r) {
+        U[r + (size_t)m * (c + (size_t)n * fr)] = Up[r + (size_t)P * (c + (size_t)Q * fr)];
+        Wt[r + (size_t)m * (c + (size_t)n * fr)] = Wp[r + (size_t)P * (c + (size_t)Q * fr)];
+      }
+}
+
+// VBM3D.m:20-63: frames mirror-padded to multiples of d; for every match spin
+// and every centre frame jj with a full window of nF frames, the circshifted
+// window is matched and denoised, and U / weights are added (in single, as
+// the reference's single Y and nn) into the window's frames; Y / nn is shifted
+// back, and the output is the mean over spins of frames (nF-1)/2 ..
+// Kf-1-(nF-1)/2, cropped.  out: m0 x n0 x (Kf - nF + 1).
+template <class T>
+void vbm3d(const double* I0, int m0, int n0, int Kf, double sigma, int d, int K, int levels, int cycleSpin,
+           int tauMode, const int* spins, int nS, int nF, const orc_filters* f, double* out) {
+  const int Mp = (m0 + d - 1) / d * d, Np = (n0 + d - 1) / d * d, M = Mp / d, N = Np / d;
+  const size_t px = (size_t)Mp * Np, px0 = (size_t)m0 * n0;
+  std::vector<double> I2(px * Kf);
+  for (int k = 0; k < Kf; ++k) mirror_pad(I0 + px0 * k, m0, n0, &I2[px * k], Mp, Np);
+  std::vector<double> tau(levels * 7);
+  get_tau(levels, tauMode, tau.data());
+  for (auto& t : tau) t *= sigma;
+  const int hw = (nF - 1) / 2, nOut = Kf - nF + 1;
+  std::vector<double> acc((size_t)px0 * nOut, 0.0);
+  std::vector<float> Y(px * Kf), nn(px * Kf);
+  std::vector<double> sh(px), U(px * nF), Wt(px * nF);
+  for (int ii = 0; ii < nS; ++ii) {
+    const int s = spins[ii];
+    std::fill(Y.begin(), Y.end(), 0.f);
+    std::fill(nn.begin(), nn.end(), 0.f);
+    for (int jj = hw; jj < Kf - hw; ++jj) {
+      std::vector<T> I3(px * nF);
+      for (int q = 0; q < nF; ++q) {
+        circshift2(&I2[px * (jj - hw + q)], Mp, Np, s, sh.data());
+        for (size_t p = 0; p < px; ++p) I3[px * q + p] = (T)sh[p];
+      }
+      std::vector<uint32_t> S((size_t)M * N * K);
+      std::vector<T> Vol(px * K);
+      match_video<T>(I3.data(), Mp, Np, nF, d, K, S.data(), Vol.data());
+      denoise_video<T>(Vol.data(), M, N, d, nF, K, S.data(), levels, cycleSpin, tau.data(), f, U.data(), Wt.data());
+      for (int q = 0; q < nF; ++q)
+        for (size_t p = 0; p < px; ++p) {
+          const size_t o = px * (jj - hw + q) + p;
+          Y[o] = (float)((double)Y[o] + U[px * q + p]);
+          nn[o] = (float)((double)nn[o] + Wt[px * q + p]);
+        }
+    }
+    for (int k = hw; k < Kf - hw; ++k)
+      for (int c = 0; c < n0; ++c)
+        for (int r = 0; r < m0; ++r) {
+          // circshift(Y ./ nn, [-s, -s, 0]): output (r, c) reads (r + s, c + s)
+          const size_t o = px * k + pmod(r + s, Mp) + (size_t)Mp * pmod(c + s, Np);
+          acc[px0 * (k - hw) + r + (size_t)m0 * c] += (double)(Y[o] / nn[o]);
+        }
+  }
+  for (size_t o = 0; o < acc.size(); ++o) out[o] = (double)(float)(acc[o] / nS);
+}
+
+// ---------------------------------------------------------------------------
 // Global matcher — matchBlocksGPU.m:19-91 (A12)
 // ---------------------------------------------------------------------------
 
@@ -1185,6 +1353,33 @@ int orc_gbm3d(int prec, const double* I, int m, int n, double sigma, const orc_o
   if (o->Wiener && (o->blockSize - o->blockSizeWie) % std::gcd(st1, st2) != 0) return 1;
   if (prec == 32) gbm3d<float>(I, m, n, sigma, o, U, U1);
   else gbm3d<double>(I, m, n, sigma, o, U, U1);
+  return 0;
+}
+
+int orc_match_video(int prec, const double* I, int m, int n, int F, int d, int K, uint32_t* S, void* Volume) {
+  const size_t px = (size_t)m * n;
+  if (prec == 32) {
+    std::vector<float> t(px * F);
+    for (size_t i = 0; i < t.size(); ++i) t[i] = (float)I[i];
+    match_video<float>(t.data(), m, n, F, d, K, S, (float*)Volume);
+  } else {
+    match_video<double>(I, m, n, F, d, K, S, (double*)Volume);
+  }
+  return 0;
+}
+
+int orc_denoise_video(int prec, const void* Volume, int M, int N, int d, int F, int K, const uint32_t* S, int levels,
+                      int cycleSpin, const double* tau, const orc_filters* f, double* U, double* W) {
+  if (prec == 32) denoise_video<float>((const float*)Volume, M, N, d, F, K, S, levels, cycleSpin, tau, f, U, W);
+  else denoise_video<double>((const double*)Volume, M, N, d, F, K, S, levels, cycleSpin, tau, f, U, W);
+  return 0;
+}
+
+int orc_vbm3d(int prec, const double* I, int m, int n, int Kf, double sigma, int d, int K, int levels, int cycleSpin,
+              int tauMode, const int* spins, int nS, int nF, const orc_filters* f, double* out) {
+  if (nF < 1 || nF % 2 == 0 || nF > Kf) return 1;
+  if (prec == 32) vbm3d<float>(I, m, n, Kf, sigma, d, K, levels, cycleSpin, tauMode, spins, nS, nF, f, out);
+  else vbm3d<double>(I, m, n, Kf, sigma, d, K, levels, cycleSpin, tauMode, spins, nS, nF, f, out);
   return 0;
 }
 
