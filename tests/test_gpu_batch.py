@@ -4,8 +4,9 @@ Batch: images of uneven sizes and noise levels denoised in one call, first
 eagerly while the launch sequence is captured into a CUDA graph, then by
 replaying the graph; every output must equal the single-image pipeline's bit
 for bit.  Colour: the opponent-space pipeline with luma-driven matching; on a
-grey image (R = G = B) the chroma channels are zero, so every output channel
-must equal the grey pipeline at the luma noise level sigma / sqrt(3).
+grey image (R = G = B) the chroma channels are constant, so every output
+channel must equal the grey pipeline at the luma noise level sigma / sqrt(3)
+(to float rounding of the constant chroma).
 """
 import numpy as np
 import pytest
@@ -49,8 +50,8 @@ def test_rgb_grey_image_equals_grey_pipeline(gpu):
     o = _dense()
     out = api.GBM3D_rgb(rgb, 25.0, o)
     grey, _ = api.GBM3D(noisy, 25.0 / np.sqrt(3.0), o)
-    for k in range(3):
-        assert np.array_equal(out[:, :, k], grey)
+    for k in range(3):  # the constant chroma (offset 128) comes back up to float rounding
+        assert np.abs(out[:, :, k] - grey).max() <= 1e-3
 
 
 def test_rgb_denoises_colour_noise(gpu):
