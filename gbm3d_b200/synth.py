@@ -63,3 +63,26 @@ def colored_noisy_image(m: int, n: int, sigma: float, omega: float = 1.0, seed: 
     noise = np.real(np.fft.ifft2(np.fft.fft2(w) * ghat))
     psd = sigma ** 2 * np.abs(ghat) ** 2
     return clean, np.asfortranarray(clean + noise), np.asfortranarray(psd)
+
+
+def video(m: int, n: int, frames: int, sigma: float, seed: int = 0, n_ellipses: int = 40):
+    """(clean, noisy) m x n x frames on a 0-255 scale: a gradient background and
+    ellipses that each translate by a fixed (dy, dx) of 0-3 px per frame."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    yy, xx = np.meshgrid(np.arange(m, dtype=np.float64), np.arange(n, dtype=np.float64), indexing="ij")
+    g0, gy, gx = rng.uniform(40, 120), rng.uniform(-60, 60), rng.uniform(-60, 60)
+    ell = []
+    for _ in range(n_ellipses):
+        ell.append((rng.uniform(0, m), rng.uniform(0, n), rng.uniform(0.02, 0.2) * m, rng.uniform(0.02, 0.2) * n,
+                    rng.uniform(0, np.pi), rng.uniform(0, 255), rng.uniform(-3, 3), rng.uniform(-3, 3)))
+    clean = np.zeros((m, n, frames))
+    for f in range(frames):
+        img = g0 + gy * yy / max(m - 1, 1) + gx * xx / max(n - 1, 1)
+        for cy, cx, ry, rx, th, val, vy, vx in ell:
+            c, s = np.cos(th), np.sin(th)
+            u = ((yy - cy - vy * f) * c + (xx - cx - vx * f) * s) / ry
+            v = (-(yy - cy - vy * f) * s + (xx - cx - vx * f) * c) / rx
+            img[u * u + v * v <= 1.0] = val
+        clean[:, :, f] = img
+    noise = np.random.Generator(np.random.PCG64(seed + 3_000_017)).standard_normal((m, n, frames))
+    return np.asfortranarray(clean), np.asfortranarray(clean + sigma * noise)

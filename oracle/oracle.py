@@ -316,3 +316,59 @@ def medfilt3(V, prec=64):
     m, n, K = V.shape
     lib().orc_medfilt3(prec, _p(V), m, n, K, _p(out))
     return out
+
+
+def sym4_haar_filters() -> orc_filters:
+    """getWaveFilters3D('sym','db',4,1) (waveTransforms3D/getWaveFilters3D.m:6-33):
+    sym4 decomposition filters on the spatial axes, db1 (Haar) on the slot
+    axis; the video path synthesises with the same filters (Psi2 = Psi)."""
+    from .fft_route import SYM4_HI, SYM4_LO
+    f = orc_filters()
+    cc = np.sqrt(2.0) / 2
+    f.len_xy = 8
+    f.len_z = 2
+    for pre in ("a", "s"):
+        getattr(f, pre + "_lo_xy")[0:8] = list(SYM4_LO)
+        getattr(f, pre + "_hi_xy")[0:8] = list(SYM4_HI)
+        getattr(f, pre + "_lo_z")[0:2] = [cc, cc]
+        getattr(f, pre + "_hi_z")[0:2] = [-cc, cc]
+    return f
+
+
+def matchBlocksV(I, d, K, prec=32):
+    """[S, Volume] = matchBlocksV(I, sigma, opts) (source/matchBlocksV.m), top-K branch."""
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n, F = I.shape
+    M, N = m // d, n // d
+    S = np.zeros((K, M, N), dtype=np.uint32, order="F")
+    Vol = np.zeros((m, n, K), dtype=np.float32 if prec == 32 else np.float64, order="F")
+    lib().orc_match_video(prec, _p(I), m, n, F, d, K, _p(S), _p(Vol))
+    return S, Vol
+
+
+def denoiseAndAggregateV(Volume, S, d, F, tau, levels, cycleSpin, filters=None, prec=32):
+    """[U, out.K] of denoiseAndAggregateV.m (U, W: m x n x F, float64)."""
+    f = filters if filters is not None else sym4_haar_filters()
+    K, M, N = S.shape
+    Volume = np.asfortranarray(Volume, dtype=np.float32 if prec == 32 else np.float64)
+    S = np.asfortranarray(S, dtype=np.uint32)
+    tau = np.asfortranarray(tau, dtype=np.float64)
+    U = np.zeros((M * d, N * d, F), order="F")
+    W = np.zeros_like(U)
+    lib().orc_denoise_video(prec, _p(Volume), M, N, d, F, K, _p(S), levels, cycleSpin, _p(tau), C.byref(f), _p(U),
+                            _p(W))
+    return U, W
+
+
+def VBM3D(I, sigma, d=8, K=16, levels=3, cycleSpin=2, tauMode=2, spins=(0, 4), nF=3, filters=None, prec=32):
+    """Y = VBM3D(I, sigma, opts) (source/VBM3D.m): frames I m x n x Kf on the
+    reference's [0,1] scale; returns frames (nF-1)/2 .. Kf-1-(nF-1)/2."""
+    f = filters if filters is not None else sym4_haar_filters()
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n, Kf = I.shape
+    out = np.zeros((m, n, Kf - nF + 1), order="F")
+    sp = np.ascontiguousarray(spins, dtype=np.int32)
+    if lib().orc_vbm3d(prec, _p(I), m, n, Kf, C.c_double(sigma), d, K, levels, cycleSpin, tauMode, _p(sp), len(sp),
+                       nF, C.byref(f), _p(out)) != 0:
+        raise ValueError("nF must be odd and at most the number of frames")
+    return out

@@ -16,7 +16,7 @@ from conftest import max_abs
 from gbm3d_b200 import options, synth
 
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("global"))
+                if not os.path.basename(p).startswith(("global", "video")))
 FP64_TOL = 1e-9  # relative, FFT route vs direct arithmetic, both float64
 
 
@@ -215,3 +215,16 @@ def test_colored_pipeline_oracle_denoises(oracle):
     U, _ = oracle.GBM3D_colored(noisy, float(np.mean(np.sqrt(psd))), tau, sw, o, prec=64)
     # strongly correlated noise (std 7 after the blur) is the hard case: a smaller gain
     assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255) + 1
+
+
+def test_video_oracle_matches_golden(oracle):
+    """matchBlocksV / denoiseAndAggregateV / VBM3D against the FFT-route golden
+    vectors (nF = 3, patch 8, sym4 x Haar, tauMode 2, spins [0 4])."""
+    g = _load(os.path.join(os.path.dirname(__file__), "golden", "video_32x40x4_s25.npz"))
+    I, s = g["noisy"] / 255.0, float(g["sigma"]) / 255.0
+    S, Vol = oracle.matchBlocksV(I[:, :, :3], 8, 16, prec=64)
+    assert np.array_equal(S, g["S"]) and max_abs(Vol, g["Vol"]) == 0
+    U, W = oracle.denoiseAndAggregateV(Vol, S, 8, 3, s * options.getTau(3, 2), 3, 2, prec=64)
+    assert max_abs(U, g["U"]) <= 1e-12 and max_abs(W, g["W"]) <= 1e-12
+    Y = oracle.VBM3D(I, s, prec=64)
+    assert max_abs(Y, g["Y"]) <= 1e-6  # the reference's Y and nn are single
