@@ -33,7 +33,7 @@ class gbm3d_opts(C.Structure):
         ("nMatchSpins", C.c_int), ("matchSpins", C.c_int * 8),
         ("nMatchSpinsWie", C.c_int), ("matchSpinsWie", C.c_int * 8),
         ("staleWeights", C.c_int), ("refStrideWie", C.c_int), ("wavelet", C.c_int),
-        ("form", C.c_int),
+        ("form", C.c_int), ("videoFrames", C.c_int),
     ]
 
 
@@ -78,6 +78,10 @@ _SIGS = {
     "gbm3d_ctx_synchronize": (C.c_int, [_P]),
     "gbm3d_denoise_rgb_device": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts),
                                            _P, _P, _P]),
+    "gbm3d_vbm3d_device": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P]),
+    "gbm3d_matchBlocksV": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.POINTER(gbm3d_opts), _P, _P]),
+    "gbm3d_denoiseAndAggregateV": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, C.POINTER(gbm3d_filters),
+                                             C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise_batch": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, C.POINTER(gbm3d_opts), _P, C.c_int]),
     "gbm3d_pilot_param_count": (C.c_int, []),
     "gbm3d_pilot_set_params": (C.c_int, [_P, _P]),

@@ -14,6 +14,10 @@ C ABI.  Arrays follow MATLAB's column-major layout (numpy order='F'):
                                                               source/denoiseAndAggregateWieFast.m:1
   U, W            = denoiseAndAggregateWie(V1, V2, S, sigma, opts)
                                                               source/denoiseAndAggregateWie.m:1
+  Y, out          = VBM3D(I, sigma, opts)                     source/VBM3D.m:1
+  S, Volume       = matchBlocksV(I, sigma, opts)              source/matchBlocksV.m:1
+  U, out          = denoiseAndAggregateV(Y, Volume, I, S, sigma, opts)
+                                                              source/denoiseAndAggregateV.m:1
 
 S is returned as a MatchSet: a uint32 array of shape (K, M, N) whose column
 S[:, i, j] is the reference's cell S{i+1, j+1}, plus the per-cell counts.
@@ -312,3 +316,111 @@ def GBM3D_rgb(I, sigma, opts: dict | None = None, ctx: Context | None = None):
                                              C.byref(co), *[C.c_void_p(u.data_ptr()) for u in outs]))
     ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
     return np.stack([u.cpu().numpy().reshape(m, n, order="F") for u in outs], axis=2)
+
+
+# ---- video ------------------------------------------------------------------------
+
+def video_opts(opts: dict | None = None) -> dict:
+    """The defaults of VBM3D.m:8-20 (blockSize 32, numMax = numMin = 16, the
+    sym4 x Haar bank, levels 3, cycleSpin 2, matchSpins [0, d/2], tauMode 2,
+    nF 11) for the fields opts does not set."""
+    o = dict(opts or {})
+    o.setdefault("blockSize", 32)
+    o.setdefault("numMax", 16)
+    o.setdefault("numMin", 16)
+    o.setdefault("wname", "sym")
+    o.setdefault("levels", 3)
+    o.setdefault("cycleSpin", 2)
+    o.setdefault("matchSpins", [0, int(o["blockSize"]) // 2])
+    o.setdefault("tauMode", 2)
+    o.setdefault("nF", 11)
+    return o
+
+
+def c_video_opts(opts: dict) -> gbm3d_opts:
+    o = video_opts(opts)
+    if o.get("wname") not in ("sym",) or o.get("wnamez", "db") != "db" or int(o.get("order", 4)) != 4 \
+            or int(o.get("orderz", 1)) != 1:
+        raise GBM3DError(5, "the video path's bank is getWaveFilters3D('sym','db',4,1)")
+    if o.get("wiener", False):
+        raise GBM3DError(5, "VBM3D has no Wiener step")
+    c = gbm3d_opts()
+    c.numMax, c.numMin = int(o["numMax"]), int(o["numMin"])
+    c.blockSize = c.blockSizeWie = int(o["blockSize"])
+    c.matchSize = 2 * int(o["blockSize"])
+    c.levels, c.cycleSpin, c.tauMode = int(o["levels"]), int(o["cycleSpin"]), int(o["tauMode"])
+    ms = list(o["matchSpins"])
+    if len(ms) > 8:
+        raise GBM3DError(1, "at most 8 match spins")
+    c.nMatchSpins = c.nMatchSpinsWie = len(ms)
+    for i, v in enumerate(ms):
+        c.matchSpins[i] = c.matchSpinsWie[i] = int(v)
+    c.staleWeights = 1
+    c.wavelet = 2
+    c.videoFrames = int(o["nF"])
+    return c
+
+
+def VBM3D(I, sigma, opts: dict | None = None, ctx: Context | None = None):
+    """[Y, out] = VBM3D(I, sigma, opts): frames I (m x n x K, values in [0,1]);
+    Y holds frames (nF+1)/2 .. K-(nF-1)/2 (1-based), the ones with a full
+    temporal window (VBM3D.m:44-63)."""
+    import torch
+    ctx = ctx or context()
+    co = c_video_opts(opts)
+    I = np.asfortranarray(I, dtype=np.float64)
+    if I.ndim != 3:
+        raise GBM3DError(1, "VBM3D takes an m x n x frames array")
+    m, n, Kf = I.shape
+    nF = co.videoFrames
+    if Kf < nF:
+        raise GBM3DError(1, "fewer frames than the temporal window")
+    dev = torch.device("cuda", ctx.device)
+    dI = torch.from_numpy(I.ravel(order="F").copy()).to(dev)
+    dY = torch.empty(m * n * (Kf - nF + 1), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    ctx.check(lib().gbm3d_vbm3d_device(ctx.h, C.c_void_p(dI.data_ptr()), m, n, Kf, float(sigma), C.byref(co),
+                                       C.c_void_p(dY.data_ptr())))
+    ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
+    return dY.cpu().numpy().reshape(m, n, Kf - nF + 1, order="F"), {"frames": (nF + 1) // 2 - 1 + np.arange(Kf - nF + 1)}
+
+
+def matchBlocksV(I, sigma, opts: dict | None = None, ctx: Context | None = None):
+    """[S, Volume] = matchBlocksV(I, sigma, opts): I is m x n x F (F odd);
+    S (K x M x N) indexes the d x d x F candidate window (1-based), Volume is
+    m x n x K single."""
+    ctx = ctx or context()
+    co = c_video_opts(opts)
+    I = np.asfortranarray(I, dtype=np.float64)
+    m, n, F = I.shape
+    if F % 2 != 1:
+        raise GBM3DError(1, "input volume should have odd number of frames")  # matchBlocksV.m:24
+    d, K = co.blockSize, co.numMax
+    M, N = m // d, n // d
+    S = np.zeros((K, M, N), dtype=np.uint32, order="F")
+    V = np.zeros((m, n, K), dtype=np.float32, order="F")
+    ctx.check(lib().gbm3d_matchBlocksV(ctx.h, _p(I), m, n, F, C.byref(co), _p(S), _p(V)))
+    return _as_set(S), V
+
+
+def denoiseAndAggregateV(Y, Volume, I, S, sigma, opts: dict | None = None, ctx: Context | None = None):
+    """[U, out] = denoiseAndAggregateV(Y, Volume, I, S, sigma, opts): U and
+    out['K'] are (M d) x (N d) x F double (F = frames of I); Y is unused, as in
+    the reference."""
+    ctx = ctx or context()
+    o = video_opts(opts)
+    co = c_video_opts(o)
+    d = co.blockSize
+    F = np.shape(I)[2]
+    K, M, N = np.shape(S)
+    Volume = np.asfortranarray(Volume, dtype=np.float32)
+    if Volume.shape[2] != K or Volume.shape[0] < M * d or Volume.shape[1] < N * d:
+        raise GBM3DError(1, "Volume does not match S")
+    Volume = np.asfortranarray(Volume[: M * d, : N * d, :])
+    Sa = np.asfortranarray(S, dtype=np.uint32)
+    tau = np.asfortranarray(float(sigma) * _opt.getTau(int(o["levels"]), int(o["tauMode"])))
+    U = np.zeros((M * d, N * d, F), order="F")
+    W = np.zeros_like(U)
+    ctx.check(lib().gbm3d_denoiseAndAggregateV(ctx.h, _p(Volume), _p(Sa), M, N, F, _p(tau), None, C.byref(co),
+                                               _p(U), _p(W)))
+    return U, {"K": W}

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgbm3d.so")
 SOURCES = ["match.cu", "wavelet.cu", "wiener.cu", "aggregate.cu", "gbm3d_api.cu", "noalloc.cu", "global_match.cu",
-           "tc_check.cu", "match_tc.cu", "pilot.cu"]
+           "tc_check.cu", "match_tc.cu", "pilot.cu", "video.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O2",

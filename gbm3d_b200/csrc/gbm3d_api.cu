@@ -230,6 +230,34 @@ void bior(gbm3d_filters* f) {
   f->s_lo_z[0] = Cc; f->s_lo_z[1] = Cc; f->s_hi_z[0] = -Cc; f->s_hi_z[1] = Cc;
 }
 
+// sym4 x Haar bank of the video path (getWaveFilters3D('sym','db',4,1),
+// waveTransforms3D/getWaveFilters3D.m:6-33; VBM3D synthesises with the same
+// filters): the published symlet-4 decomposition pair on the spatial axes.
+void sym4haar(gbm3d_filters* f) {
+  std::memset(f, 0, sizeof(*f));
+  static const double lo[8] = {-0.07576571478927333, -0.02963552764599851, 0.49761866763201545, 0.8037387518059161,
+                               0.29785779560527736, -0.09921954357684722, -0.012603967262037833, 0.0322231006040427};
+  const double Cc = std::sqrt(2.0) / 2;
+  f->len_xy = 8;
+  for (int k = 0; k < 8; ++k) {
+    f->a_lo_xy[k] = f->s_lo_xy[k] = lo[k];
+    f->a_hi_xy[k] = f->s_hi_xy[k] = (k % 2 ? 1.0 : -1.0) * lo[7 - k];  // Hi_d(k) = (-1)^(k+1) Lo_d(7-k), 0-based
+  }
+  f->len_z = 2;
+  f->a_lo_z[0] = f->a_lo_z[1] = f->s_lo_z[0] = f->s_lo_z[1] = Cc;
+  f->a_hi_z[0] = f->s_hi_z[0] = -Cc;
+  f->a_hi_z[1] = f->s_hi_z[1] = Cc;
+}
+
+void haar3d(gbm3d_filters* f);
+void bior(gbm3d_filters* f);
+
+void bank_of_opts(const gbm3d_opts* o, gbm3d_filters* f) {
+  if (o->wavelet == 1) haar3d(f);
+  else if (o->wavelet == 2) sym4haar(f);
+  else bior(f);
+}
+
 // 3D Haar bank: the two-tap Haar pair on all three axes (opts.wavelet = 1).
 void haar3d(gbm3d_filters* f) {
   std::memset(f, 0, sizeof(*f));
@@ -351,7 +379,8 @@ void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
   if (o->refStrideWie < 0 || o->refStrideWie > o->blockSizeWie)
     argfail(c, "refStrideWie must be in 1..blockSizeWie (0: blockSizeWie)");
   if (o->filtType != 0 && o->filtType != 1) argfail(c, "unrecognized filtering");  // denoiseAndAggregateGPU.m:54
-  if (o->wavelet != 0 && o->wavelet != 1) argfail(c, "wavelet must be 0 (bior1.5 x Haar) or 1 (3D Haar)");
+  if (o->wavelet < 0 || o->wavelet > 2)
+    argfail(c, "wavelet must be 0 (bior1.5 x Haar), 1 (3D Haar) or 2 (sym4 x Haar)");
   if (o->form < 0 || o->form > 2) argfail(c, "form must be 0 (plain), 1 (precision) or 2 (learned pilot)");
   if (o->form == 2 && !c->pilot_ready) argfail(c, "learned pilot: no parameters loaded (gbm3d_pilot_set_params)");
   c->form = o->form;
@@ -441,10 +470,10 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
 
 // denoiseAndAggregateGPU on device buffers: vol is (M d) x (N d) x K and
 // U, W are float ((M-1) s + d) x ((N-1) s + d).
-void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cnt, int M, int N, int d,
-            int d2, int K, int levels, int cycleSpin, const double* tau, const WaveletBank& bk, float* U,
-            float* W, int filtType, int s) {
-  const int m = M * d, n = N * d;
+// The cycle-spun 3D wavelet hard threshold (or medfilt3) of an m x n x K
+// volume: Vavg = max(mean over cycle spins, 0), returned in "ht.vsum".
+float* run_wavelet_ht(gbm3d_ctx* c, const float* vol, int m, int n, int K, int levels, int cycleSpin,
+                      const double* tau, const WaveletBank& bk, int filtType) {
   float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
   if (filtType == 1) {  // medfilt3 instead of the wavelet (denoiseAndAggregateGPU.m:165-168)
     StageTimer tw(c, 2);
@@ -495,6 +524,14 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
   }
   }
   }
+  return vsum;
+}
+
+void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cnt, int M, int N, int d,
+            int d2, int K, int levels, int cycleSpin, const double* tau, const WaveletBank& bk, float* U,
+            float* W, int filtType, int s) {
+  const int m = M * d, n = N * d;
+  float* vsum = run_wavelet_ht(c, vol, m, n, K, levels, cycleSpin, tau, bk, filtType);
   StageTimer tagg(c, 3);
   float* wgt = buf<float>(c, "ht.wgt", (size_t)M * N);
   launched(c, launch_ht_weights(vsum, m, n, M, N, d, K, cnt, wgt, c->st), "ht_weights");
@@ -676,8 +713,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   if (nS < 1 || nS > 8 || nW < 0 || nW > 8 || (o->Wiener && nW < 1)) argfail(c, "match spin count out of range");
   const size_t px = (size_t)Mp * Np;
   gbm3d_filters f;
-  if (o->wavelet == 1) haar3d(&f);
-  else bior(&f);
+  bank_of_opts(o, &f);
   const WaveletBank bk = make_bank(c, &f);
   std::vector<double> tau(o->levels * 7);
   tau_table(o->levels, o->tauMode, tau.data());
@@ -1259,8 +1295,7 @@ void pipeline_rgb(gbm3d_ctx* c, const double* const* dI, int m, int n, double si
   const size_t px = (size_t)Mp * Np, pm = (size_t)m * n;
   const double csig[3] = {sigma * std::sqrt(1.0 / 3.0), sigma * std::sqrt(0.5), sigma * std::sqrt(0.375)};
   gbm3d_filters f;
-  if (o->wavelet == 1) haar3d(&f);
-  else bior(&f);
+  bank_of_opts(o, &f);
   const WaveletBank bk = make_bank(c, &f);
   std::vector<double> tau1(o->levels * 7);
   tau_table(o->levels, o->tauMode, tau1.data());
@@ -1364,6 +1399,250 @@ void pipeline_rgb(gbm3d_ctx* c, const double* const* dI, int m, int n, double si
 }  // namespace
 
 extern "C" {
+
+}  // extern "C"
+
+namespace {
+
+// ---- video (VBM3D.m, matchBlocksV.m, denoiseAndAggregateV.m) -----------------------
+
+int video_frames(const gbm3d_opts* o) { return o->videoFrames > 0 ? o->videoFrames : 11; }
+
+void check_video(gbm3d_ctx* c, const gbm3d_opts* o, int d, int F, int K) {
+  if (o->numMin != o->numMax) argfail(c, "video matching: the tolerance branch is not supported", GBM3D_ERR_UNSUPPORTED);
+  if (!video_match_supported(d, F, K))
+    argfail(c, "video matching supports blockSize 8/16/32, an odd window of frames and numMax <= 32",
+            GBM3D_ERR_UNSUPPORTED);
+}
+
+// matchBlocksV + denoiseAndAggregateV on one window whose F search images are
+// built (pads); U, W: m x n x F double (device).
+void video_window(gbm3d_ctx* c, float* const* pads, int P, int m, int n, int F, int d, int K, int levels,
+                  int cycleSpin, const double* tau, const WaveletBank& bk, uint32_t* S, float* vol, double* U,
+                  double* W) {
+  const int M = m / d, N = n / d;
+  VideoMatchArgs A{};
+  for (int f = 0; f < F; ++f) A.pads[f] = pads[f];
+  A.P = P;
+  A.M = M;
+  A.N = N;
+  A.F = F;
+  A.K = K;
+  A.m = m;
+  A.n = n;
+  A.S = S;
+  A.volume = vol;
+  {
+    StageTimer t(c, 1);
+    launched(c, launch_match_video(d, A, c->st), "match_video");
+  }
+  float* vsum;
+  {
+    StageTimer t(c, 2);
+    vsum = run_wavelet_ht(c, vol, m, n, K, levels, cycleSpin, tau, bk, 0);
+    launched(c, launch_clamp01(vsum, (size_t)m * n * K, c->st), "clamp");  // Vavg = min(max(.,0),1)
+  }
+  StageTimer t(c, 3);
+  float* wgt = buf<float>(c, "v.wgt", (size_t)M * N);
+  launched(c, launch_ht_weights(vsum, m, n, M, N, d, K, nullptr, wgt, c->st), "ht_weights");
+  VideoAggArgs G{};
+  G.S = S;
+  G.wgt = wgt;
+  G.vsum = vsum;
+  G.M = M;
+  G.N = N;
+  G.d = d;
+  G.K = K;
+  G.F = F;
+  G.m = m;
+  G.n = n;
+  G.U = U;
+  G.W = W;
+  launched(c, launch_aggregate_video(G, c->st), "aggregate_video");
+}
+
+__global__ void k_video_accum(const double* __restrict__ U, const double* __restrict__ W, size_t n,
+                              float* __restrict__ Y, float* __restrict__ nn) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    Y[i] = (float)((double)Y[i] + U[i]);  // the reference's Y and nn are single arrays
+    nn[i] = (float)((double)nn[i] + W[i]);
+  }
+}
+
+// out frame (k - hw) += (Y ./ nn)(r + s, c + s) of frame k (the shift back), cropped to m0 x n0
+__global__ void k_video_out(const float* __restrict__ Y, const float* __restrict__ nn, int Mp, int Np, int m0,
+                            int n0, int hw, int nOut, int s, double* __restrict__ acc, int first) {
+  const size_t total = (size_t)m0 * n0 * nOut;
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(p % m0), c = (int)((p / m0) % n0), k = (int)(p / ((size_t)m0 * n0)) + hw;
+    const size_t o = (size_t)Mp * Np * k + pmod(r + s, Mp) + (size_t)Mp * pmod(c + s, Np);
+    const double v = (double)(Y[o] / nn[o]);
+    acc[p] = first ? v : acc[p] + v;
+  }
+}
+
+__global__ void k_video_final(const double* __restrict__ acc, size_t n, double nS, double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (double)(float)(acc[i] / nS);
+}
+
+// VBM3D.m:20-63 on device frames I (m0 x n0 x Kf, float64 column-major, the
+// reference's [0,1] scale): out (m0 x n0 x (Kf - nF + 1)).
+void pipeline_video(gbm3d_ctx* c, const double* I, int m0, int n0, int Kf, double sigma, const gbm3d_opts* o,
+                    double* out) {
+  check_opts(c, o);
+  const int d = o->blockSize, K = o->numMax, F = video_frames(o), hw = (F - 1) / 2;
+  check_video(c, o, d, F, K);
+  if (Kf < F) argfail(c, "fewer frames than the temporal window");
+  if (m0 < 1 || n0 < 1 || m0 > 32000 || n0 > 32000) argfail(c, "frame size out of range");
+  const int Mp = (m0 + d - 1) / d * d, Np = (n0 + d - 1) / d * d;
+  if (Mp - m0 > m0 || Np - n0 > n0) argfail(c, "frame smaller than the padding it needs");
+  const int nS = o->nMatchSpins;
+  if (nS < 1 || nS > 8) argfail(c, "match spin count out of range");
+  gbm3d_filters f;
+  bank_of_opts(o, &f);
+  const WaveletBank bk = make_bank(c, &f);
+  std::vector<double> tau(o->levels * 7);
+  tau_table(o->levels, o->tauMode, tau.data());
+  for (auto& t : tau) t *= sigma;
+  const size_t px = (size_t)Mp * Np, px0 = (size_t)m0 * n0;
+  const int P = pitch4(Mp + d), nOut = Kf - F + 1;
+  StageTimer tall(c, 7);
+  float* fr = buf<float>(c, "v.frames", px * Kf);
+  ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+  for (int k = 0; k < Kf; ++k) {
+    k_prep<<<grid2(Mp, Np), 256, 0, c->st>>>(I + px0 * k, m0, n0, fr + px * k, Mp, Np, c->flag);
+    launched(c, cudaGetLastError(), "prep");
+  }
+  float* Y = buf<float>(c, "v.Y", px * Kf);
+  float* nn = buf<float>(c, "v.nn", px * Kf);
+  double* U = buf<double>(c, "v.U", px * F);
+  double* W = buf<double>(c, "v.W", px * F);
+  double* acc = buf<double>(c, "v.acc", px0 * nOut);
+  uint32_t* S = buf<uint32_t>(c, "v.S", (size_t)K * (Mp / d) * (Np / d));
+  float* vol = buf<float>(c, "v.vol", px * K);
+  std::vector<float*> pads(F);
+  for (int q = 0; q < F; ++q) pads[q] = buf<float>(c, ("v.pad" + std::to_string(q)).c_str(), (size_t)P * (Np + d));
+  for (int ii = 0; ii < nS; ++ii) {
+    const int s = o->matchSpins[ii];
+    ck(c, cudaMemsetAsync(Y, 0, px * Kf * sizeof(float), c->st), "memset");
+    ck(c, cudaMemsetAsync(nn, 0, px * Kf * sizeof(float), c->st), "memset");
+    for (int jj = hw; jj < Kf - hw; ++jj) {
+      for (int q = 0; q < F; ++q)  // circshift(I3, [s, s, 0]) and matchBlocksV's search images
+        launched(c, launch_make_pad(fr + px * (jj - hw + q), Mp, Np, d, s, pads[q], P, c->st), "make_pad");
+      video_window(c, pads.data(), P, Mp, Np, F, d, K, o->levels, o->cycleSpin, tau.data(), bk, S, vol, U, W);
+      k_video_accum<<<1184, 256, 0, c->st>>>(U, W, px * F, Y + px * (jj - hw), nn + px * (jj - hw));
+      launched(c, cudaGetLastError(), "video_accum");
+    }
+    k_video_out<<<1184, 256, 0, c->st>>>(Y, nn, Mp, Np, m0, n0, hw, nOut, s, acc, ii == 0);
+    launched(c, cudaGetLastError(), "video_out");
+  }
+  k_video_final<<<1184, 256, 0, c->st>>>(acc, px0 * nOut, (double)nS, out);
+  launched(c, cudaGetLastError(), "video_out");
+}
+
+}  // namespace
+
+extern "C" {
+
+int gbm3d_vbm3d_device(gbm3d_ctx* c, const double* I, int m, int n, int frames, double sigma, const gbm3d_opts* o,
+                       double* out) {
+  return guarded(c, [&] {
+    if (!I || !out) argfail(c, "missing argument");
+    pipeline_video(c, I, m, n, frames, sigma, o, out);
+  });
+}
+
+int gbm3d_matchBlocksV(gbm3d_ctx* c, const double* I, int m, int n, int frames, const gbm3d_opts* o, uint32_t* S,
+                       float* Volume) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    const int d = o->blockSize, K = o->numMax;
+    check_video(c, o, d, frames, K);
+    if (!I || !S) argfail(c, "I and S are required");
+    if (m < 2 * d || n < 2 * d) argfail(c, "frames smaller than two blocks");
+    const int M = m / d, N = n / d, P = pitch4(m + d);
+    const size_t px = (size_t)m * n;
+    double* dI = buf<double>(c, "io.I", px * frames);
+    ck(c, cudaMemcpyAsync(dI, I, px * frames * 8, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    float* fr = buf<float>(c, "io.If", px * frames);
+    std::vector<float*> pads(frames);
+    VideoMatchArgs A{};
+    for (int q = 0; q < frames; ++q) {
+      k_prep<<<grid2(m, n), 256, 0, c->st>>>(dI + px * q, m, n, fr + px * q, m, n, c->flag);
+      launched(c, cudaGetLastError(), "prep");
+      pads[q] = buf<float>(c, ("v.pad" + std::to_string(q)).c_str(), (size_t)P * (n + d));
+      launched(c, launch_make_pad(fr + px * q, m, n, d, 0, pads[q], P, c->st), "make_pad");
+      A.pads[q] = pads[q];
+    }
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    float* dV = buf<float>(c, "io.V", px * K);
+    ck(c, cudaMemsetAsync(dV, 0, px * K * 4, c->st), "memset");
+    A.P = P;
+    A.M = M;
+    A.N = N;
+    A.F = frames;
+    A.K = K;
+    A.m = m;
+    A.n = n;
+    A.S = dS;
+    A.volume = dV;
+    launched(c, launch_match_video(d, A, c->st), "match_video");
+    ck(c, cudaMemcpyAsync(S, dS, (size_t)K * M * N * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    if (Volume) ck(c, cudaMemcpyAsync(Volume, dV, px * K * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    report_flag(c, flag);
+  });
+}
+
+int gbm3d_denoiseAndAggregateV(gbm3d_ctx* c, const float* Volume, const uint32_t* S, int M, int N, int frames,
+                               const double* tau, const gbm3d_filters* filters, const gbm3d_opts* o, double* U,
+                               double* W) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    const int d = o->blockSize, K = o->numMax;
+    check_video(c, o, d, frames, K);
+    if (!Volume || !S || !tau || !U || !W) argfail(c, "missing argument");
+    const int m = M * d, n = N * d;
+    const size_t px = (size_t)m * n;
+    for (size_t g = 0; g < (size_t)M * N * K; ++g)
+      if (S[g] < 1 || S[g] > (uint32_t)(d * d * frames)) argfail(c, "S holds an index outside the d x d x frames window");
+    gbm3d_filters fb;
+    if (filters) fb = *filters;
+    else sym4haar(&fb);
+    const WaveletBank bk = make_bank(c, &fb);
+    float* dV = buf<float>(c, "io.V", px * K);
+    uint32_t* dS = buf<uint32_t>(c, "io.S", (size_t)K * M * N);
+    ck(c, cudaMemcpyAsync(dV, Volume, px * K * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemcpyAsync(dS, S, (size_t)K * M * N * 4, cudaMemcpyHostToDevice, c->st), "H2D");
+    float* vsum = run_wavelet_ht(c, dV, m, n, K, o->levels, o->cycleSpin, tau, bk, 0);
+    launched(c, launch_clamp01(vsum, px * K, c->st), "clamp");
+    float* wgt = buf<float>(c, "v.wgt", (size_t)M * N);
+    launched(c, launch_ht_weights(vsum, m, n, M, N, d, K, nullptr, wgt, c->st), "ht_weights");
+    double* dU = buf<double>(c, "v.U", px * frames);
+    double* dW = buf<double>(c, "v.W", px * frames);
+    VideoAggArgs G{};
+    G.S = dS;
+    G.wgt = wgt;
+    G.vsum = vsum;
+    G.M = M;
+    G.N = N;
+    G.d = d;
+    G.K = K;
+    G.F = frames;
+    G.m = m;
+    G.n = n;
+    G.U = dU;
+    G.W = dW;
+    launched(c, launch_aggregate_video(G, c->st), "aggregate_video");
+    ck(c, cudaMemcpyAsync(U, dU, px * frames * 8, cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaMemcpyAsync(W, dW, px * frames * 8, cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+  });
+}
 
 int gbm3d_denoise_rgb_device(gbm3d_ctx* c, const double* R, const double* G, const double* B, int m, int n,
                              double sigma, const gbm3d_opts* o, double* UR, double* UG, double* UB) {

@@ -121,6 +121,27 @@ cudaError_t launch_match_global(int d, const GlobalMatchArgs& A, cudaStream_t st
 // in-place sym4 prefilter; work holds 8 * m * n floats
 cudaError_t launch_sym4_prefilter(float* I, int m, int n, float tau, float* work, cudaStream_t st);
 
+// ---- video (video.cu) ---------------------------------------------------------------------
+struct VideoMatchArgs {
+  const float* pads[32];  // search images of the window's frames (pitch P), circshifted as matched
+  int P, M, N, F, K;      // references M x N (stride d), window of F frames, group size K
+  int m, n;               // frame size (volume rows / columns)
+  uint32_t* S;            // K x M x N, 1-based index a + b d + f d^2 into the d x d x F window
+  float* volume;          // m x n x K
+};
+bool video_match_supported(int d, int F, int K);
+cudaError_t launch_match_video(int d, const VideoMatchArgs& A, cudaStream_t st);
+struct VideoAggArgs {
+  const uint32_t* S;
+  const float* wgt;       // weight per group
+  const float* vsum;      // denoised volume, m x n x K
+  int M, N, d, K, F, m, n;
+  double* U;              // m x n x F
+  double* W;
+};
+cudaError_t launch_aggregate_video(const VideoAggArgs& A, cudaStream_t st);
+cudaError_t launch_clamp01(float* v, size_t n, cudaStream_t st);
+
 // ---- learned pilot (pilot.cu) ----------------------------------------------------------
 constexpr int PILOT_LAYERS = 8;
 struct PilotNet {

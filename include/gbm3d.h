@@ -69,6 +69,10 @@ typedef struct gbm3d_opts {
    * pilot: the step-1 estimate comes from the pilot network (gbm3d_pilot_*).
    * Not in the reference. */
   int form;
+  /* video (gbm3d_vbm3d_device, gbm3d_matchBlocksV): frames in the temporal
+   * window, odd; 0 means VBM3D.m's default of 11.  opts.wavelet = 2 selects
+   * the video path's sym4 x Haar bank (getWaveFilters3D('sym','db',4,1)). */
+  int videoFrames;
 } gbm3d_opts;
 
 /* Separable 3D wavelet bank: 1D analysis (a_) and synthesis (s_) filters for the
@@ -198,6 +202,26 @@ int gbm3d_pilot_gradients(gbm3d_ctx* ctx, const float* img, const float* target,
  * reference. */
 int gbm3d_denoise_rgb_device(gbm3d_ctx* ctx, const double* R, const double* G, const double* B, int m, int n,
                              double sigma, const gbm3d_opts* opts, double* UR, double* UG, double* UB);
+
+/* ---- video (source/VBM3D.m, matchBlocksV.m, denoiseAndAggregateV.m) ------------
+ * Frames are float64 column-major m x n x frames on the reference's [0,1]
+ * scale (the video step clamps its estimate to [0,1]).
+ * [S,Volume] = matchBlocksV(I,sigma,opts)      source/matchBlocksV.m:21-116 (top-K)
+ *   I: m x n x F (F = the window, odd); S: K x M x N (M = floor(m/d)), 1-based
+ *   index a + (b-1) d + (f-1) d^2 into the d x d x F window; Volume m x n x K. */
+int gbm3d_matchBlocksV(gbm3d_ctx* ctx, const double* I, int m, int n, int frames, const gbm3d_opts* opts,
+                       uint32_t* S, float* Volume);
+/* [U,out] = denoiseAndAggregateV(Y,Volume,I,S,sigma,opts)   source/denoiseAndAggregateV.m:11-90
+ *   Volume (M d) x (N d) x K single; tau levels x 7 (sigma * getTau(levels, tauMode));
+ *   filters NULL = sym4 x Haar.  U and W (= out.K): (M d) x (N d) x frames double. */
+int gbm3d_denoiseAndAggregateV(gbm3d_ctx* ctx, const float* Volume, const uint32_t* S, int M, int N, int frames,
+                               const double* tau, const gbm3d_filters* filters, const gbm3d_opts* opts, double* U,
+                               double* W);
+/* Y = VBM3D(I,sigma,opts)                                  source/VBM3D.m:20-63
+ * Device pointers; out: m x n x (frames - videoFrames + 1), the frames with a
+ * full temporal window.  Asynchronous on the context stream. */
+int gbm3d_vbm3d_device(gbm3d_ctx* ctx, const double* I, int m, int n, int frames, double sigma,
+                       const gbm3d_opts* opts, double* out);
 
 /* Batched form: nimg images of any sizes (device pointers, float64
  * column-major, sigma per image) denoised with one option set.  With
