@@ -1,11 +1,15 @@
 // Block matching, precision form: BF16 tensor-core distances + exact FP32 re-rank.
 //
-// For a reference block a and a candidate b (8 x 8 patches, values centred by
-// the tile mean c), ||a - b||^2 = ||a'||^2 + ||b'||^2 - 2 a'.b' with a' = a - c,
-// b' = b - c.  ||a'||^2 is the same for every candidate of a reference, so the
-// candidates are ranked by ||b'||^2 - 2 a'.b', where a'.b' is a bf16 x bf16
-// product accumulated in fp32 on the tensor cores (tcgen05.mma, accumulator in
-// TMEM) and ||b'||^2 is exact fp32.  The 2K best by that approximate distance
+// For a reference block a and a candidate b (8 x 8 patches) with block means
+// ma, mb and zero-mean residuals a' = a - ma, b' = b - mb,
+//   ||a - b||^2 = 64 (ma - mb)^2 + ||a'||^2 + ||b'||^2 - 2 a'.b'
+// (the residuals are orthogonal to the constant block).  ||a'||^2 is the same
+// for every candidate of a reference, so the candidates are ranked by
+// 64 (ma - mb)^2 + ||b'||^2 - 2 a'.b', where a'.b' is a bf16 x bf16 product
+// accumulated in fp32 on the tensor cores (tcgen05.mma, accumulator in TMEM)
+// and the other terms are fp32.  Removing each block's mean before the bf16
+// rounding keeps the operands at the scale of the noise and texture, not of
+// the grey level, which is what bounds the rounding error of a'.b'.  The 2K best by that approximate distance
 // are then re-ranked by the exact FP32 sum of squared differences of the plain
 // matcher (same operation order), and the K best by (exact distance, window
 // index) are kept, so the match set equals the plain one whenever the true K
@@ -39,7 +43,7 @@ constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
 struct TcGeom {
   int PR, PC, NP;   // candidate-position grid of a tile
   int CH, CW;       // region (fp32 image) rows (padded even) and columns
-  size_t off_img32, off_nb2, off_A, off_B, off_heap, off_misc, bytes;
+  size_t off_img32, off_nb2, off_bm, off_A, off_B, off_heap, off_misc, bytes;
 };
 
 __host__ __device__ inline TcGeom tc_geom(int s, int d2) {
@@ -60,6 +64,7 @@ __host__ __device__ inline TcGeom tc_geom(int s, int d2) {
   g.off_B = take((size_t)2 * NC * TKD * 2, 1024);
   g.off_img32 = take((size_t)g.CH * g.CW * 4, 16);
   g.off_nb2 = take((size_t)2 * NC * 4, 16);             // ||b'||^2 of the two chunks in flight
+  g.off_bm = take((size_t)2 * NC * 4, 16);              // block means of the two chunks in flight
   g.off_heap = take((size_t)2 * CAND * 128 * 4, 16);    // per-thread heaps: values, then positions
   g.off_misc = take(64, 16);
   g.bytes = o;
@@ -74,14 +79,14 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
   const TcGeom G = tc_geom(s, D2);
   float* img32 = reinterpret_cast<float*>(smem + G.off_img32);        // column-major CH x CW
   float* nb2 = reinterpret_cast<float*>(smem + G.off_nb2);            // ||b'||^2, chunk buffer b at b*NC
+  float* bmean = reinterpret_cast<float*>(smem + G.off_bm);           // block means, same layout
   float* hv = reinterpret_cast<float*>(smem + G.off_heap);            // heap node q of thread t at q*128+t
   int* hp = reinterpret_cast<int*>(hv + CAND * 128);
   unsigned char* sA = smem + G.off_A;
   unsigned char* sB = smem + G.off_B;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + G.off_misc);    // [2]
   uint32_t* taddr_s = reinterpret_cast<uint32_t*>(mbar + 2);
-  float* red = reinterpret_cast<float*>(taddr_s + 1);                 // [4] warp partial sums
-  int* fail_s = reinterpret_cast<int*>(red + 4);
+  int* fail_s = reinterpret_cast<int*>(taddr_s + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tiles_i = (A.M + TI - 1) / TI;
@@ -103,35 +108,29 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
   // ---- region of the padded search image: pad rows i0*s .., cols j0*s .. ----
   const int R = A.m + D2, Q = A.n + D2;  // padded search-image extent
   const int y0 = i0 * s, x0 = j0 * s;
-  float part = 0.f;
-  int cntp = 0;
   for (int e = tid; e < G.CH * G.CW; e += 128) {
     const int y = e % G.CH, x = e / G.CH;
     float v = 0.f;
-    if (y0 + y < R && x0 + x < Q && y < G.PR + TD - 1) {
-      v = A.pad[(size_t)(y0 + y) + (size_t)(x0 + x) * A.P];
-      part += v;
-      ++cntp;
-    }
+    if (y0 + y < R && x0 + x < Q && y < G.PR + TD - 1) v = A.pad[(size_t)(y0 + y) + (size_t)(x0 + x) * A.P];
     img32[e] = v;
   }
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    part += __shfl_xor_sync(0xffffffffu, part, o);
-    cntp += __shfl_xor_sync(0xffffffffu, cntp, o);
-  }
-  if (lane == 0) {
-    red[warp] = part;
-    reinterpret_cast<int*>(fail_s)[1 + warp] = cntp;
-  }
   __syncthreads();
-  const int ntot = fail_s[1] + fail_s[2] + fail_s[3] + fail_s[4];
-  const float mean = ntot > 0 ? (red[0] + red[1] + red[2] + red[3]) / (float)ntot : 0.f;
   const int NPc = (G.NP + NC - 1) / NC * NC;
-  auto bf = [&](float x) -> uint32_t { return tc::bf16_bits(x - mean); };
+  // mean of the 8 x 8 block at (y, x) of the staged region
+  auto block_mean = [&](int y, int x) -> float {
+    float sum = 0.f;
+#pragma unroll
+    for (int cc = 0; cc < TD; ++cc)
+#pragma unroll
+      for (int r = 0; r < TD; ++r) sum += img32[(y + r) + (x + cc) * G.CH];
+    return sum * (1.f / TKD);
+  };
   // ---- A: this thread's reference block (at window offset (H, H)) ------------
+  float amean;
   {
     const int ry = s * li + H, rx = s * lj + H;
+    amean = block_mean(ry, rx);
+    auto bf = [&](float x) -> uint32_t { return tc::bf16_bits(x - amean); };
 #pragma unroll
     for (int r = 0; r < TD; ++r) {
       uint32_t w[4];
@@ -141,13 +140,15 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
       *reinterpret_cast<uint4*>(sA + tc::kmajor_offset(tid, r * TD, TKD)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
-  // B chunk: thread t builds the row of position chunk*NC + t (k = r*8 + c)
-  // and its squared norm ||b'||^2 (fp32 of the centred values; 0 past the grid)
+  // B chunk: thread t builds the row of position chunk*NC + t (k = r*8 + c):
+  // the block's mean, its zero-mean residual in bf16 and the residual's
+  // squared norm ||b'||^2 in fp32 (all 0 past the grid)
   auto build_B = [&](int chunk, int buf) {
     const int p = chunk * NC + tid;
     unsigned char* base = sB + (size_t)buf * NC * TKD * 2;
     const int pr = p % G.PR, pc = p / G.PR;
     const bool in = p < G.NP;
+    const float mean = in ? block_mean(pr, pc) : 0.f;
     float acc = 0.f;
 #pragma unroll
     for (int r = 0; r < TD; ++r) {
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
       *reinterpret_cast<uint4*>(base + tc::kmajor_offset(tid, r * TD, TKD)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     nb2[buf * NC + tid] = acc;
+    bmean[buf * NC + tid] = mean;
   };
   const int nch = NPc / NC;
   // chunks are visited from the middle of the position grid outwards: positions
@@ -239,7 +241,9 @@ __global__ void __launch_bounds__(128) k_match_tc(MatchArgs A) {
         uint32_t qm = 0;
 #pragma unroll
         for (int u = 0; u < 32; ++u) {
+          const float dm = amean - bmean[(c & 1) * NC + q0 + u];
           v[u] = fmaf(-2.f, v[u], nb2[(c & 1) * NC + q0 + u]);  // approximate distance (less ||a'||^2)
+          v[u] = fmaf((float)TKD * dm, dm, v[u]);
           qm |= (v[u] < thr ? 1u : 0u) << u;
         }
         qm &= inm;

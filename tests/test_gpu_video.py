@@ -38,7 +38,7 @@ CASES_MATCH = [
 def test_matchBlocksV_bit_identical(gpu, oracle, m, n, F, d, K, seed):
     _, I, s = _frames(m, n, F, 25.0, seed)
     o = {"blockSize": d, "numMax": K, "numMin": K, "nF": F}
-    S, V = api.matchBlocksV(I, s, o, ctx=gpu)
+    S, V = api.matchBlocksV(I, s, o)
     S0, V0 = oracle.matchBlocksV(I, d, K, prec=32)
     assert np.array_equal(np.asarray(S), S0), f"{np.mean(np.asarray(S) != S0):.4f} of the indices differ"
     assert np.array_equal(V, V0)
@@ -51,7 +51,7 @@ def test_denoiseAndAggregateV_bit_identical(gpu, oracle, m, n, F, d, K, seed):
     _, I, s = _frames(m, n, F, 25.0, seed)
     S0, V0 = oracle.matchBlocksV(I, d, K, prec=32)
     o = {"blockSize": d, "numMax": K, "numMin": K, "nF": F, "levels": 3}
-    U, out = api.denoiseAndAggregateV(None, V0, I, S0, s, o, ctx=gpu)
+    U, out = api.denoiseAndAggregateV(None, V0, I, S0, s, o)
     U0, W0 = oracle.denoiseAndAggregateV(V0, S0, d, F, s * options.getTau(3, 2), 3, 2, prec=32)
     assert np.array_equal(U, U0), f"U max-abs {max_abs(U, U0):.3e}"
     assert np.array_equal(out["K"], W0), f"W max-abs {max_abs(out['K'], W0):.3e}"
@@ -70,7 +70,7 @@ CASES_VBM3D = [
 def test_vbm3d_bit_identical(gpu, oracle, m, n, Kf, nF, d, spins, seed):
     clean, I, s = _frames(m, n, Kf, 25.0, seed)
     o = {"blockSize": d, "nF": nF, "matchSpins": list(spins)}
-    Y, out = api.VBM3D(I, s, o, ctx=gpu)
+    Y, out = api.VBM3D(I, s, o)
     Y0 = oracle.VBM3D(I, s, d=d, K=16, spins=spins, nF=nF, prec=32)
     assert Y.shape == (m, n, Kf - nF + 1)
     assert np.array_equal(Y, Y0), f"max-abs {max_abs(Y, Y0):.3e} on [0,1]"
@@ -85,9 +85,9 @@ def test_vbm3d_golden(gpu):
     """Against the FP64 FFT-route golden vectors (nF = 3, patch 8, spins [0 4])."""
     g = np.load(GOLDEN)
     I, s = g["noisy"] / 255.0, float(g["sigma"]) / 255.0
-    S, V = api.matchBlocksV(I[:, :, :3], s, {"blockSize": 8, "nF": 3}, ctx=gpu)
+    S, V = api.matchBlocksV(I[:, :, :3], s, {"blockSize": 8, "nF": 3})
     print(f"matchBlocksV: {np.mean(np.asarray(S) == g['S']):.4f} of the indices agree with FP64")
-    Y, _ = api.VBM3D(I, s, {"blockSize": 8, "nF": 3}, ctx=gpu)
+    Y, _ = api.VBM3D(I, s, {"blockSize": 8, "nF": 3})
     err = max_abs(Y, g["Y"])
     print(f"VBM3D: max-abs vs FP64 golden {err:.3e} on [0,1] ({err * 255:.3e} on 0-255)")
     assert err * 255 < 1.0
@@ -96,10 +96,10 @@ def test_vbm3d_golden(gpu):
 def test_video_option_errors(gpu):
     _, I, s = _frames(32, 32, 4, 25.0, 9)
     with pytest.raises(api.GBM3DError):
-        api.matchBlocksV(I, s, {"blockSize": 8}, ctx=gpu)  # an even number of frames
+        api.matchBlocksV(I, s, {"blockSize": 8})  # an even number of frames
     with pytest.raises(api.GBM3DError):
-        api.VBM3D(I[:, :, :3], s, {"blockSize": 8, "nF": 5}, ctx=gpu)  # fewer frames than the window
+        api.VBM3D(I[:, :, :3], s, {"blockSize": 8, "nF": 5})  # fewer frames than the window
     with pytest.raises(api.GBM3DError):
-        api.VBM3D(I, s, {"blockSize": 8, "nF": 3, "numMin": 8}, ctx=gpu)  # the tolerance branch
+        api.VBM3D(I, s, {"blockSize": 8, "nF": 3, "numMin": 8})  # the tolerance branch
     with pytest.raises(api.GBM3DError):
-        api.VBM3D(I, s, {"blockSize": 8, "nF": 3, "wname": "bior"}, ctx=gpu)
+        api.VBM3D(I, s, {"blockSize": 8, "nF": 3, "wname": "bior"})
