@@ -8,7 +8,8 @@ here = fileparts(mfilename('fullpath'));
 inc = ['-I' fullfile(here, '..', '..', 'include')];
 lib = ['-L' fullfile(here, '..')];
 gateways = {'matchBlocksCPU', 'denoiseAndAggregateGPU', 'matchBlocksWie', ...
-            'denoiseAndAggregateWieFast', 'denoiseAndAggregateWie', 'matchBlocksGPU'};
+            'denoiseAndAggregateWieFast', 'denoiseAndAggregateWie', 'matchBlocksGPU', ...
+            'matchBlocksV', 'denoiseAndAggregateV'};
 for k = 1:numel(gateways)
     mex('-outdir', here, inc, lib, '-lgbm3d', fullfile(here, [gateways{k} '.c']));
 end

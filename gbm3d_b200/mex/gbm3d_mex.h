@@ -106,6 +106,34 @@ static void gm_opts(const mxArray* o, gbm3d_opts* out) {
   }
 }
 
+/* The video functions' options: VBM3D.m:8-19's defaults for absent fields
+ * (blockSize 32, numMax = numMin = 16, levels 3, cycleSpin 2, tauMode 2) and
+ * the one bank it supports, getWaveFilters3D('sym','db',4,1). */
+static void gm_video_opts(const mxArray* o, gbm3d_opts* out) {
+  if (o && !mxIsStruct(o)) mexErrMsgIdAndTxt("gbm3d:opts", "opts must be a struct");
+  gbm3d_default_opts("default", out);
+  out->blockSize = gm_int_field(o, "blockSize", 32);
+  out->blockSizeWie = out->blockSize;
+  out->matchSize = 2 * out->blockSize;
+  out->numMax = gm_int_field(o, "numMax", 16);
+  out->numMin = gm_int_field(o, "numMin", 16);
+  out->levels = gm_int_field(o, "levels", 3);
+  out->cycleSpin = gm_int_field(o, "cycleSpin", 2);
+  out->tauMode = gm_int_field(o, "tauMode", 2);
+  out->Wiener = 0;
+  out->wavelet = 2;
+  out->videoFrames = gm_int_field(o, "nF", 11);
+  const char* want[2][2] = {{"wname", "sym"}, {"wnamez", "db"}};
+  for (int k = 0; k < 2; ++k) {
+    const mxArray* v = gm_field(o, want[k][0]);
+    char s[16] = {0};
+    if (v && (!mxIsChar(v) || mxGetString(v, s, sizeof(s)) != 0 || strcmp(s, want[k][1]) != 0))
+      mexErrMsgIdAndTxt("gbm3d:opts", "opts.%s: the video path supports '%s' only", want[k][0], want[k][1]);
+  }
+  if (gm_int_field(o, "order", 4) != 4 || gm_int_field(o, "orderz", 1) != 1)
+    mexErrMsgIdAndTxt("gbm3d:opts", "the video path supports opts.order = 4 and opts.orderz = 1 only");
+}
+
 /* ---- arguments ----------------------------------------------------------------- */
 
 static const double* gm_real_double(const mxArray* a, const char* what) {

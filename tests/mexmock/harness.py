@@ -20,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 MEXDIR = os.path.join(ROOT, "gbm3d_b200", "mex")
 OUT = os.path.join(HERE, "_build")
 GATEWAYS = ["matchBlocksCPU", "denoiseAndAggregateGPU", "matchBlocksWie", "denoiseAndAggregateWieFast",
-            "denoiseAndAggregateWie", "matchBlocksGPU"]
+            "denoiseAndAggregateWie", "matchBlocksGPU", "matchBlocksV", "denoiseAndAggregateV"]
 CLS = {np.dtype(np.float64): 6, np.dtype(np.float32): 7, np.dtype(np.int8): 8, np.dtype(np.uint8): 9,
        np.dtype(np.int32): 12, np.dtype(np.uint32): 13, np.dtype(np.int64): 14, np.dtype(np.bool_): 3}
 NP = {v: k for k, v in CLS.items()}
@@ -78,7 +78,8 @@ def mm():
             ("mm_err_id", C.c_char_p, []), ("mm_err_msg", C.c_char_p, []), ("mm_run_atexit", None, []),
             ("mm_class", C.c_int, [P]), ("mm_ndim", C.c_int, [P]), ("mm_dim", C.c_size_t, [P, C.c_int]),
             ("mm_numel", C.c_size_t, [P]), ("mm_data", P, [P]), ("mm_get_cell", P, [P, C.c_size_t]),
-            ("mm_destroy", None, [P])]:
+            ("mm_destroy", None, [P]), ("mm_nfields", C.c_int, [P]), ("mm_field_name", C.c_char_p, [P, C.c_int]),
+            ("mm_field_value", P, [P, C.c_int])]:
             f = getattr(_mm, name)
             f.restype, f.argtypes = res, args
     return _mm
@@ -123,6 +124,8 @@ def from_mx(p):
     if cls == 1:  # cell
         n = m.mm_numel(p)
         return Cell(shape, [from_mx(m.mm_get_cell(p, i)) for i in range(n)])
+    if cls == 2:  # 1 x 1 struct
+        return {m.mm_field_name(p, f).decode(): from_mx(m.mm_field_value(p, f)) for f in range(m.mm_nfields(p))}
     dt = NP[cls]
     n = m.mm_numel(p)
     buf = (C.c_char * (n * dt.itemsize)).from_address(m.mm_data(p))

@@ -57,6 +57,8 @@ mxArray* mxCreateCellMatrix(mwSize m, mwSize n);
 mxArray* mxCreateNumericMatrix(mwSize m, mwSize n, mxClassID c, mxComplexity x);
 mxArray* mxCreateNumericArray(mwSize nd, const mwSize* dims, mxClassID c, mxComplexity x);
 mxArray* mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity x);
+mxArray* mxCreateStructMatrix(mwSize m, mwSize n, int nfields, const char** names);
+void mxSetField(mxArray* a, mwIndex i, const char* name, mxArray* v);
 void mxDestroyArray(mxArray* a);
 void* mxMalloc(size_t n);
 void mxFree(void* p);

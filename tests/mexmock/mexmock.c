@@ -162,6 +162,26 @@ mxArray* mxCreateNumericArray(mwSize nd, const mwSize* dims, mxClassID c, mxComp
 }
 mxArray* mxCreateDoubleMatrix(mwSize m, mwSize n, mxComplexity x) { return mxCreateNumericMatrix(m, n, mxDOUBLE_CLASS, x); }
 
+/* 1 x 1 structs only (all the gateways create) */
+mxArray* mxCreateStructMatrix(mwSize m, mwSize n, int nfields, const char** names) {
+  mwSize d[2] = {m, n};
+  mxArray* a = make(mxSTRUCT_CLASS, 2, d);
+  a->cells = (mxArray**)calloc(64, sizeof(mxArray*));
+  a->fnames = (char**)calloc(64, sizeof(char*));
+  for (int f = 0; f < nfields && f < 64; ++f) a->fnames[f] = strdup(names[f]);
+  a->nfields = nfields;
+  return a;
+}
+void mxSetField(mxArray* a, mwIndex i, const char* name, mxArray* v) {
+  if (!mxIsStruct(a) || i != 0) return;
+  for (int f = 0; f < a->nfields; ++f)
+    if (strcmp(a->fnames[f], name) == 0) {
+      mxDestroyArray(a->cells[f]);
+      a->cells[f] = v;
+      return;
+    }
+}
+
 void mxDestroyArray(mxArray* a) {
   if (!a) return;
   if (a->cls == mxCELL_CLASS || a->cls == mxSTRUCT_CLASS) {
@@ -249,4 +269,7 @@ size_t mm_dim(const mxArray* a, int k) { return k < (int)a->nd ? a->dims[k] : 1;
 size_t mm_numel(const mxArray* a) { return numel(a); }
 void* mm_data(const mxArray* a) { return a->data; }
 mxArray* mm_get_cell(const mxArray* a, size_t i) { return mxGetCell(a, i); }
+int mm_nfields(const mxArray* a) { return mxIsStruct(a) ? a->nfields : 0; }
+const char* mm_field_name(const mxArray* a, int f) { return a->fnames[f]; }
+mxArray* mm_field_value(const mxArray* a, int f) { return a->cells[f]; }
 void mm_destroy(mxArray* a) { mxDestroyArray(a); }

@@ -232,3 +232,72 @@ def test_GBM3D_driver_through_gateways(gw, m, n, profile):
     Ua, out = api.GBM3D(I0, sigma, {"profile": profile})
     assert np.array_equal(U1[:m, :n], out["U1"])
     assert np.array_equal(Uf, Ua)
+
+
+# ---- video gateways ----------------------------------------------------------------
+
+def _vopts(**kw):
+    o = {"blockSize": 8.0, "numMax": 16.0, "numMin": 16.0, "wname": "sym", "wnamez": "db", "order": 4.0,
+         "orderz": 1.0, "levels": 3.0, "cycleSpin": 2.0, "tauMode": 2.0, "nF": 3.0,
+         "matchSpins": np.array([0.0, 4.0])}
+    o.update(kw)
+    return o
+
+
+def test_video_gateways_check_arguments(gw):
+    with pytest.raises(H.MexError) as e:
+        gw["matchBlocksV"](np.zeros((32, 32, 4)), 0.1, _vopts(), nargout=2)
+    assert e.value.ident == "gbm3d:args" and "odd number of frames" in e.value.msg
+    with pytest.raises(H.MexError) as e:
+        gw["matchBlocksV"](np.zeros((32, 32, 3)), 0.1, _vopts(wname="bior"), nargout=2)
+    assert e.value.ident == "gbm3d:opts" and "sym" in e.value.msg
+    with pytest.raises(H.MexError) as e:
+        gw["denoiseAndAggregateV"](0, np.zeros((32, 32, 16), dtype=np.float32), np.zeros((30, 32, 3)),
+                                   _set_to_cell(np.ones((16, 4, 4), dtype=np.uint32)), 0.1, _vopts(), nargout=2)
+    assert e.value.ident == "gbm3d:args" and "frames must be" in e.value.msg
+
+
+@pytest.mark.gpu
+def test_video_gateways_match_api(gw):
+    from gbm3d_b200 import api
+    _, noisy = synth.video(32, 40, 3, 25.0, seed=46)
+    I, s = noisy / 255.0, 25.0 / 255.0
+    C, V = gw["matchBlocksV"](I, s, _vopts(), nargout=2)
+    S, cnt = _cell_to_set(C, 16)
+    Sa, Va = api.matchBlocksV(I, s, {"blockSize": 8, "nF": 3})
+    assert np.array_equal(S, np.asarray(Sa)) and np.all(cnt == 16) and np.array_equal(V, Va)
+    U, out = gw["denoiseAndAggregateV"](0, V, I, C, s, _vopts(), nargout=2)
+    Ua, outa = api.denoiseAndAggregateV(None, Va, I, Sa, s, {"blockSize": 8, "nF": 3})
+    assert np.array_equal(U, Ua) and np.array_equal(out["K"], outa["K"])
+    assert out["Z"].shape == (32, 40) and np.all(out["Z"] == 16)
+
+
+@pytest.mark.gpu
+def test_VBM3D_driver_through_gateways(gw):
+    """VBM3D.m:24-63 replayed with only the two video gateways equals api.VBM3D
+    (Y and nn single, each window's U and out.K added as float32(Y + U))."""
+    from gbm3d_b200 import api
+    _, noisy = synth.video(30, 44, 5, 25.0, seed=47)
+    I0, sigma = noisy / 255.0, 25.0 / 255.0
+    d, nF, spins = 8, 3, [0, 4]
+    m, n, Kf = I0.shape
+    M, N = -(-m // d) * d, -(-n // d) * d
+    I2 = np.stack([options.myMirrorPadImage(I0[:, :, k], M, N) for k in range(Kf)], axis=2)
+    mo = _vopts(nF=float(nF), matchSpins=np.array(spins, dtype=np.float64))
+    hw = (nF - 1) // 2
+    acc = np.zeros((m, n, Kf - nF + 1))
+    for s in spins:
+        Y = np.zeros((M, N, Kf), dtype=np.float32)
+        nn = np.zeros((M, N, Kf), dtype=np.float32)
+        for jj in range(hw, Kf - hw):
+            I3 = np.roll(I2[:, :, jj - hw:jj + hw + 1], (s, s), axis=(0, 1))
+            C, V = gw["matchBlocksV"](I3, sigma, mo, nargout=2)
+            U, out = gw["denoiseAndAggregateV"](0, V, I3, C, sigma, mo, nargout=2)
+            Y[:, :, jj - hw:jj + hw + 1] = (Y[:, :, jj - hw:jj + hw + 1].astype(np.float64) + U).astype(np.float32)
+            nn[:, :, jj - hw:jj + hw + 1] = (nn[:, :, jj - hw:jj + hw + 1].astype(np.float64)
+                                             + out["K"]).astype(np.float32)
+        R = np.roll(Y / nn, (-s, -s), axis=(0, 1))
+        acc += R[:m, :n, hw:Kf - hw].astype(np.float64)
+    Yd = (acc / len(spins)).astype(np.float32).astype(np.float64)
+    Ya, _ = api.VBM3D(I0, sigma, {"blockSize": d, "nF": nF, "matchSpins": spins})
+    assert np.array_equal(Yd, Ya)
