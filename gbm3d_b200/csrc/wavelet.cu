@@ -337,32 +337,50 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
 
 constexpr int FSY = 64, FSX = 32;  // fast synthesis tile: samples along y and x
 
+// Synthesis of one level for the bior / Haar banks.  A CTA makes FSY x FSX
+// outputs of the two slots of one qz: the 8 bands' coefficients it needs are
+// staged in shared memory, then each output is the same serial fmaf chain, in
+// the same tap order, as the generic kernel and the oracle.  Each thread
+// produces a run of outputs from one window of coefficients held in
+// registers, so a staged coefficient is read from shared memory about once
+// per run instead of once per tap:
+//   y-pass: a thread makes 16 consecutive outputs (8 even/odd pairs) of one
+//           (band combination, qx) column from 8 + LO lo and 8 + HI hi values;
+//   x-pass: a thread makes 8 consecutive columns of one output row for both
+//           slot bands, then the slot pass and the write/accumulate, in
+//           registers.
+// Row strides of the staged arrays are odd, so lanes that walk neighbouring
+// rows hit distinct banks.
 template <int SL0, int SH>
-__global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restrict__ bands,
-                                                            const float* __restrict__ approx, int Oy, int Ox,
-                                                            int Oz, SynthOut o, FastBank fb) {
+__global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restrict__ bands,
+                                                           const float* __restrict__ approx, int Oy, int Ox,
+                                                           int Oz, SynthOut o, FastBank fb) {
   constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
   constexpr int NQY = (FSY - 1 + REACH) / 2 + 1;  // staged coefficients along y
   constexpr int NQX = (FSX - 1 + REACH) / 2 + 1;  // and along x
+  constexpr int BQ = NQY | 1;                     // row stride of the staged coefficients
+  constexpr int YS = FSY + 1;                     // row stride of the y-pass outputs
+  constexpr int LW = (SL0 + 2) / 2;               // lo reach beyond a pair index (t + LW at most)
+  constexpr int HW = SH / 2;                      // hi reach
+  static_assert(FSY % 16 == 0 && FSX % 8 == 0 && FSY * (FSX / 8) == 256, "tile shape");
   extern __shared__ float sm[];
-  float* B = sm;                    // [8 code][NQX qx][NQY qy]
-  float* Y = sm + 8 * NQX * NQY;    // [4 comb][NQX qx][FSY py]
-  float* X = sm;                    // [2 fz][FSX px][FSY py]  (reuses B after the y-pass)
+  float* B = sm;                    // [8 code][NQX qx][BQ]
+  float* Y = sm + 8 * NQX * BQ;     // [4 comb][NQX qx][YS]
   const int Iy = Oy >> 1, Ix = Ox >> 1, Iz = Oz >> 1;
   const int py0 = blockIdx.x * FSY, px0 = blockIdx.y * FSX, qz = blockIdx.z;
   const int qy0 = py0 >> 1, qx0 = px0 >> 1;
   const size_t bsz = (size_t)Iy * Ix * Iz, zoff = (size_t)Iy * Ix * qz;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  constexpr int QT = (NQY + 31) / 32;  // coefficient rows per lane
+  constexpr int QT = (NQY + 31) / 32;
 
-  // stage 1: stage the 8 bands (warps over (code, qx) rows, lanes over qy)
+  // stage the 8 bands (warps over (code, qx) rows, lanes over qy)
   int qyv[QT];
 #pragma unroll
   for (int t = 0; t < QT; ++t) qyv[t] = wrap1(qy0 + lane + 32 * t, Iy);
   for (int row = w; row < 8 * NQX; row += 8) {
-    const int code = row / NQX, qxl = row % NQX;
+    const int code = row / NQX, qxl = row - code * NQX;
     const float* src = (code ? bands + code * bsz : approx) + zoff + (size_t)Iy * wrap1(qx0 + qxl, Ix);
-    float* dst = B + row * NQY;
+    float* dst = B + row * BQ;
 #pragma unroll
     for (int t = 0; t < QT; ++t) {
       const int qyl = lane + 32 * t;
@@ -370,76 +388,94 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_fast(const float* __restr
     }
   }
   __syncthreads();
-  // y-pass: rows py = 2t and 2t+1 from coefficients t + j (warps over (comb, qx), lanes over t)
-  for (int row = w; row < 4 * NQX; row += 8) {
-    const int comb = row / NQX, qxl = row % NQX;
-    const float* bl = B + ((0 + 2 * comb) * NQX + qxl) * NQY + lane;
-    const float* bh = B + ((1 + 2 * comb) * NQX + qxl) * NQY + lane;
-    float ev = 0.f, od = 0.f;
-    // even output 2t: taps k even, coefficient t + k/2; odd output 2t+1: k odd, t + (k+1)/2
+  // y-pass: item = (comb, run, qx); outputs py = 16 run .. 16 run + 15 of column qx
+  constexpr int NRUN = FSY / 16;
+  for (int it = threadIdx.x; it < 4 * NRUN * NQX; it += 256) {
+    const int qxl = it % NQX, r = it / NQX, run = r % NRUN, comb = r / NRUN;
+    const float* bl = B + ((2 * comb) * NQX + qxl) * BQ + 8 * run;
+    const float* bh = B + ((2 * comb + 1) * NQX + qxl) * BQ + 8 * run;
+    float lw[8 + LW], hw[8 + HW];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int k = SL0 + u;
-      if (k % 2 == 0) ev = fmaf(fb.slo[u], bl[k / 2], ev);
-      else od = fmaf(fb.slo[u], bl[(k + 1) / 2], od);
-    }
+    for (int j = 0; j < 8 + LW; ++j) lw[j] = bl[j];
 #pragma unroll
-    for (int k = 0; k < SH; ++k) {
-      if (k % 2 == 0) ev = fmaf(fb.shi[k], bh[k / 2], ev);
-      else od = fmaf(fb.shi[k], bh[(k + 1) / 2], od);
+    for (int j = 0; j < 8 + HW; ++j) hw[j] = bh[j];
+    float* dst = Y + (comb * NQX + qxl) * YS + 16 * run;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      float ev = 0.f, od = 0.f;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int k = SL0 + u;
+        if (k % 2 == 0) ev = fmaf(fb.slo[u], lw[t + k / 2], ev);
+        else od = fmaf(fb.slo[u], lw[t + (k + 1) / 2], od);
+      }
+#pragma unroll
+      for (int k = 0; k < SH; ++k) {
+        if (k % 2 == 0) ev = fmaf(fb.shi[k], hw[t + k / 2], ev);
+        else od = fmaf(fb.shi[k], hw[t + (k + 1) / 2], od);
+      }
+      dst[2 * t] = ev;
+      dst[2 * t + 1] = od;
     }
-    float* dst = Y + row * FSY + 2 * lane;
-    dst[0] = ev;
-    dst[1] = od;
   }
   __syncthreads();
-  // x-pass: columns px = 2t and 2t+1 (lanes along py)
-  const int py = lane + 32 * (w & 1);
-  for (int j = w >> 1; j < FSX; j += 4) {
-    const int t = j % (FSX / 2), fz = j / (FSX / 2);
-    const float* yl = Y + ((0 + 2 * fz) * NQX + t) * FSY + py;
-    const float* yh = Y + ((1 + 2 * fz) * NQX + t) * FSY + py;
-    float ev = 0.f, od = 0.f;
+  // x-pass for both slot bands, then the slot pass: thread = (run of 8 columns, row py)
+  const int py = threadIdx.x % FSY, run = threadIdx.x / FSY;
+  float xv[2][8];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int k = SL0 + u;
-      if (k % 2 == 0) ev = fmaf(fb.slo[u], yl[(k / 2) * FSY], ev);
-      else od = fmaf(fb.slo[u], yl[((k + 1) / 2) * FSY], od);
-    }
+  for (int fz = 0; fz < 2; ++fz) {
+    const float* yl = Y + ((2 * fz) * NQX + 4 * run) * YS + py;      // lo in x
+    const float* yh = Y + ((2 * fz + 1) * NQX + 4 * run) * YS + py;  // hi in x
+    float lw[4 + LW], hw[4 + HW];
 #pragma unroll
-    for (int k = 0; k < SH; ++k) {
-      if (k % 2 == 0) ev = fmaf(fb.shi[k], yh[(k / 2) * FSY], ev);
-      else od = fmaf(fb.shi[k], yh[((k + 1) / 2) * FSY], od);
+    for (int j = 0; j < 4 + LW; ++j) lw[j] = yl[j * YS];
+#pragma unroll
+    for (int j = 0; j < 4 + HW; ++j) hw[j] = yh[j * YS];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      float ev = 0.f, od = 0.f;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int k = SL0 + u;
+        if (k % 2 == 0) ev = fmaf(fb.slo[u], lw[t + k / 2], ev);
+        else od = fmaf(fb.slo[u], lw[t + (k + 1) / 2], od);
+      }
+#pragma unroll
+      for (int k = 0; k < SH; ++k) {
+        if (k % 2 == 0) ev = fmaf(fb.shi[k], hw[t + k / 2], ev);
+        else od = fmaf(fb.shi[k], hw[t + (k + 1) / 2], od);
+      }
+      xv[fz][2 * t] = ev;
+      xv[fz][2 * t + 1] = od;
     }
-    // X aliases B, which no thread reads after the barrier above
-    X[(fz * FSX + 2 * t) * FSY + py] = ev;
-    X[(fz * FSX + 2 * t + 1) * FSY + py] = od;
   }
-  __syncthreads();
   // slot-axis pass: slot 2qz from tap 0, slot 2qz-1 from tap 1; write or accumulate
   const int gy = py0 + py;
   if (gy < Oy) {
     const int oy = wrap1(gy - o.shift, Oy);
     float* r0 = o.out + oy + (size_t)Oy * Ox * pmod(2 * qz - o.shift, Oz);
     float* r1 = o.out + oy + (size_t)Oy * Ox * pmod(2 * qz - 1 - o.shift, Oz);
-    const int pxe = min(FSX, Ox - px0);
-    for (int px = w >> 1; px < pxe; px += 4) {
-      const float x0 = X[(0 * FSX + px) * FSY + py], x1 = X[(1 * FSX + px) * FSY + py];
-      const float v0 = fmaf(fb.szh[0], x1, fmaf(fb.szl[0], x0, 0.f));
-      const float v1 = fmaf(fb.szh[1], x1, fmaf(fb.szl[1], x0, 0.f));
-      const size_t col = (size_t)Oy * wrap1(px0 + px - o.shift, Ox);
-      float* d0 = r0 + col;
-      float* d1 = r1 + col;
-      float a0 = o.first ? v0 : *d0 + v0;
-      float a1 = o.first ? v1 : *d1 + v1;
-      if (o.last) {
-        a0 = a0 / o.cycles;
-        a0 = a0 > 0.f ? a0 : 0.f;
-        a1 = a1 / o.cycles;
-        a1 = a1 > 0.f ? a1 : 0.f;
+#pragma unroll
+    for (int px = 0; px < 8; ++px) {
+      const int gx = px0 + 8 * run + px;
+      if (gx < Ox) {
+        const float x0 = xv[0][px], x1 = xv[1][px];
+        const float v0 = fmaf(fb.szh[0], x1, fmaf(fb.szl[0], x0, 0.f));
+        const float v1 = fmaf(fb.szh[1], x1, fmaf(fb.szl[1], x0, 0.f));
+        const size_t col = (size_t)Oy * wrap1(gx - o.shift, Ox);
+        float* d0 = r0 + col;
+        float* d1 = r1 + col;
+        float a0 = o.first ? v0 : *d0 + v0;
+        float a1 = o.first ? v1 : *d1 + v1;
+        if (o.last) {
+          a0 = a0 / o.cycles;
+          a0 = a0 > 0.f ? a0 : 0.f;
+          a1 = a1 / o.cycles;
+          a1 = a1 > 0.f ? a1 : 0.f;
+        }
+        *d0 = a0;
+        *d1 = a1;
       }
-      *d0 = a0;
-      *d1 = a1;
     }
   }
 }
@@ -497,12 +533,11 @@ static cudaError_t launch_synthesis_fast(const float* bands, const float* approx
                                          const SynthOut& o, const FastBank& fb, cudaStream_t st) {
   constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
   constexpr int NQY = (FSY - 1 + REACH) / 2 + 1, NQX = (FSX - 1 + REACH) / 2 + 1;
-  const size_t a = (size_t)8 * NQX * NQY, x = (size_t)2 * FSX * FSY;
-  const size_t sm = ((a > x ? a : x) + (size_t)4 * NQX * FSY) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_fast<SL0, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const size_t sm = ((size_t)8 * NQX * (NQY | 1) + (size_t)4 * NQX * (FSY + 1)) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_win<SL0, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   dim3 grid((Oy + FSY - 1) / FSY, (Ox + FSX - 1) / FSX, Oz / 2);
-  k_wav_synthesis_fast<SL0, SH><<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, fb);
+  k_wav_synthesis_win<SL0, SH><<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, fb);
   return cudaGetLastError();
 }
 
