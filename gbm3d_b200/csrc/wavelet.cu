@@ -284,26 +284,28 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
     }
   }
   __syncthreads();
-  // stage 2: pass along the slow axis, lo and hi together from the same inputs
-  // (warps over (fz, qx), lanes over rows)
-  for (int pq = w; pq < 2 * FQX; pq += 8) {
-    const int fz = pq / FQX, qx = pq % FQX;
+  // stage 2: pass along the slow axis, lo and hi together from the same inputs.
+  // Item = (fz, run of RX coefficients qx, row yy), lanes over rows; the run's
+  // inputs (staged columns 2 q0 .. 2 (q0 + RX - 1) + HALO) are read once into
+  // registers.
+  constexpr int RX = 8, NRX = FQX / RX, NV = 2 * RX + LA - 2;
+  for (int it = threadIdx.x; it < 2 * NRX * NY; it += 256) {
+    const int yy = it % NY, r = it / NY, run = r % NRX, fz = r / NRX;
+    const int q0 = run * RX;
+    const float* col = tz + fz * NX * NY + yy + 2 * q0 * NY;
+    float v[NV];
 #pragma unroll
-    for (int t = 0; t < RT; ++t) {
-      const int yy = lane + 32 * t;
-      if (yy >= NY) continue;
-      const float* src = tz + fz * NX * NY + yy + (2 * qx + HALO) * NY;  // input x = 2qx - k
-      float v[LA];
+    for (int j = 0; j < NV; ++j) v[j] = col[j * NY];
+    float* dst = tx + (yy & 1) * NYHP + (yy >> 1);
 #pragma unroll
-      for (int k = 0; k < LA; ++k) v[k] = src[-k * NY];
-      float lo = 0.f, hi = 0.f;
+    for (int q = 0; q < RX; ++q) {
+      float lo = 0.f, hi = 0.f;  // tap k reads input x = 2 qx - k: staged column 2 q + HALO - k of the run
 #pragma unroll
-      for (int k = 0; k < LA; ++k) lo = fmaf(fb.alo[k], v[k], lo);
+      for (int k = 0; k < LA; ++k) lo = fmaf(fb.alo[k], v[2 * q + HALO - k], lo);
 #pragma unroll
-      for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[HA0 + k], hi);
-      float* dst = tx + (yy & 1) * NYHP + (yy >> 1);
-      dst[((0 + 2 * fz) * FQX + qx) * 2 * NYHP] = lo;
-      dst[((1 + 2 * fz) * FQX + qx) * 2 * NYHP] = hi;
+      for (int k = 0; k < 2; ++k) hi = fmaf(fb.ahi[k], v[2 * q + HALO - HA0 - k], hi);
+      dst[((0 + 2 * fz) * FQX + q0 + q) * 2 * NYHP] = lo;
+      dst[((1 + 2 * fz) * FQX + q0 + q) * 2 * NYHP] = hi;
     }
   }
   __syncthreads();
@@ -377,14 +379,17 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restri
   int qyv[QT];
 #pragma unroll
   for (int t = 0; t < QT; ++t) qyv[t] = wrap1(qy0 + lane + 32 * t, Iy);
-  for (int row = w; row < 8 * NQX; row += 8) {
-    const int code = row / NQX, qxl = row - code * NQX;
-    const float* src = (code ? bands + code * bsz : approx) + zoff + (size_t)Iy * wrap1(qx0 + qxl, Ix);
-    float* dst = B + row * BQ;
+  for (int qxl = w; qxl < NQX; qxl += 8) {  // the 8 bands' rows of column qx, one band after another
+    const size_t coff = zoff + (size_t)Iy * wrap1(qx0 + qxl, Ix);
 #pragma unroll
-    for (int t = 0; t < QT; ++t) {
-      const int qyl = lane + 32 * t;
-      if (qyl < NQY) dst[qyl] = __ldg(src + qyv[t]);
+    for (int code = 0; code < 8; ++code) {
+      const float* src = (code ? bands + code * bsz : approx) + coff;
+      float* dst = B + (code * NQX + qxl) * BQ;
+#pragma unroll
+      for (int t = 0; t < QT; ++t) {
+        const int qyl = lane + 32 * t;
+        if (qyl < NQY) dst[qyl] = __ldg(src + qyv[t]);
+      }
     }
   }
   __syncthreads();
@@ -455,14 +460,15 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restri
     const int oy = wrap1(gy - o.shift, Oy);
     float* r0 = o.out + oy + (size_t)Oy * Ox * pmod(2 * qz - o.shift, Oz);
     float* r1 = o.out + oy + (size_t)Oy * Ox * pmod(2 * qz - 1 - o.shift, Oz);
+    const int gx0 = px0 + 8 * run;
+    int ox = wrap1(gx0 - o.shift, Ox);  // output column of gx0, then stepped by one with wrap
 #pragma unroll
     for (int px = 0; px < 8; ++px) {
-      const int gx = px0 + 8 * run + px;
-      if (gx < Ox) {
+      if (gx0 + px < Ox) {
         const float x0 = xv[0][px], x1 = xv[1][px];
         const float v0 = fmaf(fb.szh[0], x1, fmaf(fb.szl[0], x0, 0.f));
         const float v1 = fmaf(fb.szh[1], x1, fmaf(fb.szl[1], x0, 0.f));
-        const size_t col = (size_t)Oy * wrap1(gx - o.shift, Ox);
+        const size_t col = (size_t)Oy * ox;
         float* d0 = r0 + col;
         float* d1 = r1 + col;
         float a0 = o.first ? v0 : *d0 + v0;
@@ -476,6 +482,7 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restri
         *d0 = a0;
         *d1 = a1;
       }
+      ox = ox + 1 == Ox ? 0 : ox + 1;
     }
   }
 }
