@@ -682,6 +682,57 @@ cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy
   return cudaGetLastError();
 }
 
+// k_ht_weights for patch 8: the whole group (nm slots of 8 x 8) is staged in
+// shared memory slot-major ([k][c][r]), then each lane walks its elements
+// e = lane + 32 t of the three difference arrays in increasing e, as the
+// other versions do.  In that layout the slot term's element e sits at e and
+// e + 64, and the x term's at e + 24 k (k = e / 40), so most of the per-term
+// index arithmetic goes away.
+__global__ void __launch_bounds__(128) k_ht_weights_8(const float* __restrict__ V, int m, int n, int M, int N,
+                                                      int K, const int32_t* __restrict__ cnt,
+                                                      float* __restrict__ wgt) {
+  constexpr int D = 8, DM = D - 3, SL = D * D, SX = D * DM;
+  extern __shared__ float shw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * 4 + warp;
+  if (g >= M * N) return;
+  float* sg = shw + warp * K * SL;
+  const int i = g % M, j = g / M;
+  const int nm = cnt ? cnt[g] : K;
+  const size_t sz = (size_t)m * n;
+  // lane: row r = lane % 8 of columns lane / 8 and lane / 8 + 4 of every slot
+  const float* p0 = V + (size_t)i * D + (size_t)(j * D + (lane >> 3)) * m + (lane & 7);
+  const float* p1 = p0 + (size_t)4 * m;
+  for (int k = 0; k < nm; ++k) {
+    sg[k * SL + lane] = __ldg(p0 + sz * k);
+    sg[k * SL + 32 + lane] = __ldg(p1 + sz * k);
+  }
+  __syncwarp();
+  float tx = 0.f, ty = 0.f, tz = 0.f;
+  // x term: element r + D (c + DM k) -> V(r, c .. c+3, k) at r + D c + SL k = e + (SL - SX) k
+  for (int e = lane; e < nm * SX; e += 32) {
+    const int k = e / SX;
+    const float* q = sg + e + (SL - SX) * k;
+    tx = tx + fabsf(d3(q[0], q[D], q[2 * D], q[3 * D]));
+  }
+  // y term: element r + DM (c + D k) -> V(r .. r+3, c, k)
+  for (int e = lane; e < nm * SX; e += 32) {
+    const int k = e / SX, rem = e - k * SX, c = rem / DM, r = rem - c * DM;
+    const float* q = sg + k * SL + c * D + r;
+    ty = ty + fabsf(d3(q[0], q[1], q[2], q[3]));
+  }
+  // slot term: element r + D (c + D k) of the pair (k, k+1)
+  for (int e = lane; e < (nm - 1) * SL; e += 32) tz = tz + fabsf(sg[e + SL] - sg[e]);
+  tx = warp_sum(tx);
+  ty = warp_sum(ty);
+  tz = warp_sum(tz);
+  if (lane == 0) {
+    float w = tx * 0.25f + ty * 0.25f;
+    w = w + tz;
+    wgt[g] = 1.f / (w + 2.220446049250313e-16f);
+  }
+}
+
 cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int d, int K,
                               const int32_t* cnt, float* wgt, cudaStream_t st) {
   const int G = M * N;
@@ -690,7 +741,10 @@ cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int
     return cudaGetLastError();
   }
   if (d == 8) {
-    k_ht_weights_t<8><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    const size_t smb = (size_t)4 * K * 64 * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(k_ht_weights_8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
+    if (e != cudaSuccess) return e;
+    k_ht_weights_8<<<(G + 3) / 4, 128, smb, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
     return cudaGetLastError();
   }
   if (d == 32) {
