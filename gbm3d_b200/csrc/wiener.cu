@@ -113,15 +113,33 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
   // ---- load the two groups -----------------------------------------------
   if (A.padP) {
     const int i = g % A.M, j = g / A.M;
-    for (int k = 0; k < K; ++k) {
-      int e = (int)A.S[(size_t)g * K + k] - 1;
+    // lane k decodes match k (window offsets a, b), then the offsets are broadcast
+    int ma = 0, mb = 0;
+    if (lane < K) {
+      int e = (int)A.S[(size_t)g * K + lane] - 1;
       if ((unsigned)e >= (unsigned)(A.d2 * A.d2)) e = (A.d2 / 2) * (A.d2 + 1);  // never read outside the window
-      const int a = e % A.d2, b = e / A.d2;
-      const size_t o = (size_t)(i * A.s + a) + (size_t)(j * A.s + b) * A.P;
-      for (int t = lane; t < DD; t += 32) {
-        const int rr = t % D, c = t / D;
-        b1[k * PG + t] = A.padP[o + rr + (size_t)c * A.P];
-        b2[k * PG + t] = A.padN[o + rr + (size_t)c * A.P];
+      mb = e / A.d2;
+      ma = e - mb * A.d2;
+    }
+    // the lane's elements t = lane + 32 u of a page: row t % D, column t / D
+    constexpr int NU = (DD + 31) / 32;
+    size_t toff[NU];
+#pragma unroll
+    for (int u = 0; u < NU; ++u) {
+      const int t = lane + 32 * u;
+      toff[u] = (size_t)(t % D) + (size_t)(t / D) * A.P;
+    }
+    const size_t ibase = (size_t)(i * A.s) + (size_t)(j * A.s) * A.P;
+    for (int k = 0; k < K; ++k) {
+      const int a = __shfl_sync(0xffffffffu, ma, k), b = __shfl_sync(0xffffffffu, mb, k);
+      const size_t o = ibase + a + (size_t)b * A.P;
+#pragma unroll
+      for (int u = 0; u < NU; ++u) {
+        const int t = lane + 32 * u;
+        if (t < DD) {
+          b1[k * PG + t] = __ldg(A.padP + o + toff[u]);
+          b2[k * PG + t] = __ldg(A.padN + o + toff[u]);
+        }
       }
     }
   } else {
