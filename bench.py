@@ -129,6 +129,16 @@ def padded_side(o) -> int:
     return p
 
 
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one ncu capture of each kernel on the 1024 x 1024 case of the dense workload,
+# where the step-1 grid has 340 x 340 references and the step-2 grid the same.  A launch's traffic grows with its
+# reference count, so it is scaled by the workload's count.  Wavelet kernels:
+# the level-0 launch (the one the bytes describe).
+TRAFFIC_1024 = {"match": 432.4e6, "wav_synthesis": 909.4e6, "wav_analysis": 909.1e6, "aggregate": 1065.1e6,
+                "wiener": 463.9e6, "ht_weights": 478.2e6}
+REFS_1024 = 340 * 340
+
+
 def roofline(o, ktimes, peaks, sm_mhz):
     """Algorithmic bytes (or flops) per step of each kernel family divided by
     its live CUDA-event time; the family with the largest time is the headline.
@@ -185,8 +195,11 @@ def roofline(o, ktimes, peaks, sm_mhz):
         return None, out
     top = max(out, key=lambda f: out[f]["ms_per_step"])
     r = out[top]
+    traffic = TRAFFIC_1024[top] * G1 / REFS_1024 if top in TRAFFIC_1024 else None
     roof = {"kernel": top, "bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"], "unit": r["unit"],
-            "frac": r["frac"], "traffic": None,
+            "frac": r["frac"], "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step-1 launch on the "
+                              "1024x1024 case, scaled by the reference count (bytes per launch)",
             "peak_source": {"hbm": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                             "tensor": "MEASURED_PEAKS.json bf16_tflops (of measured)",
                             "fp32": "derived: 148 SMs x 128 FP32 lanes x 2 flop x median SM clock under load"}[r["bound"]],
