@@ -67,8 +67,10 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
 
   // ---- stage the search window (column-major, stride WD) --------------------
   const float* src = A.pad + (size_t)i * A.s + (size_t)j * A.s * A.P;
-  for (int c = 0; c < WD; ++c)
-    for (int r = lane; r < WD; r += 32) win[r + c * WD] = src[r + (size_t)c * A.P];
+  for (int t = lane; t < WD * WD; t += 32) {  // flat over the window: every lane busy
+    const int c = t / WD, r = t - c * WD;
+    win[t] = src[r + (size_t)c * A.P];
+  }
   __syncwarp();
 
   // ---- exact SSD for the lane's candidates (a = lane, b = 0..D2-1) ----------
@@ -272,16 +274,24 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
 
   // ---- optional gathers: Volume (matchBlocksCPU.m:107-114), V1/V2 (matchBlocksWie.m:85-89)
   if (A.volume) {
+    // lane-parallel over the block: element t = lane + 32 u is row t % D, column t / D
     const size_t mn = (size_t)A.m * A.n;
+    float* vol0 = A.volume + (size_t)(i * D) + (size_t)A.m * (j * D);
     for (int k = 0; k < K; ++k) {
       int aa = H, bb = H;
       if (k < count) {
         const int e = (int)lS[k] - 1;
         if ((unsigned)e < (unsigned)(D2 * D2)) { aa = e % D2; bb = e / D2; }
       }
-      for (int c = 0; c < D; ++c)
-        for (int r = lane; r < D; r += 32)
-          A.volume[(size_t)(i * D + r) + (size_t)A.m * (j * D + c) + mn * k] = win[(aa + r) + (bb + c) * WD];
+      const float* wsrc = win + aa + bb * WD;
+#pragma unroll
+      for (int u = 0; u < (D * D + 31) / 32; ++u) {
+        const int t = lane + 32 * u;
+        if (t < D * D) {
+          const int r = t % D, c = t / D;
+          vol0[(size_t)r + (size_t)A.m * c + mn * k] = wsrc[r + c * WD];
+        }
+      }
     }
   }
   if (A.V1 || A.V2) {
