@@ -49,7 +49,7 @@ WORKLOADS = {
 WL = "dense"
 STAGES = ["glue", "match1", "wavelet1", "agg1", "match2", "wiener2", "agg2", "total"]
 # arithmetic of each form: plain FP32; precision: bf16 tensor-core distances (+ exact FP32 re-rank)
-FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32"}
+FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32", "tuned": "f32"}
 FAMILIES = ["match", "match_tc", "wav_analysis", "wav_synthesis", "aggregate", "wiener", "ht_weights", "make_pad",
             "accum", "ratio", "prep", "medfilt3"]
 
@@ -268,6 +268,14 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
+    def bcast(obj):
+        """rank 0's value of a small picklable object, on every rank"""
+        if world == 1:
+            return obj
+        box = [obj]
+        dist.broadcast_object_list(box, src=0)
+        return box[0]
+
     from gbm3d_b200 import _lib, api, build, synth
     build.build()
     ctx = _lib.Context(local)
@@ -328,9 +336,23 @@ def run_ours(args):
     have_pilot = os.path.exists(pilot.WEIGHTS)
     if have_pilot:
         pilot.load(ctx=ctx)
-    forms = (["plain", "precision"] + (["learned"] if have_pilot else [])) if args.form == "auto" \
+    forms = (["plain", "precision"] + (["learned"] if have_pilot else []) + ["tuned"]) if args.form == "auto" \
         else sorted({"plain", args.form})
-    res = {f: measure(dict(o_plain, form=f), True) for f in forms}
+    form_opts = {f: dict(o_plain, form=f) for f in forms if f != "tuned"}
+    tuning = None
+    if "tuned" in forms:
+        # the autotuner searches strides, spin schedule, cycle spins and search
+        # size on its own calibration image (another seed, at most 2048^2); the
+        # bench image only checks the result
+        from gbm3d_b200 import autotune
+        if args.tuned_opts:  # a known result (profiling runs): no search
+            form_opts["tuned"] = dict(o_plain, **{**autotune.BASELINE, **json.loads(args.tuned_opts)})
+        else:
+            if rank == 0:
+                tuning = autotune.tune(size=min(2048, SIZE), sigma=SIGMA, ctx=ctx, log=None)
+            tuning = bcast(tuning)  # every rank runs rank 0's choice
+            form_opts["tuned"] = dict(o_plain, **tuning["opts"])
+    res = {f: measure(form_opts[f], True) for f in forms}
     plain = res["plain"]
     if "learned" in res:
         # the learned form decides per image (on a 512^2 tile, host-orchestrated)
@@ -348,8 +370,9 @@ def run_ours(args):
     # the chosen form: the fastest one within 0.05 dB PSNR of the plain path
     ok = [f for f in forms if res[f]["psnr"] >= plain["psnr"] - 0.05]
     form = min(ok, key=lambda f: res[f]["ms"]) if args.form == "auto" else args.form
+    form = bcast(form)  # rank 0 decides, so every rank takes the same collective steps below
     chosen = res[form]
-    o = dict(o_plain, form=form)
+    o = form_opts[form]
     if form != forms[-1]:  # leave the chosen form's output in dU for the end-to-end check
         measure(o, False)
     ms, stages, ktimes, launches, clk = (chosen[k] for k in ("ms", "stages", "ktimes", "launches", "clk"))
@@ -389,7 +412,14 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": FORM_DTYPE[form], "data": "synthetic",
-            "config": _config({"form": form}),
+            "config": _config({"form": form, "form_opts": {k: o[k] for k in (
+                "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin", "form")}}),
+            "autotune": None if tuning is None else {
+                k: tuning[k] for k in ("opts", "size", "sigma", "seed", "budget_db", "margin_db", "evaluated",
+                                       "timed", "seconds")} | {
+                "calibration_psnr_db": tuning["chosen"]["psnr"], "calibration_baseline_psnr_db":
+                    tuning["baseline"]["psnr"], "calibration_ms": tuning["chosen"]["ms"],
+                "calibration_baseline_ms": tuning["baseline"]["ms"]},
             "forms": {f: {"value": world * mpix / (r["ms"] / 1e3), "unit": "MPix/s", "ms_per_step": r["ms"],
                           "psnr_db": r["psnr"], "stages_ms": dict(zip(STAGES, r["stages"])),
                           "gate": r.get("gate"),
@@ -434,6 +464,8 @@ def main():
     ap.add_argument("--form", default="auto", choices=["auto"] + sorted(FORM_DTYPE),
                     help="the form timed for `value` (auto: the fastest within 0.05 dB of plain); "
                          "the plain path is timed beside it")
+    ap.add_argument("--tuned-opts", default=None,
+                    help="JSON option overrides used as the tuned form instead of running the autotuner")
     args = ap.parse_args()
     SIZE, WL = args.size, args.workload
     if args.impl == "reference":

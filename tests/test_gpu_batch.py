@@ -68,3 +68,20 @@ def test_rgb_denoises_colour_noise(gpu):
     print(f"colour: noisy {options.myPSNR(clean, noisy, 255):.2f} dB, per-channel {p_sep:.2f} dB, "
           f"opponent + luma matching {p_rgb:.2f} dB")
     assert p_rgb > options.myPSNR(clean, noisy, 255) + 4 and p_rgb > p_sep - 0.5
+
+
+def test_autotune_choice_runs_within_budget(gpu):
+    """A small search: the chosen options denoise the calibration image within
+    budget - margin of the dense baseline and no slower than it, and they run
+    through the whole-image entry point."""
+    from gbm3d_b200 import api, autotune
+    cands = [dict(c, matchSize=32) for c in autotune.candidates(strides1=(8,), strides2=(4, 8), searches=(32,),
+                                                                 cycle_spins=(2,))]
+    t = autotune.tune(size=256, sigma=25.0, cands=cands, seed=11, log=None)
+    best, base = t["chosen"], t["baseline"]
+    assert best["ms"] <= base["ms"]
+    assert best.get("baseline") or best["psnr"] >= base["psnr"] - (t["budget_db"] - t["margin_db"])
+    assert t["evaluated"] == len(cands) + 1
+    clean, noisy = synth.noisy_image(256, 256, 25.0, seed=11)
+    U, _ = api.GBM3D(noisy, 25.0, t["opts"])
+    assert abs(options.myPSNR(clean, U, 255) - (best["psnr"])) < 1e-9

@@ -142,3 +142,35 @@ def test_no_device_fails_loudly():
     from gbm3d_b200 import _lib
     with pytest.raises(_lib.GBM3DError):
         _lib.Context(0)
+
+
+def test_autotune_search_space():
+    """Candidates keep patch, group and wavelet; strides never exceed the patch."""
+    from gbm3d_b200 import autotune
+    cs = autotune.candidates()
+    assert len(cs) == len({json_key(c) for c in cs})
+    for c in cs:
+        assert 1 <= c["refStride"] <= 8 and 1 <= c["refStrideWie"] <= 8
+        assert c["matchSpins"] in ([0], [0, 4]) and c["matchSpinsWie"][0] == 0
+        assert c["cycleSpin"] in (1, 2) and c["matchSize"] in (24, 32)
+        assert not ({"blockSize", "blockSizeWie", "numMax", "wname", "levels"} & set(c))
+    assert not autotune.candidates(strides1=(9,))
+
+
+def json_key(d):
+    import json
+    return json.dumps(d, sort_keys=True)
+
+
+def test_autotune_select_rule():
+    """The fastest row within budget - margin of the baseline wins; untimed rows never do."""
+    from gbm3d_b200 import autotune
+    rows = [{"baseline": True, "opts": {}, "psnr": 30.0, "ms": 100.0},
+            {"opts": {"refStride": 8}, "psnr": 29.90, "ms": 10.0},   # 0.10 dB worse: out
+            {"opts": {"refStride": 6}, "psnr": 29.975, "ms": 20.0},  # 0.025 dB worse: in at margin 0.02
+            {"opts": {"refStride": 4}, "psnr": 30.2, "ms": 40.0},
+            {"opts": {"refStride": 5}, "psnr": 29.0}]                # not timed
+    assert autotune.select(rows, 0.05, 0.02)["opts"] == {"refStride": 6}
+    assert autotune.select(rows, 0.05, 0.04)["opts"] == {"refStride": 4}
+    assert autotune.select(rows, 0.2, 0.0)["opts"] == {"refStride": 8}
+    assert autotune.select(rows[:1], 0.05)["baseline"]
