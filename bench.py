@@ -137,6 +137,12 @@ def padded_side(o) -> int:
 TRAFFIC_1024 = {"match": 432.4e6, "wav_synthesis": 909.4e6, "wav_analysis": 909.1e6, "aggregate": 1065.1e6,
                 "wiener": 463.9e6, "ht_weights": 478.2e6}
 REFS_1024 = 340 * 340
+# The same (bytes per launch, averaged over the family's launches of one call)
+# for the tuned option set below, captured on a 2048 x 2048 image (padded side
+# 2048); a launch's traffic grows with the padded image area.
+TUNED_KEY = (8, 6, (0,), (0,), 1, 32)  # refStride, refStrideWie, matchSpins, matchSpinsWie, cycleSpin, matchSize
+TRAFFIC_TUNED_2048 = {"match": 125.1e6, "wav_analysis": 177.0e6, "wav_synthesis": 177.6e6, "ht_weights": 269.2e6,
+                      "aggregate": 419.8e6, "wiener": 488.1e6}
 
 
 def roofline(o, ktimes, peaks, sm_mhz):
@@ -195,11 +201,18 @@ def roofline(o, ktimes, peaks, sm_mhz):
         return None, out
     top = max(out, key=lambda f: out[f]["ms_per_step"])
     r = out[top]
-    traffic = TRAFFIC_1024[top] * G1 / REFS_1024 if top in TRAFFIC_1024 else None
+    key = (s1, s2, tuple(o["matchSpins"]), tuple(o["matchSpinsWie"]), cs, d2)
+    if key == TUNED_KEY:
+        traffic = TRAFFIC_TUNED_2048.get(top)
+        traffic = None if traffic is None else traffic * (Mp / 2048) ** 2
+        tsrc = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this option set on a 2048x2048 image, "
+                "averaged over the family's launches of one call and scaled by the padded area (bytes per launch)")
+    else:
+        traffic = TRAFFIC_1024[top] * G1 / REFS_1024 if top in TRAFFIC_1024 else None
+        tsrc = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one step-1 launch of the dense workload on "
+                "the 1024x1024 case, scaled by the reference count (bytes per launch)")
     roof = {"kernel": top, "bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"], "unit": r["unit"],
-            "frac": r["frac"], "traffic": traffic,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step-1 launch on the "
-                              "1024x1024 case, scaled by the reference count (bytes per launch)",
+            "frac": r["frac"], "traffic": traffic, "traffic_source": tsrc,
             "peak_source": {"hbm": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                             "tensor": "MEASURED_PEAKS.json bf16_tflops (of measured)",
                             "fp32": "derived: 148 SMs x 128 FP32 lanes x 2 flop x median SM clock under load"}[r["bound"]],
