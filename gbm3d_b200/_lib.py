@@ -48,6 +48,17 @@ class gbm3d_filters(C.Structure):
     ]
 
 
+class gbm3d_mixed_batch(C.Structure):
+    _fields_ = [
+        ("n_grey", C.c_int), ("grey", C.c_void_p), ("grey_m", C.c_void_p), ("grey_n", C.c_void_p),
+        ("grey_sigma", C.c_void_p), ("grey_out", C.c_void_p),
+        ("n_rgb", C.c_int), ("rgb", C.c_void_p), ("rgb_m", C.c_void_p), ("rgb_n", C.c_void_p),
+        ("rgb_sigma", C.c_void_p), ("rgb_out", C.c_void_p),
+        ("video", C.c_void_p), ("video_m", C.c_int), ("video_n", C.c_int), ("video_frames", C.c_int),
+        ("video_sigma", C.c_double), ("video_out", C.c_void_p),
+    ]
+
+
 _P = C.c_void_p
 _SIGS = {
     "gbm3d_version": (C.c_int, []),
@@ -83,6 +94,8 @@ _SIGS = {
     "gbm3d_denoiseAndAggregateV": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, C.POINTER(gbm3d_filters),
                                              C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise_batch": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, C.POINTER(gbm3d_opts), _P, C.c_int]),
+    "gbm3d_denoise_mixed": (C.c_int, [_P, C.POINTER(gbm3d_mixed_batch), C.POINTER(gbm3d_opts),
+                                      C.POINTER(gbm3d_opts), C.c_int]),
     "gbm3d_pilot_param_count": (C.c_int, []),
     "gbm3d_pilot_set_params": (C.c_int, [_P, _P]),
     "gbm3d_pilot_get_params": (C.c_int, [_P, _P]),

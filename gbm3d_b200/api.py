@@ -31,7 +31,7 @@ import ctypes as C
 import numpy as np
 
 from . import options as _opt
-from ._lib import Context, GBM3DError, context, gbm3d_filters, gbm3d_opts, lib
+from ._lib import Context, GBM3DError, context, gbm3d_filters, gbm3d_mixed_batch, gbm3d_opts, lib
 
 
 class MatchSet(np.ndarray):
@@ -316,6 +316,62 @@ def GBM3D_rgb(I, sigma, opts: dict | None = None, ctx: Context | None = None):
                                              C.byref(co), *[C.c_void_p(u.data_ptr()) for u in outs]))
     ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
     return np.stack([u.cpu().numpy().reshape(m, n, order="F") for u in outs], axis=2)
+
+
+def GBM3D_mixed(grey=(), grey_sigma=(), rgb=(), rgb_sigma=(), video=None, video_sigma: float = 0.0,
+                opts: dict | None = None, vopts: dict | None = None, use_graph: bool = True,
+                ctx: Context | None = None, outputs=None):
+    """Batched form over a mixed submission (gbm3d_denoise_mixed): grey
+    device images (torch float64 (n, m) tensors, i.e. column-major m x n),
+    colour images as (R, G, B) triples of such tensors, and one video (a
+    torch float64 (frames, n, m) tensor on the [0, 1] scale), denoised in one
+    call; with use_graph the whole launch sequence is captured into one CUDA
+    graph on the first call and replayed by later calls with the same
+    geometry.  Grey and colour images use ``opts``, the video ``vopts``
+    (VBM3D.m's defaults).  Returns (grey outputs, colour output triples, video
+    output (frames - nF + 1, n, m) or None) once the work has finished."""
+    import torch
+    ctx = ctx or context()
+    o = c_opts(_opt.resolve_opts(opts))
+    cv = c_video_opts(vopts) if video is not None else None
+    grey, rgb = list(grey), [tuple(t) for t in rgb]
+    if outputs is None:
+        outputs = ([torch.empty_like(x) for x in grey], [tuple(torch.empty_like(p) for p in t) for t in rgb],
+                   None if video is None else torch.empty((video.shape[0] - cv.videoFrames + 1,) + tuple(video.shape[1:]),
+                                                          dtype=torch.float64, device=video.device))
+    g_out, c_out, v_out = outputs
+    b = gbm3d_mixed_batch()
+    keep = []
+
+    def arr(ctype, vals):
+        a = (ctype * max(len(vals), 1))(*vals)
+        keep.append(a)
+        return C.cast(a, C.c_void_p)
+
+    b.n_grey = len(grey)
+    b.grey = arr(C.c_void_p, [x.data_ptr() for x in grey])
+    b.grey_m = arr(C.c_int, [int(x.shape[1]) for x in grey])
+    b.grey_n = arr(C.c_int, [int(x.shape[0]) for x in grey])
+    b.grey_sigma = arr(C.c_double, [float(v) for v in grey_sigma])
+    b.grey_out = arr(C.c_void_p, [u.data_ptr() for u in g_out])
+    b.n_rgb = len(rgb)
+    b.rgb = arr(C.c_void_p, [p.data_ptr() for t in rgb for p in t])
+    b.rgb_m = arr(C.c_int, [int(t[0].shape[1]) for t in rgb])
+    b.rgb_n = arr(C.c_int, [int(t[0].shape[0]) for t in rgb])
+    b.rgb_sigma = arr(C.c_double, [float(v) for v in rgb_sigma])
+    b.rgb_out = arr(C.c_void_p, [p.data_ptr() for t in c_out for p in t])
+    if video is not None:
+        b.video = video.data_ptr()
+        b.video_frames, b.video_n, b.video_m = (int(x) for x in video.shape)
+        b.video_sigma = float(video_sigma)
+        b.video_out = v_out.data_ptr()
+    if len(grey_sigma) != len(grey) or len(rgb_sigma) != len(rgb):
+        raise GBM3DError(1, "one sigma per image")
+    torch.cuda.synchronize()
+    ctx.check(lib().gbm3d_denoise_mixed(ctx.h, C.byref(b), C.byref(o), C.byref(cv) if cv is not None else None,
+                                        1 if use_graph else 0))
+    ctx.check(lib().gbm3d_ctx_synchronize(ctx.h))
+    return outputs
 
 
 # ---- video ------------------------------------------------------------------------

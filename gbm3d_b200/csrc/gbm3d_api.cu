@@ -1654,6 +1654,58 @@ int gbm3d_denoise_rgb_device(gbm3d_ctx* c, const double* R, const double* G, con
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// Runs run_all() eagerly, or, with use_graph, replays the context's captured
+// graph when its key matches; otherwise runs it eagerly (which sizes every
+// workspace buffer and produces this call's result) and then captures the
+// same launch sequence once for later calls with this key.
+template <class F>
+void run_graph(gbm3d_ctx* c, const std::string& key, bool use_graph, F&& run_all) {
+  if (!use_graph) {
+    run_all();
+    return;
+  }
+  if (c->graph_exec && c->graph_key == key) {  // same geometry: replay
+    ck(c, cudaGraphLaunch(c->graph_exec, c->st), "cudaGraphLaunch");
+    c->launches = 1;
+    return;
+  }
+  run_all();
+  const bool tm = c->timing;
+  c->timing = false;
+  ck(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+  cudaGraph_t g = nullptr;
+  try {
+    run_all();
+  } catch (...) {
+    cudaStreamEndCapture(c->st, &g);
+    if (g) cudaGraphDestroy(g);
+    c->timing = tm;
+    throw;
+  }
+  c->timing = tm;
+  ck(c, cudaStreamEndCapture(c->st, &g), "cudaStreamEndCapture");
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  c->graph_exec = nullptr;
+  c->graph_key.clear();
+  const cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+  cudaGraphDestroy(g);
+  ck(c, e, "cudaGraphInstantiate");
+  c->graph_key = key;
+}
+
+template <class T>
+void key_add(std::string& key, const T& v) {
+  key.append(reinterpret_cast<const char*>(&v), sizeof(T));
+}
+
+}  // namespace
+
+extern "C" {
+
 int gbm3d_denoise_batch(gbm3d_ctx* c, int nimg, const double* const* I, const int* m, const int* n,
                         const double* sigma, const gbm3d_opts* o, double* const* U, int use_graph) {
   return guarded(c, [&] {
@@ -1664,49 +1716,78 @@ int gbm3d_denoise_batch(gbm3d_ctx* c, int nimg, const double* const* I, const in
     std::vector<int> ord(nimg);
     for (int k = 0; k < nimg; ++k) ord[k] = k;
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return (long)m[a] * n[a] > (long)m[b] * n[b]; });
-    auto run_all = [&] {
-      for (int k : ord) pipeline(c, I[k], m[k], n[k], sigma[k], o, U[k], nullptr);
-    };
-    if (!use_graph) {
-      run_all();
-      return;
-    }
-    std::string key(reinterpret_cast<const char*>(o), sizeof(*o));
+    std::string key("batch");
+    key_add(key, *o);
     for (int k = 0; k < nimg; ++k) {
-      const void* p[2] = {I[k], U[k]};
-      key.append(reinterpret_cast<const char*>(p), sizeof(p));
-      key.append(reinterpret_cast<const char*>(&m[k]), sizeof(int));
-      key.append(reinterpret_cast<const char*>(&n[k]), sizeof(int));
-      key.append(reinterpret_cast<const char*>(&sigma[k]), sizeof(double));
+      key_add(key, I[k]);
+      key_add(key, U[k]);
+      key_add(key, m[k]);
+      key_add(key, n[k]);
+      key_add(key, sigma[k]);
     }
-    if (c->graph_exec && c->graph_key == key) {  // same batch geometry: replay
-      ck(c, cudaGraphLaunch(c->graph_exec, c->st), "cudaGraphLaunch");
-      c->launches = 1;
-      return;
+    run_graph(c, key, use_graph != 0, [&] {
+      for (int k : ord) pipeline(c, I[k], m[k], n[k], sigma[k], o, U[k], nullptr);
+    });
+  });
+}
+
+int gbm3d_denoise_mixed(gbm3d_ctx* c, const gbm3d_mixed_batch* b, const gbm3d_opts* o,
+                        const gbm3d_opts* ov, int use_graph) {
+  return guarded(c, [&] {
+    if (!b || !o) argfail(c, "missing argument");
+    if (b->n_grey < 0 || b->n_rgb < 0) argfail(c, "negative image count");
+    if (b->n_grey > 0 && (!b->grey || !b->grey_m || !b->grey_n || !b->grey_sigma || !b->grey_out))
+      argfail(c, "missing grey-image arrays");
+    if (b->n_rgb > 0 && (!b->rgb || !b->rgb_m || !b->rgb_n || !b->rgb_sigma || !b->rgb_out))
+      argfail(c, "missing colour-image arrays");
+    if (b->video && (!ov || !b->video_out)) argfail(c, "video without options or output");
+    for (int k = 0; k < b->n_grey; ++k)
+      if (!b->grey[k] || !b->grey_out[k]) argfail(c, "missing grey image or output pointer");
+    for (int k = 0; k < 3 * b->n_rgb; ++k)
+      if (!b->rgb[k] || !b->rgb_out[k]) argfail(c, "missing colour plane or output pointer");
+    if (b->n_grey == 0 && b->n_rgb == 0 && !b->video) argfail(c, "empty batch");
+    std::vector<int> og(b->n_grey), orgb(b->n_rgb);
+    for (int k = 0; k < b->n_grey; ++k) og[k] = k;
+    for (int k = 0; k < b->n_rgb; ++k) orgb[k] = k;
+    auto larger = [](const int* mm, const int* nn) {
+      return [mm, nn](int x, int y) { return (long)mm[x] * nn[x] > (long)mm[y] * nn[y]; };
+    };
+    std::stable_sort(og.begin(), og.end(), larger(b->grey_m, b->grey_n));
+    std::stable_sort(orgb.begin(), orgb.end(), larger(b->rgb_m, b->rgb_n));
+    std::string key("mixed");
+    key_add(key, *o);
+    if (b->video) key_add(key, *ov);
+    for (int k = 0; k < b->n_grey; ++k) {
+      key_add(key, b->grey[k]);
+      key_add(key, b->grey_out[k]);
+      key_add(key, b->grey_m[k]);
+      key_add(key, b->grey_n[k]);
+      key_add(key, b->grey_sigma[k]);
     }
-    // eager run (sizes every workspace buffer and produces this call's result),
-    // then the same launch sequence captured once for later calls
-    run_all();
-    const bool tm = c->timing;
-    c->timing = false;
-    ck(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
-    cudaGraph_t g = nullptr;
-    try {
-      run_all();
-    } catch (...) {
-      cudaStreamEndCapture(c->st, &g);
-      if (g) cudaGraphDestroy(g);
-      c->timing = tm;
-      throw;
+    for (int k = 0; k < b->n_rgb; ++k) {
+      for (int q = 0; q < 3; ++q) {
+        key_add(key, b->rgb[3 * k + q]);
+        key_add(key, b->rgb_out[3 * k + q]);
+      }
+      key_add(key, b->rgb_m[k]);
+      key_add(key, b->rgb_n[k]);
+      key_add(key, b->rgb_sigma[k]);
     }
-    c->timing = tm;
-    ck(c, cudaStreamEndCapture(c->st, &g), "cudaStreamEndCapture");
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
-    const cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
-    cudaGraphDestroy(g);
-    ck(c, e, "cudaGraphInstantiate");
-    c->graph_key = key;
+    key_add(key, b->video);
+    if (b->video) {
+      key_add(key, b->video_out);
+      key_add(key, b->video_m);
+      key_add(key, b->video_n);
+      key_add(key, b->video_frames);
+      key_add(key, b->video_sigma);
+    }
+    run_graph(c, key, use_graph != 0, [&] {
+      for (int k : og) pipeline(c, b->grey[k], b->grey_m[k], b->grey_n[k], b->grey_sigma[k], o, b->grey_out[k], nullptr);
+      for (int k : orgb)
+        pipeline_rgb(c, b->rgb + 3 * k, b->rgb_m[k], b->rgb_n[k], b->rgb_sigma[k], o, b->rgb_out + 3 * k);
+      if (b->video)
+        pipeline_video(c, b->video, b->video_m, b->video_n, b->video_frames, b->video_sigma, ov, b->video_out);
+    });
   });
 }
 

@@ -24,9 +24,17 @@ def clean_image(m: int, n: int, seed: int = 0, n_ellipses: int = 40, n_textures:
         th = rng.uniform(0, np.pi)
         val = rng.uniform(0, 255)
         c, s = np.cos(th), np.sin(th)
-        u = ((yy - cy) * c + (xx - cx) * s) / ry
-        v = (-(yy - cy) * s + (xx - cx) * c) / rx
-        img[u * u + v * v <= 1.0] = val
+        # only the ellipse's bounding box (2 px of margin) is tested: the same
+        # elementwise arithmetic as over the whole grid, on fewer pixels
+        ey, ex = np.hypot(ry * c, rx * s), np.hypot(ry * s, rx * c)
+        r0, r1 = max(int(np.floor(cy - ey)) - 2, 0), min(int(np.ceil(cy + ey)) + 3, m)
+        c0, c1 = max(int(np.floor(cx - ex)) - 2, 0), min(int(np.ceil(cx + ex)) + 3, n)
+        if r0 >= r1 or c0 >= c1:
+            continue
+        by, bx = yy[r0:r1, c0:c1], xx[r0:r1, c0:c1]
+        u = ((by - cy) * c + (bx - cx) * s) / ry
+        v = (-(by - cy) * s + (bx - cx) * c) / rx
+        img[r0:r1, c0:c1][u * u + v * v <= 1.0] = val
     for _ in range(n_textures):
         h = int(rng.uniform(0.1, 0.3) * m) + 1
         w = int(rng.uniform(0.1, 0.3) * n) + 1
@@ -80,9 +88,17 @@ def video(m: int, n: int, frames: int, sigma: float, seed: int = 0, n_ellipses: 
         img = g0 + gy * yy / max(m - 1, 1) + gx * xx / max(n - 1, 1)
         for cy, cx, ry, rx, th, val, vy, vx in ell:
             c, s = np.cos(th), np.sin(th)
-            u = ((yy - cy - vy * f) * c + (xx - cx - vx * f) * s) / ry
-            v = (-(yy - cy - vy * f) * s + (xx - cx - vx * f) * c) / rx
-            img[u * u + v * v <= 1.0] = val
+            # bounding box of the moved ellipse, 2 px of margin (see clean_image)
+            ey, ex = np.hypot(ry * c, rx * s), np.hypot(ry * s, rx * c)
+            ccy, ccx = cy + vy * f, cx + vx * f
+            r0, r1 = max(int(np.floor(ccy - ey)) - 2, 0), min(int(np.ceil(ccy + ey)) + 3, m)
+            c0, c1 = max(int(np.floor(ccx - ex)) - 2, 0), min(int(np.ceil(ccx + ex)) + 3, n)
+            if r0 >= r1 or c0 >= c1:
+                continue
+            by, bx = yy[r0:r1, c0:c1], xx[r0:r1, c0:c1]
+            u = ((by - cy - vy * f) * c + (bx - cx - vx * f) * s) / ry
+            v = (-(by - cy - vy * f) * s + (bx - cx - vx * f) * c) / rx
+            img[r0:r1, c0:c1][u * u + v * v <= 1.0] = val
         clean[:, :, f] = img
     noise = np.random.Generator(np.random.PCG64(seed + 3_000_017)).standard_normal((m, n, frames))
     return np.asfortranarray(clean), np.asfortranarray(clean + sigma * noise)

@@ -232,6 +232,39 @@ int gbm3d_vbm3d_device(gbm3d_ctx* ctx, const double* I, int m, int n, int frames
 int gbm3d_denoise_batch(gbm3d_ctx* ctx, int nimg, const double* const* I, const int* m, const int* n,
                         const double* sigma, const gbm3d_opts* opts, double* const* U, int use_graph);
 
+/* Mixed batch: grey images, colour images and one video in one submission
+ * (device pointers, float64 column-major).  Grey images run the whole-image
+ * pipeline of gbm3d_denoise_device with opts at their own sigma, colour images
+ * the opponent-space pipeline of gbm3d_denoise_rgb_device with opts, and the
+ * video the VBM3D pipeline of gbm3d_vbm3d_device with video_opts (frames on
+ * the [0,1] scale).  Any part may be empty (count 0, video null).  With
+ * use_graph the first call runs everything and captures the whole launch
+ * sequence into one CUDA graph; a later call with the same pointers, sizes,
+ * sigmas and options replays it with a single graph launch (this replaces the
+ * graph of gbm3d_denoise_batch, and the reverse).  Every output equals the
+ * single-image entry's.  Asynchronous on the context stream.  Not in the
+ * reference. */
+typedef struct gbm3d_mixed_batch {
+  int n_grey;
+  const double* const* grey;      /* n_grey images */
+  const int* grey_m;
+  const int* grey_n;
+  const double* grey_sigma;
+  double* const* grey_out;
+  int n_rgb;
+  const double* const* rgb;       /* 3 n_rgb planes: R, G, B of image 0, then of image 1, ... */
+  const int* rgb_m;
+  const int* rgb_n;
+  const double* rgb_sigma;
+  double* const* rgb_out;         /* 3 n_rgb output planes, in the same order */
+  const double* video;            /* video_m x video_n x video_frames, or null */
+  int video_m, video_n, video_frames;
+  double video_sigma;
+  double* video_out;              /* video_m x video_n x (video_frames - videoFrames + 1) */
+} gbm3d_mixed_batch;
+int gbm3d_denoise_mixed(gbm3d_ctx* ctx, const gbm3d_mixed_batch* batch, const gbm3d_opts* opts,
+                        const gbm3d_opts* video_opts, int use_graph);
+
 /* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
  * the context stream (synchronise before reading U). */
 int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,

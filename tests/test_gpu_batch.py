@@ -85,3 +85,51 @@ def test_autotune_choice_runs_within_budget(gpu):
     clean, noisy = synth.noisy_image(256, 256, 25.0, seed=11)
     U, _ = api.GBM3D(noisy, 25.0, t["opts"])
     assert abs(options.myPSNR(clean, U, 255) - (best["psnr"])) < 1e-9
+
+
+def test_mixed_batch_matches_single_entries(gpu):
+    """Grey images, colour images and a video in one submission: eager, then
+    captured, then replayed twice; every output equals its own single-image
+    entry's bit for bit."""
+    import torch
+    from gbm3d_b200 import api
+    o = _dense()
+    dev = torch.device("cuda", 0)
+
+    def col(a):
+        return torch.from_numpy(np.asfortranarray(a).ravel(order="F").copy()).to(dev)
+
+    grey_sizes, grey_sig = [(96, 80), (64, 72), (120, 96)], [10.0, 30.0, 45.0]
+    grey = [col(synth.noisy_image(m, n, s, seed=80 + k)[1]).view(n, m)
+            for k, ((m, n), s) in enumerate(zip(grey_sizes, grey_sig))]
+    grey_ref = [api.GBM3D(synth.noisy_image(m, n, s, seed=80 + k)[1], s, o)[0]
+                for k, ((m, n), s) in enumerate(zip(grey_sizes, grey_sig))]
+    rgb_sizes, rgb_sig = [(80, 64), (64, 96)], [20.0, 35.0]
+    rgb, rgb_ref = [], []
+    for k, ((m, n), s) in enumerate(zip(rgb_sizes, rgb_sig)):
+        planes = np.stack([synth.noisy_image(m, n, s, seed=90 + 3 * k + q)[1] for q in range(3)], axis=2)
+        rgb.append(tuple(col(planes[:, :, q]).view(n, m) for q in range(3)))
+        rgb_ref.append(api.GBM3D_rgb(planes, s, o))
+    vm, vn, vf, vs = 48, 40, 5, 25.0
+    _, frames = synth.video(vm, vn, vf, vs, seed=7)
+    frames = frames / 255.0
+    vo = {"blockSize": 8, "nF": 3}
+    video = col(frames).view(vf, vn, vm)
+    video_ref = api.VBM3D(frames, vs / 255.0, vo)[0]
+    for use_graph, calls in ((False, 1), (True, 3)):
+        for _ in range(calls):
+            g_out, c_out, v_out = api.GBM3D_mixed(grey, grey_sig, rgb, rgb_sig, video, vs / 255.0, o, vo,
+                                                  use_graph=use_graph)
+            for k, (m, n) in enumerate(grey_sizes):
+                got = g_out[k].cpu().numpy().reshape(-1).reshape(m, n, order="F")
+                assert np.array_equal(got, grey_ref[k]), f"grey image {k} (graph={use_graph})"
+            for k, (m, n) in enumerate(rgb_sizes):
+                for q in range(3):
+                    got = c_out[k][q].cpu().numpy().reshape(-1).reshape(m, n, order="F")
+                    assert np.array_equal(got, rgb_ref[k][:, :, q]), f"colour image {k} plane {q} (graph={use_graph})"
+            got = v_out.cpu().numpy().reshape(-1).reshape(video_ref.shape, order="F")
+            assert np.array_equal(got, video_ref), f"video (graph={use_graph})"
+    # a different geometry is captured anew
+    g_out, _, _ = api.GBM3D_mixed(grey[:1], grey_sig[:1], opts=o)
+    m, n = grey_sizes[0]
+    assert np.array_equal(g_out[0].cpu().numpy().reshape(-1).reshape(m, n, order="F"), grey_ref[0])
