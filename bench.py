@@ -221,18 +221,46 @@ def roofline(o, ktimes, peaks, sm_mhz):
     return roof, out
 
 
-def cpu_baseline(size: int = 512):
-    """The oracle (FP32 restatement of the reference path) on a bounded crop, all host threads."""
-    from gbm3d_b200 import synth
+def cpu_baseline(o_chosen=None, size: int = 512):
+    """The oracle (the CPU restatement of the reference path) timed on a
+    bounded crop with all host threads, in FP32 (the kernels' operation
+    order) and in FP64.  As the checker, the same crop denoised on the GPU is
+    then compared with the oracle's outputs, for the plain configuration and
+    for the chosen form's options, and the precision form's step-1 match sets
+    with the plain matcher's.  Returns (cpu_baseline, parity)."""
+    from gbm3d_b200 import api, synth
+    from gbm3d_b200 import options as _opt
     from oracle import oracle as O
     O.lib()
-    _, noisy = synth.noisy_image(size, size, SIGMA, seed=2024)
+    clean, noisy = synth.noisy_image(size, size, SIGMA, seed=2024)
     t0 = time.perf_counter()
-    O.GBM3D(noisy, SIGMA, opts(), prec=32)
+    U32, _ = O.GBM3D(noisy, SIGMA, opts(), prec=32)
     dt = time.perf_counter() - t0
-    return {"value": size * size / 1e6 / dt, "unit": "MPix/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"one {size}x{size} crop of the same synthetic workload, FP32 oracle, OpenMP",
-            "seconds": dt}
+    t0 = time.perf_counter()
+    U64, _ = O.GBM3D(noisy, SIGMA, opts(), prec=64)
+    dt64 = time.perf_counter() - t0
+    base = {"value": size * size / 1e6 / dt, "unit": "MPix/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"one {size}x{size} image of the same synthetic workload (seed 2024), FP32 oracle, OpenMP",
+            "seconds": dt, "fp64": {"value": size * size / 1e6 / dt64, "unit": "MPix/s", "seconds": dt64}}
+
+    def compare(Ug, U32, U64):
+        return {"bit_identical_to_fp32_oracle": bool(np.array_equal(Ug, U32)),
+                "max_abs_vs_fp32_oracle": float(np.max(np.abs(Ug - U32))),
+                "max_abs_vs_fp64_oracle": float(np.max(np.abs(Ug - U64))),
+                "psnr_gpu_db": float(_opt.myPSNR(clean, Ug, 255)), "psnr_fp64_oracle_db": float(_opt.myPSNR(clean, U64, 255))}
+
+    parity = {"sample": f"{size}x{size}, sigma {SIGMA:g}, seed 2024; the GPU through gbm3d_denoise, the oracle "
+                        "as the checker", "plain": compare(api.GBM3D(noisy, SIGMA, opts())[0], U32, U64)}
+    if o_chosen is not None and o_chosen.get("form", "plain") == "plain" and \
+            {k: v for k, v in o_chosen.items() if k != "form"} != opts():
+        Uc32, _ = O.GBM3D(noisy, SIGMA, o_chosen, prec=32)
+        Uc64, _ = O.GBM3D(noisy, SIGMA, o_chosen, prec=64)
+        parity["chosen"] = compare(api.GBM3D(noisy, SIGMA, o_chosen)[0], Uc32, Uc64)
+    Sp, _ = api.matchBlocksCPU(noisy, SIGMA, opts())
+    Sq, _ = api.matchBlocksCPU(noisy, SIGMA, dict(opts(), form="precision"))
+    Sp, Sq = np.asarray(Sp), np.asarray(Sq)
+    parity["precision_step1_match_sets_identical"] = float(np.mean(np.all(Sp == Sq, axis=0)))
+    return base, parity
 
 
 def run_reference(args):
@@ -454,7 +482,7 @@ def run_ours(args):
             "roofline": roof,
             "roofline_all": work}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_size)
+        line["cpu_baseline"], line["parity"] = cpu_baseline(o, args.cpu_size)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
