@@ -71,18 +71,63 @@ def _config(extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 5 ms from a thread (a timed region of ~0.1 s
+    still gets ~20 samples), or nvidia-smi at 200 ms when NVML is missing.
+    Reads only; no setting of the GPU is changed."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.rows = []
         self.proc = None
+        self.nv = None
+        self.stop_flag = threading.Event()
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = self._handle(nv, index)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            self.bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        except Exception:  # no NVML: nvidia-smi below
+            self.nv = None
+
+    @staticmethod
+    def _handle(nv, index):
+        """The NVML device of CUDA device `index` (matched by PCI location when torch reports it)."""
+        import torch
+        p = torch.cuda.get_device_properties(index)
+        bus, dev, dom = (getattr(p, k, None) for k in ("pci_bus_id", "pci_device_id", "pci_domain_id"))
+        if bus is not None:
+            for i in range(nv.nvmlDeviceGetCount()):
+                h = nv.nvmlDeviceGetHandleByIndex(i)
+                pci = nv.nvmlDeviceGetPciInfo(h)
+                if pci.bus == bus and pci.device == dev and (dom is None or pci.domain == dom):
+                    return h
+        return nv.nvmlDeviceGetHandleByIndex(index)
+
+    def _poll(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                why = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.rows.append((mhz, why))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.005)
 
     def start(self):
+        if self.nv is not None:
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -97,6 +142,13 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self) -> dict:
+        if self.nv is not None:
+            self.stop_flag.set()
+            self.t.join(timeout=2)
+            sm = [r[0] for r in self.rows]
+            reasons = sorted({self.NAMES[i] for _, why in self.rows for i, b in enumerate(self.bits) if why & b})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "source": "NVML, 5 ms polling"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -106,11 +158,10 @@ class ClockSampler:
             self.proc.kill()
         sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4)
+        reasons = sorted({self.NAMES[i] for r in self.rows if len(r) >= 9 for i in range(4)
                           if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(sm)}
+                "reasons": reasons, "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def padded_side(o) -> int:
@@ -138,11 +189,15 @@ TRAFFIC_1024 = {"match": 432.4e6, "wav_synthesis": 909.4e6, "wav_analysis": 909.
                 "wiener": 463.9e6, "ht_weights": 478.2e6}
 REFS_1024 = 340 * 340
 # The same (bytes per launch, averaged over the family's launches of one call)
-# for the tuned option set below, captured on a 2048 x 2048 image (padded side
-# 2048); a launch's traffic grows with the padded image area.
-TUNED_KEY = (8, 6, (0,), (0,), 1, 32)  # refStride, refStrideWie, matchSpins, matchSpinsWie, cycleSpin, matchSize
-TRAFFIC_TUNED_2048 = {"match": 125.1e6, "wav_analysis": 177.0e6, "wav_synthesis": 177.6e6, "ht_weights": 269.2e6,
-                      "aggregate": 419.8e6, "wiener": 488.1e6}
+# for the option sets the autotuner picks, each captured on a 2048 x 2048 image
+# (padded side given); a launch's traffic grows with the padded image area.
+# Key: refStride, refStrideWie, matchSpins, matchSpinsWie, cycleSpin, matchSize.
+TRAFFIC_TUNED_2048 = {
+    (8, 6, (0,), (0,), 1, 32): (2048, {"match": 125.1e6, "wav_analysis": 177.0e6, "wav_synthesis": 177.6e6,
+                                       "ht_weights": 269.2e6, "aggregate": 419.8e6, "wiener": 488.1e6}),
+    (8, 7, (0,), (0,), 1, 32): (2080, {"match": 129.9e6, "wav_analysis": 183.5e6, "wav_synthesis": 183.3e6,
+                                       "ht_weights": 277.5e6, "aggregate": 363.0e6, "wiener": 365.1e6}),
+}
 
 
 def roofline(o, ktimes, peaks, sm_mhz):
@@ -202,9 +257,10 @@ def roofline(o, ktimes, peaks, sm_mhz):
     top = max(out, key=lambda f: out[f]["ms_per_step"])
     r = out[top]
     key = (s1, s2, tuple(o["matchSpins"]), tuple(o["matchSpinsWie"]), cs, d2)
-    if key == TUNED_KEY:
-        traffic = TRAFFIC_TUNED_2048.get(top)
-        traffic = None if traffic is None else traffic * (Mp / 2048) ** 2
+    if key in TRAFFIC_TUNED_2048:
+        side, table = TRAFFIC_TUNED_2048[key]
+        traffic = table.get(top)
+        traffic = None if traffic is None else traffic * (Mp / side) ** 2
         tsrc = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this option set on a 2048x2048 image, "
                 "averaged over the family's launches of one call and scaled by the padded area (bytes per launch)")
     else:
@@ -383,14 +439,14 @@ def run_ours(args):
     tuning = None
     if "tuned" in forms:
         # the autotuner searches strides, spin schedule, cycle spins and search
-        # size on its own calibration image (another seed, at most 2048^2); the
+        # size on its own calibration image (same size, another seed); the
         # bench image only checks the result
         from gbm3d_b200 import autotune
         if args.tuned_opts:  # a known result (profiling runs): no search
             form_opts["tuned"] = dict(o_plain, **{**autotune.BASELINE, **json.loads(args.tuned_opts)})
         else:
             if rank == 0:
-                tuning = autotune.tune(size=min(2048, SIZE), sigma=SIGMA, ctx=ctx, log=None)
+                tuning = autotune.tune(size=SIZE, sigma=SIGMA, ctx=ctx, log=None)
             tuning = bcast(tuning)  # every rank runs rank 0's choice
             form_opts["tuned"] = dict(o_plain, **tuning["opts"])
     res = {f: measure(form_opts[f], True) for f in forms}

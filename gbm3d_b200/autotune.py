@@ -73,6 +73,7 @@ class _Runner:
         self.clean, noisy = synth.noisy_image(size, size, sigma, seed=seed)
         dev = torch.device("cuda", ctx.device)
         self.dI = torch.from_numpy(np.asfortranarray(noisy).ravel(order="F").copy()).to(dev)
+        self.dC = torch.from_numpy(np.asfortranarray(self.clean).ravel(order="F").copy()).to(dev)
         self.dU = torch.empty_like(self.dI)
         self.noisy = noisy
 
@@ -80,11 +81,12 @@ class _Runner:
         api.GBM3D_device(self.dI.data_ptr(), self.size, self.size, self.sigma, self.dU.data_ptr(), o, ctx=self.ctx)
 
     def psnr(self, o) -> float:
+        """PSNR against the clean image, peak 255 (myPSNR.m), computed on the device."""
         self._run(o)
         # the library may run on its own non-blocking stream: wait for the device
         self.torch.cuda.synchronize()
-        U = self.dU.cpu().numpy().reshape(self.size, self.size, order="F")
-        return float(options.myPSNR(self.clean, U, 255))
+        mse = float(self.torch.sum((self.dC - self.dU) ** 2).item()) / self.dU.numel()
+        return float(10 * np.log10(255.0 ** 2 / mse))
 
     def device_ms(self, o, reps=2) -> float:
         self.torch.cuda.synchronize()

@@ -311,6 +311,27 @@ __global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b
 
 // acc[p] (+)= (double) v[(r+s) mod Mp, (c+s) mod Np]: circshift(.,[-s,-s]) then
 // the running sum over spins (GBM3D.m:53-57,78-83).
+// (r + s) mod L for r in [0, L): one conditional subtraction when 0 <= s <= L.
+__device__ __forceinline__ int shift_index(int r, int s, int L) {
+  if ((unsigned)s <= (unsigned)L) {
+    const int t = r + s;
+    return t >= L ? t - L : t;
+  }
+  return pmod(r + s, L);
+}
+
+// Both accumulators of one spin (U and W): acc += v shifted back by the spin.
+__global__ void k_accum2(const float* __restrict__ u, const float* __restrict__ w, int Mp, int Np, int s,
+                         double* __restrict__ ua, double* __restrict__ wa, int first) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= Mp || c >= Np) return;
+  const size_t src = shift_index(r, s, Mp) + (size_t)shift_index(c, s, Np) * Mp;
+  const double x = (double)u[src], y = (double)w[src];
+  const size_t o = r + (size_t)c * Mp;
+  ua[o] = first ? x : ua[o] + x;
+  wa[o] = first ? y : wa[o] + y;
+}
+
 __global__ void k_accum(const float* __restrict__ v, int Mp, int Np, int s, double* __restrict__ acc, int first) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
   if (r >= Mp || c >= Np) return;
@@ -769,9 +790,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
       run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1", st1, o->form);
     }
     run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType, st1);
-    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
-    launched(c, cudaGetLastError(), "accum");
-    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa, ii == 0);
+    k_accum2<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Ws, Mp, Np, s, Ua, Wa, ii == 0);
     launched(c, cudaGetLastError(), "accum");
     if (stale && ii >= nW) {
       k_shift_copy<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wstale + (size_t)(ii - nW) * px);
@@ -812,9 +831,7 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     double sg = sigma;
     fill_wiener_consts(A, dw, sigwie_in ? sigwie_in : &sg, sigwie_in ? 1 : 0, 0);
     run_wiener_agg(c, A, dw, d2, Us, Ws);
-    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Mp, Np, s, Ua, ii == 0);
-    launched(c, cudaGetLastError(), "accum");
-    k_accum<<<grid2(Mp, Np), 256, 0, c->st>>>(Ws, Mp, Np, s, Wa, ii == 0);
+    k_accum2<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Ws, Mp, Np, s, Ua, Wa, ii == 0);
     launched(c, cudaGetLastError(), "accum");
   }
   if (stale)

@@ -48,9 +48,18 @@ __global__ void k_make_pad(const float* __restrict__ img, int m, int n, int h, i
   const int y = blockIdx.x * blockDim.x + threadIdx.x;
   const int x = blockIdx.y;
   if (y >= R || x >= Q) return;
-  const int sr = pmod(pad_index(y, m, h) - spin, m);
-  const int sc = pmod(pad_index(x, n, h) - spin, n);
-  pad[y + (size_t)x * P] = img[sr + (size_t)sc * m];
+  // (pad_index(r) - spin) mod L without divisions when h <= L and 0 <= spin <= L
+  // (r < L + 2h, so pad_index needs at most one wrap); the general form otherwise
+  auto src = [&](int r, int L) {
+    if (h <= L && (unsigned)spin <= (unsigned)L) {
+      int t = r < h ? r + h : r - h;
+      if (t >= L) t -= L;
+      t -= spin;
+      return t < 0 ? t + L : t;
+    }
+    return pmod(pad_index(r, L, h) - spin, L);
+  };
+  pad[y + (size_t)x * P] = img[src(y, m) + (size_t)src(x, n) * m];
 }
 
 template <int D, int D2>
