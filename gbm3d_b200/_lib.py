@@ -80,6 +80,7 @@ _SIGS = {
                                                C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise_device": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P]),
+    "gbm3d_denoise_async": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P]),
     "gbm3d_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "gbm3d_stage_times": (C.c_int, [_P, _P, C.c_int]),
     "gbm3d_last_launch_count": (C.c_int, [_P]),
@@ -170,6 +171,11 @@ class Context:
         buf = (C.c_float * 8)()
         n = lib().gbm3d_stage_times(self.h, buf, 8)
         return [float(buf[i]) for i in range(max(n, 0))]
+
+    def synchronize(self) -> None:
+        """Wait for the context's work, including gbm3d_denoise_async copies;
+        raises on a non-finite input among the asynchronous calls."""
+        self.check(lib().gbm3d_ctx_synchronize(self.h))
 
     def launch_count(self) -> int:
         return int(lib().gbm3d_last_launch_count(self.h))

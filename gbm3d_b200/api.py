@@ -275,6 +275,18 @@ def GBM3D_device(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dic
                                          C.c_void_p(U_ptr), C.c_void_p(U1_ptr or 0)))
 
 
+def GBM3D_async(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dict | None = None,
+                ctx: Context | None = None) -> None:
+    """Enqueue one whole denoise of a host image (I_ptr: pinned float64,
+    column-major m x n) into a host output U_ptr and return at once
+    (gbm3d_denoise_async).  Successive calls overlap their copies with the
+    previous call's compute; ``ctx.synchronize()`` waits for them all."""
+    ctx = ctx or context()
+    co = c_opts(_opt.resolve_opts(opts))
+    ctx.check(lib().gbm3d_denoise_async(ctx.h, C.c_void_p(I_ptr), m, n, float(sigma), C.byref(co),
+                                        C.c_void_p(U_ptr)))
+
+
 def GBM3D_batch(images, sigmas, opts: dict | None = None, use_graph: bool = True, ctx: Context | None = None,
                 outputs=None):
     """Batched form: denoise a list of device images (torch float64 tensors of

@@ -48,6 +48,14 @@ struct gbm3d_ctx {
   int pilot_step = 0;        // Adam steps taken
   int sms = 148;
   int* flag = nullptr;  // device status word (non-finite input)
+  // asynchronous host-buffer calls (gbm3d_denoise_async): two device slots for
+  // input and output, one copy stream per direction, and the events that
+  // order the copies of a slot with the compute that uses it
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+  int slot = 0;
+  bool async_pending = false;
+  int* sticky = nullptr;  // OR of the status words of the asynchronous calls since the last synchronisation
 };
 
 namespace {
@@ -321,6 +329,8 @@ __device__ __forceinline__ int shift_index(int r, int s, int L) {
 }
 
 // Both accumulators of one spin (U and W): acc += v shifted back by the spin.
+__global__ void k_or_flag(const int* __restrict__ flag, int* __restrict__ sticky) { *sticky |= *flag; }
+
 __global__ void k_accum2(const float* __restrict__ u, const float* __restrict__ w, int Mp, int Np, int s,
                          double* __restrict__ ua, double* __restrict__ wa, int first) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
@@ -873,6 +883,16 @@ void gbm3d_ctx_destroy(gbm3d_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->st);
+  if (c->h2d) {
+    cudaStreamSynchronize(c->h2d);
+    cudaStreamSynchronize(c->d2h);
+    cudaStreamDestroy(c->h2d);
+    cudaStreamDestroy(c->d2h);
+    for (int k = 0; k < 2; ++k)
+      for (cudaEvent_t e : {c->in_ready[k], c->in_free[k], c->out_ready[k], c->out_free[k]})
+        if (e) cudaEventDestroy(e);
+  }
+  if (c->sticky) cudaFree(c->sticky);
   for (auto& kv : c->bufs) cudaFree(kv.second.first);
   for (auto& e : c->evpool) cudaEventDestroy(e);
   for (auto& e : c->kpool) cudaEventDestroy(e);
@@ -918,6 +938,24 @@ int gbm3d_ctx_synchronize(gbm3d_ctx* c) {
   if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
     c->err = "stream synchronisation failed";
     return GBM3D_ERR_CUDA;
+  }
+  if (c->async_pending) {  // gbm3d_denoise_async: its copies, then its status words
+    c->async_pending = false;
+    int flag = 0;
+    if (cudaStreamSynchronize(c->h2d) != cudaSuccess || cudaStreamSynchronize(c->d2h) != cudaSuccess ||
+        cudaMemcpy(&flag, c->sticky, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemset(c->sticky, 0, sizeof(int)) != cudaSuccess) {
+      c->err = "stream synchronisation failed";
+      return GBM3D_ERR_CUDA;
+    }
+    if (flag & 1) {
+      c->err = "input image holds NaN or Inf (an asynchronous call since the last synchronisation)";
+      return GBM3D_ERR_NONFINITE;
+    }
+    if (flag & 2) {
+      c->err = "tensor-core MMA did not complete in time";
+      return GBM3D_ERR_CUDA;
+    }
   }
   return GBM3D_OK;
 }
@@ -1839,6 +1877,45 @@ static int denoise_host(gbm3d_ctx* c, const double* I, int m, int n, double sigm
 int gbm3d_denoise(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,
                   double* U1) {
   return denoise_host(c, I, m, n, sigma, o, U, U1, nullptr, nullptr);
+}
+
+int gbm3d_denoise_async(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
+                        double* U) {
+  return guarded(c, [&] {
+    if (!I || !U || !o) argfail(c, "missing argument");
+    if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
+    if (!c->h2d) {
+      ck(c, cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(c, cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking), "cudaStreamCreate");
+      for (int k = 0; k < 2; ++k)
+        for (cudaEvent_t* e : {&c->in_ready[k], &c->in_free[k], &c->out_ready[k], &c->out_free[k]})
+          ck(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+      ck(c, cudaMalloc(&c->sticky, sizeof(int)), "cudaMalloc");
+      ck(c, cudaMemset(c->sticky, 0, sizeof(int)), "cudaMemset");
+    }
+    const size_t px = (size_t)m * n;
+    const int k = c->slot;
+    double* dI = buf<double>(c, k ? "a.I1" : "a.I0", px);
+    double* dU = buf<double>(c, k ? "a.U1" : "a.U0", px);
+    // H2D into this slot once the compute of the call two back has read it
+    ck(c, cudaStreamWaitEvent(c->h2d, c->in_free[k], 0), "cudaStreamWaitEvent");
+    ck(c, cudaMemcpyAsync(dI, I, px * 8, cudaMemcpyHostToDevice, c->h2d), "H2D");
+    ck(c, cudaEventRecord(c->in_ready[k], c->h2d), "cudaEventRecord");
+    // compute once the input is in and the D2H of the call two back has read the output slot
+    ck(c, cudaStreamWaitEvent(c->st, c->in_ready[k], 0), "cudaStreamWaitEvent");
+    ck(c, cudaStreamWaitEvent(c->st, c->out_free[k], 0), "cudaStreamWaitEvent");
+    c->async_pending = true;
+    pipeline(c, dI, m, n, sigma, o, dU, nullptr);
+    k_or_flag<<<1, 1, 0, c->st>>>(c->flag, c->sticky);
+    launched(c, cudaGetLastError(), "flag");
+    ck(c, cudaEventRecord(c->in_free[k], c->st), "cudaEventRecord");
+    ck(c, cudaEventRecord(c->out_ready[k], c->st), "cudaEventRecord");
+    // D2H of the result
+    ck(c, cudaStreamWaitEvent(c->d2h, c->out_ready[k], 0), "cudaStreamWaitEvent");
+    ck(c, cudaMemcpyAsync(U, dU, px * 8, cudaMemcpyDeviceToHost, c->d2h), "D2H");
+    ck(c, cudaEventRecord(c->out_free[k], c->d2h), "cudaEventRecord");
+    c->slot = k ^ 1;
+  });
 }
 
 // ---- learned pilot ---------------------------------------------------------------------

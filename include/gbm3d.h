@@ -265,6 +265,18 @@ typedef struct gbm3d_mixed_batch {
 int gbm3d_denoise_mixed(gbm3d_ctx* ctx, const gbm3d_mixed_batch* batch, const gbm3d_opts* opts,
                         const gbm3d_opts* video_opts, int use_graph);
 
+/* Asynchronous form of gbm3d_denoise for a stream of images (U1 is not
+ * returned): the call enqueues the host-to-device copy of I, the whole
+ * pipeline and the device-to-host copy into U, and returns.  Copies run on
+ * their own streams and the device keeps two input and two output slots, so
+ * the copies of one call overlap the compute of the previous one.  I and U
+ * must stay valid, and I unchanged, until gbm3d_ctx_synchronize, which also
+ * reports a non-finite input among the calls since the last synchronisation.
+ * Pinned (page-locked) host buffers are needed for the copies to overlap.
+ * Not in the reference. */
+int gbm3d_denoise_async(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma, const gbm3d_opts* opts,
+                        double* U);
+
 /* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
  * the context stream (synchronise before reading U). */
 int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,

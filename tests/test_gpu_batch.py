@@ -133,3 +133,33 @@ def test_mixed_batch_matches_single_entries(gpu):
     g_out, _, _ = api.GBM3D_mixed(grey[:1], grey_sig[:1], opts=o)
     m, n = grey_sizes[0]
     assert np.array_equal(g_out[0].cpu().numpy().reshape(-1).reshape(m, n, order="F"), grey_ref[0])
+
+
+def test_async_host_stream_matches_sync(gpu):
+    """gbm3d_denoise_async over a stream of host images (sizes changing along
+    the way) gives every image the synchronous entry's result bit for bit, and
+    a non-finite input is reported at synchronisation."""
+    import torch
+    from gbm3d_b200 import _lib, api
+    o = _dense()
+    ctx = _lib.Context(0)
+    sizes = [(96, 80), (96, 80), (130, 70), (96, 80), (64, 64)]
+    ins, outs, refs = [], [], []
+    for k, (m, n) in enumerate(sizes):
+        _, noisy = synth.noisy_image(m, n, 25.0, seed=300 + k)
+        ins.append(torch.from_numpy(np.asfortranarray(noisy).ravel(order="F").copy()).pin_memory())
+        outs.append(torch.zeros_like(ins[-1]).pin_memory())
+        refs.append(api.GBM3D(noisy, 25.0, o)[0])
+    for _ in range(2):
+        for (m, n), hI, hU in zip(sizes, ins, outs):
+            api.GBM3D_async(hI.data_ptr(), m, n, 25.0, hU.data_ptr(), o, ctx=ctx)
+        ctx.synchronize()
+        for k, ((m, n), hU) in enumerate(zip(sizes, outs)):
+            assert np.array_equal(hU.numpy().reshape(m, n, order="F"), refs[k]), f"image {k}"
+    bad = ins[0].clone().pin_memory()
+    bad[5] = float("nan")
+    api.GBM3D_async(bad.data_ptr(), 96, 80, 25.0, outs[0].data_ptr(), o, ctx=ctx)
+    with pytest.raises(_lib.GBM3DError):
+        ctx.synchronize()
+    ctx.synchronize()  # the report clears the status
+    ctx.close()
