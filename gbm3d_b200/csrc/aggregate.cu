@@ -41,12 +41,14 @@ constexpr int BIAS = 1 << 12;  // offset added to tile-relative block origins be
 //           denoiseAndAggregateWieFast.m), the same single-precision products
 constexpr int CR = 32, CC = 16;                    // CTA pixel tile
 constexpr int NSR = CR / TR, NSC = CC / TC;        // warp tiles per CTA tile: 4 x 4
-constexpr int CAPC = 2048;                         // CTA list capacity (entries)
 constexpr int NTC = 256;                           // threads per CTA
 constexpr int SUBS = NSR * NSC / (NTC / 32);       // warp tiles per warp: 2
 constexpr int WB = 8;                              // walk batch: entries tested and loaded together
 
-template <int D, int D2, bool WIE, bool KAHAN>
+// CAPC: CTA list capacity (entries).  A list that would overflow is walked in
+// order and refilled, so any capacity gives the same sums; a small one suits
+// sparse reference grids (fewer entries per tile) and lets more CTAs reside.
+template <int D, int D2, bool WIE, bool KAHAN, int CAPC>
 __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
   extern __shared__ int smi[];
   __shared__ int wcnt[NTC / 32];
@@ -231,15 +233,24 @@ __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
   }
 }
 
-template <int D, int D2, bool WIE, bool KAHAN = false>
-static cudaError_t launch_px(const AggArgs& A, cudaStream_t st) {
+template <int D, int D2, bool WIE, bool KAHAN, int CAPC>
+static cudaError_t launch_px_cap(const AggArgs& A, cudaStream_t st) {
   const size_t sm = (size_t)((D * D + 3) & ~3) * sizeof(float) + (size_t)(CAPC + (NTC / 32) * LCAP) * sizeof(int4);
-  cudaError_t e =
-      cudaFuncSetAttribute(k_aggregate_cta<D, D2, WIE, KAHAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = cudaFuncSetAttribute(k_aggregate_cta<D, D2, WIE, KAHAN, CAPC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = ((A.m + CR - 1) / CR) * ((A.n + CC - 1) / CC);
-  k_aggregate_cta<D, D2, WIE, KAHAN><<<tiles, NTC, sm, st>>>(A);
+  k_aggregate_cta<D, D2, WIE, KAHAN, CAPC><<<tiles, NTC, sm, st>>>(A);
   return cudaGetLastError();
+}
+
+// List capacity from the expected entries of a tile: (candidate references
+// across the tile's reach) x K, about a quarter of which touch the tile.
+template <int D, int D2, bool WIE, bool KAHAN = false>
+static cudaError_t launch_px(const AggArgs& A, cudaStream_t st) {
+  const long refs = (long)((CR + D + D2 - 2) / A.s + 1) * ((CC + D + D2 - 2) / A.s + 1);
+  if (refs * A.K / 4 <= 1024 - NTC) return launch_px_cap<D, D2, WIE, KAHAN, 1024>(A, st);
+  return launch_px_cap<D, D2, WIE, KAHAN, 2048>(A, st);
 }
 
 cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st) {
