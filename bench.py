@@ -280,8 +280,8 @@ def roofline(o, ktimes, peaks, sm_mhz):
 def cpu_baseline(o_chosen=None, size: int = 512):
     """The oracle (the CPU restatement of the reference path) timed on a
     bounded crop with all host threads, in FP32 (the kernels' operation
-    order) and in FP64.  As the checker, the same crop denoised on the GPU is
-    then compared with the oracle's outputs, for the plain configuration and
+    order) and in FP64.  The same crop denoised on the GPU is then compared
+    with the oracle's outputs, for the plain configuration and
     for the chosen form's options, and the precision form's step-1 match sets
     with the plain matcher's.  Returns (cpu_baseline, parity)."""
     from gbm3d_b200 import api, synth
@@ -306,7 +306,7 @@ def cpu_baseline(o_chosen=None, size: int = 512):
                 "psnr_gpu_db": float(_opt.myPSNR(clean, Ug, 255)), "psnr_fp64_oracle_db": float(_opt.myPSNR(clean, U64, 255))}
 
     parity = {"sample": f"{size}x{size}, sigma {SIGMA:g}, seed 2024; the GPU through gbm3d_denoise, the oracle "
-                        "as the checker", "plain": compare(api.GBM3D(noisy, SIGMA, opts())[0], U32, U64)}
+                        "as the reference for the comparison", "plain": compare(api.GBM3D(noisy, SIGMA, opts())[0], U32, U64)}
     if o_chosen is not None and o_chosen.get("form", "plain") == "plain" and \
             {k: v for k, v in o_chosen.items() if k != "form"} != opts():
         Uc32, _ = O.GBM3D(noisy, SIGMA, o_chosen, prec=32)

@@ -2,8 +2,8 @@
 //
 // A C++ restatement of the GBM3D two-step denoising path of the MATLAB
 // reference (toby-sanders/GBM3D). Only tests/, __graft_entry__.smoke() and the
-// cpu_baseline / --impl reference legs of bench.py load this library, always as
-// the checker or as the timed CPU baseline, never as the product.
+// cpu_baseline / --impl reference legs of bench.py load this library, always to
+// check results against or as the timed CPU baseline, never as the product.
 //
 // PARITY UNPINNED: the reference is MATLAB-only, ships no tests, no golden
 // vectors and no known-answer tests, and neither MATLAB nor Octave can run here.

@@ -1,7 +1,7 @@
 """ctypes front end of the CPU oracle — TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and the CPU-baseline legs of bench.py
-import this module, as the checker or as the timed CPU baseline.  The product
+import this module, to check results against or as the timed CPU baseline.  The product
 (gbm3d_b200) never imports it.
 
 The functions mirror the MATLAB reference's signatures (toby-sanders/GBM3D):

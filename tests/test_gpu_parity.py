@@ -3,7 +3,7 @@
 The kernels follow the FP32 operation order of the oracle's FP32 mode, so the
 contract checked here is bit-identity: identical match sets (ties broken by
 the lowest column-major window index, as MATLAB's mink does) and identical
-floating-point outputs.  The north-star tolerance, 1e-4 max-abs on a 0-255
+floating-point outputs.  The required tolerance, 1e-4 max-abs on a 0-255
 scale, is asserted as well so a failure reports which bar was missed, and the
 error against the FP64 run of the oracle is stated (not bounded) per case.
 Stages are also tested in isolation by feeding them the oracle's upstream
