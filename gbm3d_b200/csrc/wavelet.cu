@@ -703,7 +703,22 @@ __global__ void __launch_bounds__(128) k_ht_weights_8(const float* __restrict__ 
   // lane: row r = lane % 8 of columns lane / 8 and lane / 8 + 4 of every slot
   const float* p0 = V + (size_t)i * D + (size_t)(j * D + (lane >> 3)) * m + (lane & 7);
   const float* p1 = p0 + (size_t)4 * m;
-  for (int k = 0; k < nm; ++k) {
+  // slots in batches of 4: eight independent loads in flight per lane
+  int k = 0;
+  for (; k + 4 <= nm; k += 4) {
+    float a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = __ldg(p0 + sz * (k + u));
+      b[u] = __ldg(p1 + sz * (k + u));
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      sg[(k + u) * SL + lane] = a[u];
+      sg[(k + u) * SL + 32 + lane] = b[u];
+    }
+  }
+  for (; k < nm; ++k) {
     sg[k * SL + lane] = __ldg(p0 + sz * k);
     sg[k * SL + 32 + lane] = __ldg(p1 + sz * k);
   }
