@@ -1,4 +1,4 @@
-"""Batched and colour forms on the GPU.
+"""Batched, colour, mixed and asynchronous entries, and the autotuner, on the GPU.
 
 Batch: images of uneven sizes and noise levels denoised in one call, first
 eagerly while the launch sequence is captured into a CUDA graph, then by
@@ -6,7 +6,10 @@ replaying the graph; every output must equal the single-image pipeline's bit
 for bit.  Colour: the opponent-space pipeline with luma-driven matching; on a
 grey image (R = G = B) the chroma channels are constant, so every output
 channel must equal the grey pipeline at the luma noise level sigma / sqrt(3)
-(to float rounding of the constant chroma).
+(to float rounding of the constant chroma).  Mixed submissions (grey, colour
+and video in one captured graph) and the asynchronous host-stream entry must
+reproduce each image's single-call result bit for bit; the autotuner's choice
+must stay within its PSNR budget and run through the whole-image entry.
 """
 import numpy as np
 import pytest
