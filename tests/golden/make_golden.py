@@ -5,7 +5,9 @@
 The vectors come from oracle/fft_route.py, the restatement that follows the
 MATLAB reference's FFT route operation by operation in float64 (the reference
 itself needs MATLAB, which cannot run here).  Inputs are seeded synthetic
-images (gbm3d_b200.synth), so every case is reproducible.  Each file holds the
+images (gbm3d_b200.synth), so every case is reproducible, and one crop of the
+reference's demo photo (read from the reference checkout at generation time;
+the fixture stores the crop itself).  Each file holds the
 inputs and, per stage, the outputs of the reference function with that name.
 """
 from __future__ import annotations
@@ -50,8 +52,26 @@ CASES = [
 ]
 
 
-def make(name, m, n, sigma, seed, profile, wav, over):
-    clean, noisy = synth.noisy_image(m, n, sigma, seed=seed)
+FABIO = "/root/reference/fabio.jpeg"  # the reference's demo photo (demoDenoise.m:13), MIT licence
+
+
+def fabio_crop(m, n, sigma, seed):
+    """(clean, noisy): a central m x n crop of the reference's demo photo as
+    demoDenoise.m reads it (imread, then rgb2gray on uint8: the luma weights
+    0.298936021293775, 0.587043074451121, 0.114020904255103, rounded to uint8),
+    on the 0-255 scale, plus N(0, sigma^2) noise from the project's generator."""
+    from PIL import Image
+    rgb = np.asarray(Image.open(FABIO).convert("RGB"), dtype=np.float64)
+    w = np.array([0.298936021293775, 0.587043074451121, 0.114020904255103])
+    grey = np.clip(np.floor(rgb @ w + 0.5), 0, 255)
+    r0, c0 = (grey.shape[0] - m) // 2, (grey.shape[1] - n) // 2
+    clean = np.asfortranarray(grey[r0:r0 + m, c0:c0 + n])
+    rng = np.random.Generator(np.random.PCG64(seed + 1_000_003))
+    return clean, np.asfortranarray(clean + sigma * rng.standard_normal((m, n)))
+
+
+def make(name, m, n, sigma, seed, profile, wav, over, image=None):
+    clean, noisy = image(m, n, sigma, seed) if image else synth.noisy_image(m, n, sigma, seed=seed)
     opts = options.resolve_opts({"profile": profile})
     opts.update(over)
     fac = options.bior_factors() if wav == "bior" else options.haar_factors()
@@ -119,6 +139,8 @@ if __name__ == "__main__":
     for c in CASES:
         if not only or c[0] in only:
             make(*c)
+    if not only or "default_fabio_96x80_s25" in only:
+        make("default_fabio_96x80_s25", 96, 80, 25.0, 41, "default", "bior", {}, image=fabio_crop)
     if "video_32x40x4_s25" in only:
         make_video("video_32x40x4_s25", 32, 40, 4, 25.0, 23)
     if only:
