@@ -41,6 +41,11 @@ def banks(fac):
 # patch 8, reference stride 3, group 16, search +-12 (matchSize 24)
 STRIDE3 = dict(blockSize=8, blockSizeWie=8, matchSize=24, refStride=3, refStrideWie=3)
 
+# the option set the autotuner picks for 4096^2 at sigma 25: patch 8, step-1
+# stride 8, step-2 stride 7, one match spin per step, one cycle spin
+TUNED8X7 = dict(blockSize=8, blockSizeWie=8, matchSize=32, refStride=8, refStrideWie=7, matchSpins=[0],
+                matchSpinsWie=[0], cycleSpin=1, staleWeights=False)
+
 CASES = [
     # name, m, n, sigma, seed, profile, wavelet, option overrides
     ("default_64x96_s25", 64, 96, 25.0, 3, "default", "bior", {}),
@@ -141,6 +146,8 @@ if __name__ == "__main__":
             make(*c)
     if not only or "default_fabio_96x80_s25" in only:
         make("default_fabio_96x80_s25", 96, 80, 25.0, 41, "default", "bior", {}, image=fabio_crop)
+    if not only or "tuned8x7_fabio_96x80_s25" in only:
+        make("tuned8x7_fabio_96x80_s25", 96, 80, 25.0, 41, "default", "bior", TUNED8X7, image=fabio_crop)
     if "video_32x40x4_s25" in only:
         make_video("video_32x40x4_s25", 32, 40, 4, 25.0, 23)
     if only:

@@ -118,6 +118,22 @@ def test_GBM3D_stride_golden(gpu):
     assert max_abs(U, g["U"]) < 2e-3
 
 
+def test_GBM3D_tuned_options_golden(gpu, oracle):
+    """The tuned form's option set (step-1 stride 8, step-2 stride 7, one
+    spin per step, one cycle spin) on a crop of the reference's demo photo:
+    bit-identical to the oracle's FP32 mode, and within the FP32-vs-FP64 gap
+    of the FFT-route golden vectors."""
+    path = os.path.join(os.path.dirname(__file__), "golden", "tuned8x7_fabio_96x80_s25.npz")
+    g = np.load(path)
+    o = options.resolve_opts({"profile": str(g["profile"])})
+    o.update(json.loads(str(g["opts"])))
+    U, out = gpu.GBM3D(g["noisy"], float(g["sigma"]), o)
+    Uo, U1o = oracle.GBM3D(g["noisy"], float(g["sigma"]), o, prec=32)
+    assert np.array_equal(out["U1"], U1o) and np.array_equal(U, Uo), "not bit-identical to the oracle"
+    assert max_abs(out["U1"], g["Ustep1"]) < 1e-3  # 1.1e-4 measured
+    assert max_abs(U, g["U"]) < 1e-3  # 1.0e-4 measured
+
+
 def test_stride_errors(gpu):
     from gbm3d_b200 import GBM3DError
     _, noisy = synth.noisy_image(64, 64, 25.0, seed=1)
