@@ -79,3 +79,20 @@ def test_tuned_4096_properties(gpu):
         assert p_plain - options.myPSNR(clean, noisy, 255) > 15.0
     finally:
         dev.close()
+
+
+def test_precision_form_2048_properties(gpu):
+    """The precision form (bf16 tensor-core distances, exact FP32 re-rank,
+    Kahan aggregation) at 2048^2: bf16 rounding also commutes with a
+    power-of-two scale, so the identity holds bit for bit, and its PSNR stays
+    within 0.01 dB of the plain path's on the same image."""
+    clean, noisy = synth.noisy_image(2048, 2048, 25.0, seed=2025)
+    dev = _Device(noisy)
+    try:
+        o = _dense(form="precision")
+        U = dev.run(o, 25.0)
+        assert np.array_equal(dev.run(o, 25.0, scale=2.0), 2.0 * U), "not scale-equivariant"
+        Up = dev.run(_dense(), 25.0)
+        assert abs(options.myPSNR(clean, U, 255) - options.myPSNR(clean, Up, 255)) < 0.01
+    finally:
+        dev.close()
