@@ -1,4 +1,4 @@
-// Deterministic owner-computes aggregation — denoiseAndAggregateGPU.m:186-208
+// Deterministic owner-computes aggregation — denoiseAndAggregateGPU.m:58-92 (loop :70-89)
 // and denoiseAndAggregateWieFast.m:84-100.
 //
 // The reference adds every matched block, weighted, into U and W in the loop
@@ -8,7 +8,7 @@
 // sequential loop and needs no atomics.
 //
 // Contributions falling outside the cropped image are never produced (the
-// reference crops them away, denoiseAndAggregateGPU.m:207-208).
+// reference crops them away, denoiseAndAggregateGPU.m:91-92).
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -36,7 +36,7 @@ constexpr int BIAS = 1 << 12;  // offset added to tile-relative block origins be
 //     a time; a covered lane loads its element and adds the contribution.
 // Every pixel receives its contributions in the reference's order, so the
 // sums are bit-identical to the sequential loop.
-//   step 1: value (wg * Vavg) * mask, weight wg * mask   (denoiseAndAggregateGPU.m:200-201)
+//   step 1: value (wg * Vavg) * mask, weight wg * mask   (denoiseAndAggregateGPU.m:84-85)
 //   step 2: value and weight precomputed by the Wiener kernel (:84-90 of
 //           denoiseAndAggregateWieFast.m), the same single-precision products
 constexpr int CR = 32, CC = 16;                    // CTA pixel tile

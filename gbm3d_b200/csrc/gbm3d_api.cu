@@ -506,7 +506,7 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
 float* run_wavelet_ht(gbm3d_ctx* c, const float* vol, int m, int n, int K, int levels, int cycleSpin,
                       const double* tau, const WaveletBank& bk, int filtType) {
   float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
-  if (filtType == 1) {  // medfilt3 instead of the wavelet (denoiseAndAggregateGPU.m:165-168)
+  if (filtType == 1) {  // medfilt3 instead of the wavelet (denoiseAndAggregateGPU.m:49-52)
     StageTimer tw(c, 2);
     launched(c, launch_medfilt3(vol, m, n, K, vsum, c->st), "medfilt3");
   } else {

@@ -328,12 +328,12 @@ size_t match_smem_bytes(int d, int d2) {
 template <int D, int D2>
 static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   const size_t sm = match_smem_bytes(D, D2);
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k_match<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  // The attribute belongs to the current device, so it is set before every
+  // launch (a host-side call that costs well under a microsecond) rather than
+  // remembered once per process: a second device, or another host thread on
+  // it, would otherwise launch without it.
+  cudaError_t e = cudaFuncSetAttribute(k_match<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
   k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(A);
   return cudaGetLastError();

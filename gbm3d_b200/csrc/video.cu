@@ -1,6 +1,6 @@
 // Video: block matching across a window of frames and aggregation into the
 // frames — matchBlocksV.m:21-116 (top-K branch) and the aggregation loop of
-// denoiseAndAggregateV.m:59-90.  The 3D wavelet hard threshold between them
+// denoiseAndAggregateV.m:59-89.  The 3D wavelet hard threshold between them
 // is the step-1 one (wavelet.cu) with the video's filter bank.
 #include "common.cuh"
 #include "kernels.cuh"

@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(256) k_wav_synthesis(const float* __restrict__
 }
 
 // getBM3DAggWeights(3,1) (getBM3DAggWeights.m:11-19) and weight = 1/(D+eps)
-// (denoiseAndAggregateGPU.m:191), one warp per group.  Each of the three sums
+// (denoiseAndAggregateGPU.m:75), one warp per group.  Each of the three sums
 // is a fixed-order reduction: lane l adds the elements l, l+32, ... of the
 // column-major difference array in order, then an xor butterfly.
 __device__ __forceinline__ float d3(float u0, float u1, float u2, float u3) {
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(128) k_ht_weights_t(const float* __restrict__ 
   }
 }
 
-// medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:165-168) with 'symmetric'
+// medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:49-52) with 'symmetric'
 // padding, which for a one-voxel border repeats the edge voxel.  The median
 // of 27 values is a selection, exact in any order: an odd-even transposition
 // sort in registers.

@@ -1,5 +1,5 @@
 /* [U,out] = denoiseAndAggregateV(Y,Volume,I,S,sigma,opts)
- * — shadows source/denoiseAndAggregateV.m:1-90.  Y is unused (as in the
+ * — shadows source/denoiseAndAggregateV.m:1-89.  Y is unused (as in the
  * reference); I gives the frame size m x n and the frame count F.  Volume:
  * (M d) x (N d) x numMax (single or double; the library computes in single).
  * U and out.K: m x n x F double; out.Z: m x n, the group size of each block.

@@ -211,7 +211,7 @@ int gbm3d_denoise_rgb_device(gbm3d_ctx* ctx, const double* R, const double* G, c
  *   index a + (b-1) d + (f-1) d^2 into the d x d x F window; Volume m x n x K. */
 int gbm3d_matchBlocksV(gbm3d_ctx* ctx, const double* I, int m, int n, int frames, const gbm3d_opts* opts,
                        uint32_t* S, float* Volume);
-/* [U,out] = denoiseAndAggregateV(Y,Volume,I,S,sigma,opts)   source/denoiseAndAggregateV.m:11-90
+/* [U,out] = denoiseAndAggregateV(Y,Volume,I,S,sigma,opts)   source/denoiseAndAggregateV.m:11-89
  *   Volume (M d) x (N d) x K single; tau levels x 7 (sigma * getTau(levels, tauMode));
  *   filters NULL = sym4 x Haar.  U and W (= out.K): (M d) x (N d) x frames double. */
 int gbm3d_denoiseAndAggregateV(gbm3d_ctx* ctx, const float* Volume, const uint32_t* S, int M, int N, int frames,
@@ -323,7 +323,10 @@ int gbm3d_tc_selfcheck(gbm3d_ctx* ctx, const uint16_t* A, const uint16_t* B, flo
  * host threads) race on it.  The first call on each device looks the
  * scratch's address up with cudaGetSymbolAddress; make that first call
  * before any stream capture.  No context, no gbm3d_last_error: the return
- * code is the whole report. */
+ * code is the whole report.  Unlike the context entry points, this one does
+ * not scan the image for NaN or Inf (that needs a status word and a wait):
+ * the caller passes a finite image, or gets match sets ranked on NaN
+ * distances with GBM3D_OK. */
 int gbm3d_matchBlocks_noalloc(const float* I, int m, int n, double sigma, const gbm3d_opts* opts,
                               uint32_t* S, int32_t* S_count, void* stream);
 

@@ -415,7 +415,7 @@ def match_blocks_video(I, d, K):
 
 
 def denoise_video(Volume, S, tau, Psi, Psi2, d, F, levels, cycle_spin):
-    """denoiseAndAggregateV.m:11-90."""
+    """denoiseAndAggregateV.m:11-89."""
     K, M, N = S.shape
     m, n = M * d, N * d
     Vrec = np.zeros((m, n, K, cycle_spin))

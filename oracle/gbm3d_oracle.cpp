@@ -74,7 +74,7 @@ template <class T, class F> T red32(int count, F value_at) {
   return p[0];
 }
 
-// sin window outer(sin(pi*linspace(lo,hi,d))) — denoiseAndAggregateGPU.m:181-183
+// sin window outer(sin(pi*linspace(lo,hi,d))) — denoiseAndAggregateGPU.m:65-67
 // (lo,hi)=(.1,.9) and denoiseAndAggregateWieFast.m (lo,hi)=(.2,.8).
 void sine_window(int d, double lo, double hi, double* w) {
   std::vector<double> v(d);
@@ -140,7 +140,7 @@ typedef struct {
   int nSpins, spins[8];
   int nSpinsWie, spinsWie[8];
   int staleWeights;  // GBM3D.m:26-27,82 slice-reuse behaviour (1 = mirror it)
-  int filtType;      // 0 'ht', 1 'median' (denoiseAndAggregateGPU.m:135,165)
+  int filtType;      // 0 'ht', 1 'median' (denoiseAndAggregateGPU.m:19,49)
   int refStride, refStrideWie;  // reference spacing per step; 0 = block size (the reference)
   int wavelet;                  // step-1 bank: 0 = bior1.5 x Haar (GBM3D.m:40), 1 = 3D Haar
 } orc_opts;
@@ -343,7 +343,7 @@ const int kDetailJ[8] = {-1, 0, 1, 3, 2, 4, 5, 6};
 template <class T>
 void wavelet_ht(std::vector<T>& V, int Ly, int Lx, int Lz, int levels, const double* tau,
                 const Bank1D<T>& bxy, const Bank1D<T>& bz) {
-  // analysis (myWavDec3DFFT.m:71-82) with hard threshold (denoiseAndAggregateGPU.m:151-155)
+  // analysis (myWavDec3DFFT.m:11-22) with hard threshold (denoiseAndAggregateGPU.m:35-39)
   std::vector<std::vector<T>> C(levels * 8);
   std::vector<int> dims(levels * 3);
   std::vector<T> U = V, tz[2], tx[2];
@@ -367,7 +367,7 @@ void wavelet_ht(std::vector<T>& V, int Ly, int Lx, int Lz, int levels, const dou
     U = C[lv * 8];
     y /= 2; x /= 2; z /= 2;
   }
-  // synthesis (myWavRec3DGPUfast.m:95-121): per level y-pass, x-pass, z-pass
+  // synthesis (myWavRec3DGPUfast.m:10-40): per level y-pass, x-pass, z-pass
   std::vector<T> R = C[(levels - 1) * 8];  // coarsest approximation
   for (int lv = levels - 1; lv >= 0; --lv) {
     int oy = dims[lv * 3], ox = dims[lv * 3 + 1], oz = dims[lv * 3 + 2];
@@ -385,7 +385,7 @@ void wavelet_ht(std::vector<T>& V, int Ly, int Lx, int Lz, int levels, const dou
 }
 
 // getBM3DAggWeights(3,1) (getBM3DAggWeights.m:11-19) on one group Vavg tile,
-// then weight = 1/(D + eps) (denoiseAndAggregateGPU.m:191).
+// then weight = 1/(D + eps) (denoiseAndAggregateGPU.m:75).
 template <class T>
 T ht_weight(const T* Vt, size_t sy, size_t sx, size_t sz, int d, int Nm) {
   auto at = [&](int r, int c, int k) { return Vt[r * sy + c * sx + k * sz]; };
@@ -504,7 +504,7 @@ void denoise_ht(const T* Volume, int M, int N, int d, int d2, int K, const uint3
   ht_aggregate<T>(sum, M, N, d, d2, K, stride, S, cnt, U, W);
 }
 
-// medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:165-168), 'symmetric'
+// medfilt3(Volume,[3 3 3]) (denoiseAndAggregateGPU.m:49-52), 'symmetric'
 // padding (for a one-voxel border: the edge voxel repeated).
 template <class T>
 void median3(const T* V, int m, int n, int K, std::vector<T>& out) {
@@ -535,7 +535,7 @@ void denoise_median(const T* Volume, int M, int N, int d, int d2, int K, const u
   ht_aggregate<T>(vavg, M, N, d, d2, K, stride, S, cnt, U, W);
 }
 
-// Aggregation of denoiseAndAggregateGPU.m:174-208 from the filtered volume.
+// Aggregation of denoiseAndAggregateGPU.m:58-92 from the filtered volume.
 template <class T>
 void ht_aggregate(std::vector<T>& sum, int M, int N, int d, int d2, int K, int stride, const uint32_t* S,
                   const int32_t* cnt, double* U, double* W) {
@@ -901,7 +901,7 @@ void gbm3d(const double* I0, int m0, int n0, double sigma, const orc_opts* o, do
 
 // ---------------------------------------------------------------------------
 // Video — VBM3D.m:20-63, matchBlocksV.m:21-116 (top-K branch),
-// denoiseAndAggregateV.m:11-90
+// denoiseAndAggregateV.m:11-89
 // ---------------------------------------------------------------------------
 
 // Block matching over a window of F frames (F odd): references tile the
@@ -948,7 +948,7 @@ void match_video(const T* I, int m, int n, int F, int d, int K, uint32_t* S, T* 
     }
 }
 
-// denoiseAndAggregateV.m:24-90: cycle-spun 3D wavelet hard threshold of the
+// denoiseAndAggregateV.m:24-89: cycle-spun 3D wavelet hard threshold of the
 // volume, Vavg = min(max(mean, 0), 1), weight 1/TV(blocks) (the same
 // getBM3DAggWeights(3,1) measure as step 1), and aggregation without a window:
 // block k of reference (y, x) lands in frame c at rows a + y d - d/2, columns

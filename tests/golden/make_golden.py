@@ -1,6 +1,9 @@
 """Generate the golden vectors in tests/golden/*.npz.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--reference DIR] [case ...]
+
+DIR is the reference checkout (default: $GBM3D_REFERENCE_ROOT, else
+/root/reference); only the demo-photo cases and the sym4 check read it.
 
 The vectors come from oracle/fft_route.py, the restatement that follows the
 MATLAB reference's FFT route operation by operation in float64 (the reference
@@ -57,7 +60,12 @@ CASES = [
 ]
 
 
-FABIO = "/root/reference/fabio.jpeg"  # the reference's demo photo (demoDenoise.m:13), MIT licence
+REFERENCE = os.environ.get("GBM3D_REFERENCE_ROOT", "/root/reference")  # the reference checkout (--reference)
+
+
+def fabio_path():
+    """The reference's demo photo (demoDenoise.m:13), MIT licence."""
+    return os.path.join(REFERENCE, "fabio.jpeg")
 
 
 def fabio_crop(m, n, sigma, seed):
@@ -66,7 +74,7 @@ def fabio_crop(m, n, sigma, seed):
     0.298936021293775, 0.587043074451121, 0.114020904255103, rounded to uint8),
     on the 0-255 scale, plus N(0, sigma^2) noise from the project's generator."""
     from PIL import Image
-    rgb = np.asarray(Image.open(FABIO).convert("RGB"), dtype=np.float64)
+    rgb = np.asarray(Image.open(fabio_path()).convert("RGB"), dtype=np.float64)
     w = np.array([0.298936021293775, 0.587043074451121, 0.114020904255103])
     grey = np.clip(np.floor(rgb @ w + 0.5), 0, 255)
     r0, c0 = (grey.shape[0] - m) // 2, (grey.shape[1] - n) // 2
@@ -131,7 +139,7 @@ def make_video(name, m, n, frames, sigma, seed):
 
 def check_sym4_data():
     """The restated sym4 coefficients equal the reference's filter data file."""
-    p = "/root/reference/archive/waveletFilters/sym4Filters.mat"
+    p = os.path.join(REFERENCE, "archive", "waveletFilters", "sym4Filters.mat")
     if os.path.exists(p):
         import scipy.io as sio
         d = sio.loadmat(p)
@@ -140,7 +148,12 @@ def check_sym4_data():
 
 
 if __name__ == "__main__":
-    only = sys.argv[1:]  # optional case names; default: all
+    args = sys.argv[1:]
+    if "--reference" in args:
+        i = args.index("--reference")
+        REFERENCE = args[i + 1]
+        del args[i:i + 2]
+    only = args  # optional case names; default: all
     for c in CASES:
         if not only or c[0] in only:
             make(*c)

@@ -203,7 +203,7 @@ def test_matchBlocksGPU_tolerance_branch(gpu, oracle):
 
 
 def test_denoiseAndAggregateGPU_median(gpu, oracle):
-    """filtType 'median': medfilt3 of the volume replaces the wavelet (denoiseAndAggregateGPU.m:165-168)."""
+    """filtType 'median': medfilt3 of the volume replaces the wavelet (denoiseAndAggregateGPU.m:49-52)."""
     _, noisy = synth.noisy_image(64, 96, 25.0, seed=31)
     o = _opts(filtType="median")
     So, Vo, co = oracle.matchBlocksCPU(noisy, 25.0, o, prec=32)
