@@ -55,6 +55,13 @@ def _p(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
+# opts['form']: plain (FP32, the reference's arithmetic); precision (bf16
+# tensor-core distances bound the candidates, exact FP32 re-rank, Kahan
+# aggregation); learned (the pilot network replaces step 1); tensor (the
+# tensor-core matcher with plain aggregation: the plain path's output)
+FORMS = {"plain": 0, "precision": 1, "learned": 2, "tensor": 3}
+
+
 def c_opts(opts: dict) -> gbm3d_opts:
     o = _opt.checkBM3Dopts(opts)
     c = gbm3d_opts()
@@ -84,9 +91,9 @@ def c_opts(opts: dict) -> gbm3d_opts:
         raise GBM3DError(5, f"wname '{wn}': the pipeline's banks are 'bior' (bior1.5 x Haar) and 'haar'")
     c.wavelet = 1 if wn == "haar" else 0
     form = o.get("form", "plain")
-    if form not in ("plain", "precision", "learned"):
-        raise GBM3DError(5, f"form '{form}': 'plain', 'precision' or 'learned'")
-    c.form = {"plain": 0, "precision": 1, "learned": 2}[form]
+    if form not in FORMS:
+        raise GBM3DError(5, f"form '{form}': one of {', '.join(FORMS)}")
+    c.form = FORMS[form]
     return c
 
 
@@ -110,10 +117,12 @@ def _sigma_scalar(sigma) -> float:
     return float(s.reshape(-1)[0])
 
 
-def matchBlocksCPU(I, sigma, opts: dict, ctx: Context | None = None):
+def matchBlocksCPU(I, sigma, opts: dict, ctx: Context | None = None, volume: bool = True):
     """[S, Volume] = matchBlocksCPU(I, sigma, opts).
 
     With refStride s != blockSize the Volume is tile-space, (M d) x (N d) x K.
+    volume=False skips the gather and returns None for it (the C ABI's NULL
+    Volume): large images at dense strides need only the match sets.
     """
     ctx = ctx or context()
     o = _opt.checkBM3Dopts(opts)
@@ -124,10 +133,10 @@ def matchBlocksCPU(I, sigma, opts: dict, ctx: Context | None = None):
     M, N = _opt.grid_count(m, d, s), _opt.grid_count(n, d, s)
     S = np.zeros((K, M, N), dtype=np.uint32, order="F")
     cnt = np.zeros((M, N), dtype=np.int32, order="F")
-    V = np.zeros((m, n, K) if s == d else (M * d, N * d, K), dtype=np.float32, order="F")
+    V = np.zeros((m, n, K) if s == d else (M * d, N * d, K), dtype=np.float32, order="F") if volume else None
     co = c_opts(o)
     ctx.check(lib().gbm3d_matchBlocksCPU(ctx.h, _p(I), m, n, _sigma_scalar(sigma), C.byref(co),
-                                         _p(S), _p(cnt), _p(V)))
+                                         _p(S), _p(cnt), _p(V) if volume else None))
     return _as_set(S, cnt), V
 
 
@@ -245,12 +254,14 @@ def denoiseAndAggregateWie(V1, V2, S, sigma, opts: dict, ctx: Context | None = N
 def GBM3D(I, sigma, opts: dict | None = None, ctx: Context | None = None):
     """[U, out] = GBM3D(I, sigma, opts); out['U1'] is the step-1 estimate.
 
-    ``opts`` with a 'profile' field is replaced by that profile (GBM3D.m:16-19).
+    ``opts`` with a 'profile' field is replaced by that profile (GBM3D.m:16-19);
+    the 'tuned' profile picks the calibrated option set for the image's size
+    and sigma (options.tuned_opts).
     """
     ctx = ctx or context()
-    o = _opt.resolve_opts(opts)
     I = np.asfortranarray(I, dtype=np.float64)
     m, n = I.shape
+    o = _opt.resolve_opts(opts, shape=(m, n), sigma=sigma)
     U = np.zeros((m, n), order="F")
     U1 = np.zeros((m, n), order="F")
     co = c_opts(o)
@@ -270,7 +281,7 @@ def GBM3D_device(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dic
                  U1_ptr: int = 0, ctx: Context | None = None) -> None:
     """Whole pipeline on device buffers (float64, column-major), asynchronous on the context stream."""
     ctx = ctx or context()
-    co = c_opts(_opt.resolve_opts(opts))
+    co = c_opts(_opt.resolve_opts(opts, shape=(m, n), sigma=sigma))
     ctx.check(lib().gbm3d_denoise_device(ctx.h, C.c_void_p(I_ptr), m, n, float(sigma), C.byref(co),
                                          C.c_void_p(U_ptr), C.c_void_p(U1_ptr or 0)))
 
@@ -282,7 +293,7 @@ def GBM3D_async(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dict
     (gbm3d_denoise_async).  Successive calls overlap their copies with the
     previous call's compute; ``ctx.synchronize()`` waits for them all."""
     ctx = ctx or context()
-    co = c_opts(_opt.resolve_opts(opts))
+    co = c_opts(_opt.resolve_opts(opts, shape=(m, n), sigma=sigma))
     ctx.check(lib().gbm3d_denoise_async(ctx.h, C.c_void_p(I_ptr), m, n, float(sigma), C.byref(co),
                                         C.c_void_p(U_ptr)))
 
@@ -317,9 +328,9 @@ def GBM3D_rgb(I, sigma, opts: dict | None = None, ctx: Context | None = None):
     match sets (gbm3d_denoise_rgb_device)."""
     import torch
     ctx = ctx or context()
-    o = _opt.resolve_opts(opts)
     I = np.asarray(I, dtype=np.float64)
     m, n, _ = I.shape
+    o = _opt.resolve_opts(opts, shape=(m, n), sigma=sigma)
     planes = [torch.from_numpy(np.asfortranarray(I[:, :, k]).ravel(order="F").copy()).cuda() for k in range(3)]
     outs = [torch.empty_like(p) for p in planes]
     co = c_opts(o)

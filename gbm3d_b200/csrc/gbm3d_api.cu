@@ -40,7 +40,7 @@ struct gbm3d_ctx {
   std::vector<cudaEvent_t> kpool;
   std::vector<std::string> krec;
   int launches = 0;
-  int form = 0;         // 0 plain, 1 precision form, 2 learned pilot (set from the current call's options)
+  int form = 0;         // 0 plain, 1 precision, 2 learned pilot, 3 tensor-core matching (current call's options)
   bool pilot_ready = false;  // pilot parameters loaded (gbm3d_pilot_set_params)
   // the last batch captured as one CUDA graph, and the geometry it was captured for
   std::string graph_key;
@@ -412,7 +412,8 @@ void check_opts(gbm3d_ctx* c, const gbm3d_opts* o) {
   if (o->filtType != 0 && o->filtType != 1) argfail(c, "unrecognized filtering");  // denoiseAndAggregateGPU.m:54
   if (o->wavelet < 0 || o->wavelet > 2)
     argfail(c, "wavelet must be 0 (bior1.5 x Haar), 1 (3D Haar) or 2 (sym4 x Haar)");
-  if (o->form < 0 || o->form > 2) argfail(c, "form must be 0 (plain), 1 (precision) or 2 (learned pilot)");
+  if (o->form < 0 || o->form > 3)
+    argfail(c, "form must be 0 (plain), 1 (precision), 2 (learned pilot) or 3 (tensor-core matching)");
   if (o->form == 2 && !c->pilot_ready) argfail(c, "learned pilot: no parameters loaded (gbm3d_pilot_set_params)");
   c->form = o->form;
 }
@@ -485,14 +486,24 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
   A.V1 = V1;
   A.V2 = V2;
   A.err = c->flag;
-  if (form == 1) {
-    // precision form: the V1/V2 gathers of matchBlocksWie are not produced by
-    // the tensor-core matcher, so that entry point keeps the plain search
+  A.R = m + d2;
+  A.Q = n + d2;
+  if (form == 1 || form == 3) {
+    // tensor-core distances (precision and tensor forms): the V1/V2 gathers of
+    // matchBlocksWie are not produced by the tensor-core matcher, so that
+    // entry point keeps the exhaustive search (with the same match sets)
     if (!match_tc_supported(d, d2, s, K, A.tol_branch != 0))
-      argfail(c, "precision form needs blockSize 8, numMin = numMax <= 16 and refStride <= 4",
-              GBM3D_ERR_UNSUPPORTED);
+      argfail(c, "tensor-core matching needs blockSize 8, numMin = numMax <= 16, refStride <= 8 and "
+                 "3 refStride + matchSize <= 56", GBM3D_ERR_UNSUPPORTED);
     if (!V1 && !V2 && !img2) {
+      A.ovf_list = buf<int>(c, "mtc.ovf", (size_t)A.M * A.N);
+      A.ovf_count = buf<int>(c, "mtc.novf", 1);
       launched(c, launch_match_tc(d, d2, A, c->st), "match_tc");
+      // references whose candidate list overflowed: the exhaustive search
+      MatchArgs L = A;
+      L.list = A.ovf_list;
+      L.list_count = A.ovf_count;
+      launched(c, launch_match_list(d, d2, L, c->st), "match_redo");
       return;
     }
   }

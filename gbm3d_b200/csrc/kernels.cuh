@@ -20,7 +20,15 @@ struct MatchArgs {
   int m, n;           // volume rows/cols: the image for s = d, (M d) x (N d) otherwise
   float* V1;          // d x d x K x M x N gathers (may be null)
   float* V2;
-  int* err;           // set to 1 by the tensor-core matcher when an MMA wait times out (may be null)
+  int* err;           // bit 1 set by the tensor-core matcher when a wait times out (may be null)
+  int R, Q;           // rows and columns of the search image (m + d2, n + d2)
+  // tensor-core matcher: references whose candidate set overflowed its list
+  // are appended here (count first zeroed) and searched exhaustively after it
+  int* ovf_list;
+  int* ovf_count;
+  // list mode of the exhaustive matcher: only the references list[0 .. *list_count)
+  const int* list;
+  const int* list_count;
 };
 bool match_supported(int d, int d2);
 size_t match_smem_bytes(int d, int d2);
@@ -29,8 +37,14 @@ cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, fl
                             cudaStream_t st);
 cudaError_t launch_gather_volume(const float* pad, int P, int M, int N, int s, int d, int d2, int K, const uint32_t* S,
                                  const int32_t* cnt, float* vol, cudaStream_t st);
-// Precision form (match_tc.cu): bf16 tensor-core distances, exact FP32 re-rank
-// of the 32 best; top-K branch only (numMin = numMax), d = 8, stride <= 4.
+// The exhaustive matcher on the references A.list[0 .. *A.list_count) only
+// (grid-stride over the list; the count is read on the device).
+cudaError_t launch_match_list(int d, int d2, const MatchArgs& A, cudaStream_t st);
+// Tensor-core matcher (match_tc.cu): bf16 tensor-core distances bound the
+// candidates, exact FP32 re-rank in the exhaustive matcher's operation order,
+// so the match sets equal its own.  Top-K branch only (numMin = numMax),
+// d = 8, K <= 16, stride 1..8.  References whose candidate list overflows go
+// to A.ovf_list; launch_match_list(A with list = ovf_list) finishes them.
 bool match_tc_supported(int d, int d2, int s, int K, bool tol_branch);
 cudaError_t launch_match_tc(int d, int d2, const MatchArgs& A, cudaStream_t st);
 

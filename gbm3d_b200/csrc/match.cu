@@ -13,6 +13,8 @@
 // smallest (distance, column-major window index) pairs — the stable order of
 // MATLAB's mink — found by a bitwise radix search for the K-th smallest
 // distance with warp reductions, then an index-ordered pick among ties.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -62,16 +64,13 @@ __global__ void k_make_pad(const float* __restrict__ img, int m, int n, int h, i
   pad[y + (size_t)x * P] = img[src(y, m) + (size_t)src(x, n) * m];
 }
 
+// The search of reference g by one warp: win holds (D + D2 - 1)^2 floats of
+// shared memory, lst 224 words (keys, indices, S and the bounded set).
 template <int D, int D2>
-__global__ void __launch_bounds__(128) k_match(MatchArgs A) {
+__device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float* win, uint32_t* lst,
+                                          const int lane) {
   constexpr int WD = D + D2 - 1;  // window rows/cols that candidates touch
   constexpr int H = D2 / 2;
-  extern __shared__ float smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* win = smem + warp * (WD * WD);
-  uint32_t* lst = reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 224;  // keys, idx, S, bounded set
-  const int g = blockIdx.x * 4 + warp;
-  if (g >= A.M * A.N) return;  // warp-uniform
   const int i = g % A.M, j = g / A.M;
 
   // ---- stage the search window (column-major, stride WD) --------------------
@@ -320,6 +319,32 @@ __global__ void __launch_bounds__(128) k_match(MatchArgs A) {
   }
 }
 
+template <int D, int D2>
+__global__ void __launch_bounds__(128) k_match(MatchArgs A) {
+  constexpr int WD = D + D2 - 1;
+  extern __shared__ float smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * 4 + warp;
+  if (g >= A.M * A.N) return;  // warp-uniform
+  match_ref<D, D2>(A, g, smem + warp * (WD * WD), reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 224, lane);
+}
+
+// List mode: the references A.list[0 .. *A.list_count), grid-stride over the list.
+template <int D, int D2>
+__global__ void __launch_bounds__(128) k_match_list(MatchArgs A) {
+  constexpr int WD = D + D2 - 1;
+  extern __shared__ float smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* win = smem + warp * (WD * WD);
+  uint32_t* lst = reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 224;
+  const int n = *A.list_count;
+  for (int t = blockIdx.x * 4 + warp; t < n; t += gridDim.x * 4) {
+    const int g = A.list[t];
+    if ((unsigned)g < (unsigned)(A.M * A.N)) match_ref<D, D2>(A, g, win, lst, lane);
+    __syncwarp();  // the next reference restages win and lst
+  }
+}
+
 size_t match_smem_bytes(int d, int d2) {
   const int wd = d + d2 - 1;
   return (size_t)4 * wd * wd * sizeof(float) + 4 * 224 * sizeof(uint32_t);
@@ -337,6 +362,27 @@ static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   const int G = A.M * A.N;
   k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(A);
   return cudaGetLastError();
+}
+
+template <int D, int D2>
+static cudaError_t launch_match_list_t(const MatchArgs& A, cudaStream_t st) {
+  const size_t sm = match_smem_bytes(D, D2);
+  cudaError_t e = cudaFuncSetAttribute(k_match_list<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const int G = A.M * A.N;
+  // enough warps for the rare references a list holds; the rest exit at once
+  const int blocks = std::min((G + 3) / 4, 2 * 148);
+  k_match_list<D, D2><<<blocks, 128, sm, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_match_list(int d, int d2, const MatchArgs& A, cudaStream_t st) {
+  if (A.s < 1 || A.s > d || !A.list || !A.list_count) return cudaErrorInvalidValue;
+#define GBM3D_MATCHL_CASE(DD, DD2) \
+  if (d == DD && d2 == DD2) return launch_match_list_t<DD, DD2>(A, st);
+  GBM3D_MATCHL_CASE(8, 16) GBM3D_MATCHL_CASE(8, 24) GBM3D_MATCHL_CASE(8, 32)
+#undef GBM3D_MATCHL_CASE
+  return cudaErrorInvalidValue;
 }
 
 bool match_supported(int d, int d2) {

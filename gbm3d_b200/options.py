@@ -19,6 +19,9 @@ reference but GBM3D.m ignores it (it always uses bior1.5 x Haar); here
 """
 from __future__ import annotations
 
+import json
+import os
+
 import numpy as np
 
 PROFILES = ("default", "fast", "superFast", "accuracy")
@@ -66,13 +69,56 @@ def checkBM3Dopts(opts: dict | None) -> dict:
     return o
 
 
-def resolve_opts(opts: dict | None) -> dict:
-    """GBM3D.m:15-19: a 'profile' field replaces every other field."""
+TUNED_SETS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_sets.json")
+# the dense configuration the tuned sets are measured against (and the set for
+# images below the smallest calibrated size)
+DENSE = dict(blockSize=8, blockSizeWie=8, matchSize=32, numMax=16, numMin=16, refStride=3, refStrideWie=3,
+             matchSpins=[0, 4], matchSpinsWie=[0, 4], cycleSpin=2, form="plain")
+
+
+def tuned_opts(m: int, n: int, sigma: float, table: dict | None = None) -> dict:
+    """Options of the 'tuned' profile for an m x n image at noise level sigma:
+    the autotuner's set for the largest calibrated size class not above
+    min(m, n) and the calibrated sigma nearest in log scale
+    (gbm3d_b200/tuned_sets.json, written by ``python -m gbm3d_b200.autotune
+    --classes``).  Each set stayed within 0.05 dB (less a 0.02 dB margin) of
+    the dense configuration on its calibration images; below the smallest
+    class the dense configuration itself is returned.  Not in the reference."""
+    if table is None:
+        with open(TUNED_SETS) as f:
+            table = json.load(f)
+    side = min(int(m), int(n))
+    sizes = sorted({c["size"] for c in table["classes"]})
+    fit = [z for z in sizes if z <= side]
+    o = setBM3Dopts("default")
+    o.update(DENSE)
+    if not fit:
+        return o
+    size = fit[-1]
+    rows = [c for c in table["classes"] if c["size"] == size]
+    sg = max(float(sigma), 1e-6)
+    row = min(rows, key=lambda c: (abs(np.log(c["sigma"] / sg)), c["sigma"]))
+    o.update(row["opts"])
+    return o
+
+
+def resolve_opts(opts: dict | None, shape=None, sigma=None) -> dict:
+    """GBM3D.m:15-19: a 'profile' field replaces every other field.  The
+    'tuned' profile (not in the reference) depends on the image: it needs
+    ``shape`` (m, n) and ``sigma`` and reads tuned_opts()."""
     if opts is None:
         opts = {"profile": "default"}
     if "profile" in opts:
         extra = {k: opts[k] for k in ("refStride", "refStrideWie", "staleWeights") if k in opts}
-        o = setBM3Dopts(opts["profile"])
+        if opts["profile"] == "tuned":
+            if shape is None or sigma is None:
+                raise ValueError("the 'tuned' profile needs the image size and sigma")
+            o = tuned_opts(shape[0], shape[1], float(np.mean(np.sqrt(np.asarray(sigma, float))))
+                           if np.ndim(sigma) >= 1 and np.size(sigma) > 1 else float(np.ravel(sigma)[0]))
+            if "form" in opts:
+                o["form"] = opts["form"]
+        else:
+            o = setBM3Dopts(opts["profile"])
         o.update(extra)
         opts = o
     return checkBM3Dopts(opts)

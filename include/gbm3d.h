@@ -64,10 +64,14 @@ typedef struct gbm3d_opts {
   int refStrideWie;
   int wavelet; /* step-1 bank of gbm3d_denoise: 0 = bior1.5 x Haar (GBM3D.m:40), 1 = 3D Haar */
   /* 0 plain (the reference's arithmetic, FP32); 1 precision form: block
-   * distances on the bf16 tensor cores with an exact FP32 re-rank of the 32
-   * best per reference, and Kahan-compensated FP32 aggregation; 2 learned
-   * pilot: the step-1 estimate comes from the pilot network (gbm3d_pilot_*).
-   * Not in the reference. */
+   * distances on the bf16 tensor cores bound the candidates (every position
+   * within the rounding bound of the K-th best), which are re-ranked by the
+   * exact FP32 distance, so the match sets are the plain path's; aggregation
+   * with Kahan-compensated FP32 sums; 2 learned pilot: the step-1 estimate
+   * comes from the pilot network (gbm3d_pilot_*); 3 tensor form: the
+   * precision form's matching with the plain aggregation, so the output is
+   * the plain path's.  Tensor-core matching needs blockSize 8, numMin =
+   * numMax <= 16 and 3 refStride + matchSize <= 56.  Not in the reference. */
   int form;
   /* video (gbm3d_vbm3d_device, gbm3d_matchBlocksV): frames in the temporal
    * window, odd; 0 means VBM3D.m's default of 11.  opts.wavelet = 2 selects

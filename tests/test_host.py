@@ -174,3 +174,25 @@ def test_autotune_select_rule():
     assert autotune.select(rows, 0.05, 0.04)["opts"] == {"refStride": 4}
     assert autotune.select(rows, 0.2, 0.0)["opts"] == {"refStride": 8}
     assert autotune.select(rows[:1], 0.05)["baseline"]
+
+
+def test_tuned_profile_lookup():
+    """The 'tuned' profile: the largest calibrated size class not above the
+    image's smaller side, the sigma class nearest in log scale, the dense
+    configuration below the smallest class."""
+    from gbm3d_b200 import options
+    table = {"classes": [
+        {"size": 512, "sigma": 10.0, "opts": {"refStride": 6, "refStrideWie": 4}},
+        {"size": 512, "sigma": 25.0, "opts": {"refStride": 6, "refStrideWie": 5}},
+        {"size": 2048, "sigma": 25.0, "opts": {"refStride": 8, "refStrideWie": 6, "form": "tensor"}},
+        {"size": 2048, "sigma": 50.0, "opts": {"refStride": 8, "refStrideWie": 7}}]}
+    o = options.tuned_opts(600, 700, 12.0, table)
+    assert (o["refStride"], o["refStrideWie"]) == (6, 4)
+    o = options.tuned_opts(4096, 3000, 26.0, table)
+    assert (o["refStride"], o["refStrideWie"], o["form"]) == (8, 6, "tensor")
+    o = options.tuned_opts(4096, 4096, 40.0, table)
+    assert (o["refStride"], o["refStrideWie"]) == (8, 7)
+    o = options.tuned_opts(300, 4096, 25.0, table)  # below every class: the dense configuration
+    assert (o["refStride"], o["refStrideWie"], o["cycleSpin"], o["matchSpins"]) == (3, 3, 2, [0, 4])
+    with pytest.raises(ValueError):
+        options.resolve_opts({"profile": "tuned"})
