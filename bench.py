@@ -50,8 +50,25 @@ WL = "dense"
 STAGES = ["glue", "match1", "wavelet1", "agg1", "match2", "wiener2", "agg2", "total"]
 # arithmetic of each form: plain FP32; precision: bf16 tensor-core distances (+ exact FP32 re-rank)
 FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32", "tuned": "f32"}
-FAMILIES = ["match", "match_tc", "wav_analysis", "wav_synthesis", "aggregate", "wiener", "ht_weights", "make_pad",
+# a tuned set that takes tensor-core matching computes its distances' bound in bf16
+TUNED_DTYPE = {"plain": "f32", "tensor": "bf16+f32", "precision": "bf16+f32", "learned": "bf16+f32"}
+FAMILIES = ["match", "match_tc", "match_redo", "wav_analysis", "wav_synthesis", "aggregate", "wiener", "ht_weights", "make_pad",
             "accum", "ratio", "prep", "medfilt3"]
+
+
+def describe(o: dict, name: str) -> str:
+    """The timed option set in words (the line's config.workload)."""
+    from gbm3d_b200 import options as _opt
+    s1, s2 = _opt.strides(o)
+    matcher = {"plain": "exhaustive FP32 matching", "tensor": "tensor-core matching (bf16 distance bound, exact "
+               "FP32 re-rank: the exhaustive matcher's match sets)", "precision": "tensor-core matching and "
+               "Kahan-compensated aggregation", "learned": "learned pilot in place of step 1"}[o.get("form", "plain")]
+    wav = "3D Haar" if o.get("wname") == "haar" else "bior1.5 x Haar"
+    return (f"{name}: 2-step GBM3D, patch {o['blockSize']}/{o['blockSizeWie']}, reference stride {s1}/{s2}, group "
+            f"{o['numMax']}, search +-{o['matchSize'] // 2} (matchSize {o['matchSize']}), {wav} "
+            f"{o['levels']} levels, {o['cycleSpin']} cycle spin{'s' if o['cycleSpin'] > 1 else ''}, match spins "
+            f"{list(o['matchSpins'])} + {list(o['matchSpinsWie'])}, {matcher}; one {SIZE}x{SIZE} synthetic image, "
+            f"sigma {SIGMA:g}, float64 in/out")
 
 
 def opts() -> dict:
@@ -61,8 +78,8 @@ def opts() -> dict:
     return o
 
 
-def _config(extra=None):
-    c = {"workload": WORKLOADS[WL][0].format(n=SIZE), "name": WL, "image": [SIZE, SIZE], "sigma": SIGMA,
+def _config(extra=None, workload=None):
+    c = {"workload": workload or WORKLOADS[WL][0].format(n=SIZE), "name": WL, "image": [SIZE, SIZE], "sigma": SIGMA,
          "parallelism": "replicas: one image per GPU",
          "l2": "inputs larger than L2: each step streams tens of GB of intermediates through HBM"}
     if extra:
@@ -325,6 +342,73 @@ def cpu_baseline(o_chosen=None, size: int = 512):
     return base, parity
 
 
+def quality_by_size(ctx, fresh=None, sizes=(512, 1024, 2048, 4096)):
+    """PSNR of the 'tuned' profile's set against the dense plain configuration
+    on seeded images of each size class (seeds not used in calibration), sigma
+    25.  With a fresh autotune result, that one set is checked at every size."""
+    from gbm3d_b200 import api, synth
+    from gbm3d_b200 import options as _opt
+    out = []
+    for sz in sizes:
+        clean, noisy = synth.noisy_image(sz, sz, SIGMA, seed=7000 + sz)
+        dense = opts()
+        tuned = dict(dense, **fresh["opts"]) if fresh else _opt.resolve_opts({"profile": "tuned"}, shape=(sz, sz),
+                                                                               sigma=SIGMA)
+        Ud, _ = api.GBM3D(noisy, SIGMA, dense, ctx=ctx)
+        Ut, _ = api.GBM3D(noisy, SIGMA, tuned, ctx=ctx)
+        pd, pt = float(_opt.myPSNR(clean, Ud, 255)), float(_opt.myPSNR(clean, Ut, 255))
+        out.append({"size": sz, "seed": 7000 + sz, "psnr_dense_db": pd, "psnr_tuned_db": pt, "delta_db": pt - pd,
+                    "within_0.05dB": pt >= pd - 0.05, "tuned_opts": {k: tuned[k] for k in (
+                        "refStride", "refStrideWie", "matchSpins", "matchSpinsWie", "cycleSpin", "form")}})
+    return out
+
+
+def learned_pilot_block(ctx, sigmas=(15.0, 25.0, 50.0), reps=3):
+    """The learned-pilot form on 4096^2 images at several noise levels: the
+    per-image gate's decision (fallback rate), PSNR against the clean image of
+    the network-pilot 2-step result, of the plain 2-step method and of what
+    the gate delivers, and MPix/s of the network-pilot path (device time of
+    the library's stages, CUDA events) and of the gate."""
+    import torch
+    from gbm3d_b200 import api, pilot, synth
+    from gbm3d_b200 import options as _opt
+    rows = []
+    dev = torch.device("cuda", ctx.device)
+    for sg in sigmas:
+        clean, noisy = synth.noisy_image(SIZE, SIZE, sg, seed=8000 + int(sg))
+        o = opts()
+        t0 = time.perf_counter()
+        g = pilot.gate(noisy, sg, o, ctx=ctx)
+        gate_ms = (time.perf_counter() - t0) * 1e3
+        Up, _ = api.GBM3D(noisy, sg, dict(o, form="plain"), ctx=ctx)
+        Ul, _ = api.GBM3D(noisy, sg, dict(o, form="learned"), ctx=ctx)
+        dI = torch.from_numpy(np.asfortranarray(noisy).ravel(order="F")).to(dev)
+        dU = torch.empty_like(dI)
+        times = {}
+        for f in ("learned", "plain"):
+            api.GBM3D_device(dI.data_ptr(), SIZE, SIZE, sg, dU.data_ptr(), dict(o, form=f), ctx=ctx)
+            ctx.synchronize()
+            ctx.enable_timing(True)
+            ts = []
+            for _ in range(reps):
+                api.GBM3D_device(dI.data_ptr(), SIZE, SIZE, sg, dU.data_ptr(), dict(o, form=f), ctx=ctx)
+                ctx.synchronize()
+                ts.append(ctx.stage_times()[7])
+            ctx.enable_timing(False)
+            times[f] = float(np.median(ts))
+        pl, pp = float(_opt.myPSNR(clean, Ul, 255)), float(_opt.myPSNR(clean, Up, 255))
+        rows.append({"sigma": sg, "seed": 8000 + int(sg), "fallback": bool(g["fallback"]),
+                     "gate_gap_db": g["gap_db"], "psnr_learned_db": pl, "psnr_plain_db": pp,
+                     "psnr_delivered_db": pp if g["fallback"] else pl,
+                     "mpix_s_learned": SIZE * SIZE / 1e6 / (times["learned"] / 1e3),
+                     "mpix_s_plain": SIZE * SIZE / 1e6 / (times["plain"] / 1e3),
+                     "mpix_s_delivered": SIZE * SIZE / 1e6 / (((times["plain"] if g["fallback"] else times["learned"])
+                                                               + gate_ms) / 1e3),
+                     "ms_learned": times["learned"], "ms_plain": times["plain"], "gate_ms": gate_ms})
+    return {"image": [SIZE, SIZE], "configuration": "dense (stride 3) Wiener step on the network's pilot",
+            "fallback_rate": float(np.mean([r["fallback"] for r in rows])), "rows": rows}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -344,16 +428,76 @@ def run_reference(args):
         times.append(time.perf_counter() - t0)
     per = sum(times) / len(times)
     v = size * size / 1e6 / per
+    # ms_per_step is the time of the step actually timed: one size x size crop
+    # of the workload (a whole 4096^2 image would take the CPU minutes); the
+    # rate, MPix/s, is the comparable figure
     line = {"metric": METRIC, "value": v, "unit": "MPix/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": per * 1e3 * (SIZE * SIZE) / (size * size),
+            "warmup": args.warmup, "ms_per_step": per * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": _config({"sample": f"{size}x{size} crop per step"}),
+            "config": _config({"sample": f"{size}x{size} crop per step (ms_per_step is per crop)",
+                               "ms_per_full_image_extrapolated": per * 1e3 * (SIZE * SIZE) / (size * size)}),
             "cpu_baseline": {"value": v, "unit": "MPix/s", "cores": O.num_threads(), "kind": "port",
                              "sample": f"{size}x{size} crop of the {SIZE}^2 synthetic workload per step, "
                                        "FP32 CPU restatement of the reference path, OpenMP on all host threads"},
             "e2e": {"value": v, "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def batched_block(ctx, stream, work, reps=3):
+    """The batched form's mixed submission (64 grey images of uneven sizes
+    and noise levels, 8 RGB 1024^2 images, a 32-frame 1280x720 video) through
+    gbm3d_denoise_mixed: eager launches and one captured CUDA graph, device
+    time per submission (CUDA events), MPix/s.  Grey and colour images use the
+    'tuned' profile's set of the smallest size class (the most conservative
+    one for a batch of uneven sizes), the video VBM3D.m's defaults with a
+    3-frame window."""
+    import torch
+    from gbm3d_b200 import api, options as _opt
+    grey_pairs, gs, rgb, rs, frames, vs = work
+    grey = [p[1] for p in grey_pairs]
+    dev = torch.device("cuda", ctx.device)
+    o = _opt.resolve_opts({"profile": "tuned"}, shape=(512, 512), sigma=SIGMA) \
+        if os.path.exists(_opt.TUNED_SETS) else opts()
+
+    def col(x):
+        return torch.from_numpy(np.asfortranarray(x).ravel(order="F").copy()).to(dev)
+
+    dg = [col(x).view(x.shape[1], x.shape[0]) for x in grey]
+    dr = [tuple(col(x[:, :, q]).view(x.shape[1], x.shape[0]) for q in range(3)) for x in rgb]
+    dv = col(frames).view(frames.shape[2], frames.shape[1], frames.shape[0])
+    mpix = (sum(x.shape[0] * x.shape[1] for x in grey) + sum(3 * x.shape[0] * x.shape[1] for x in rgb)
+            + frames.shape[0] * frames.shape[1] * (frames.shape[2] - 2)) / 1e6
+    vo = {"nF": 3}
+
+    def timed(use_graph):
+        outs = api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, use_graph=use_graph, ctx=ctx)  # warm-up / capture
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, use_graph=use_graph, ctx=ctx, outputs=outs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, ctx.launch_count(), outs
+
+    eager_ms, eager_launches, outs = timed(False)
+    ref = [u.cpu().numpy().copy() for u in outs[0]]
+    graph_ms, graph_launches, outs = timed(True)
+    same = all(np.array_equal(r, u.cpu().numpy()) for r, u in zip(ref, outs[0]))
+    gains = []
+    for k, (clean, x) in enumerate(grey_pairs):
+        U = outs[0][k].cpu().numpy().reshape(-1).reshape(x.shape, order="F")
+        gains.append(float(_opt.myPSNR(clean, U, 255) - _opt.myPSNR(clean, x, 255)))
+    return {"workload": "64 grey (200x300 .. 2048x1536, sigma 5-50) + 8 RGB 1024^2 (opponent colour, luma "
+                        "matching) + 32-frame 1280x720 video (+-1 frame), one gbm3d_denoise_mixed submission",
+            "megapixels": mpix, "opts": {k: o[k] for k in ("refStride", "refStrideWie", "matchSize", "matchSpins",
+                                                           "matchSpinsWie", "cycleSpin", "form")},
+            "eager_ms": eager_ms, "graph_ms": graph_ms, "value": mpix / (min(eager_ms, graph_ms) / 1e3),
+            "unit": "MPix/s", "eager_mpix_s": mpix / (eager_ms / 1e3), "graph_mpix_s": mpix / (graph_ms / 1e3),
+            "launches_eager": eager_launches, "graph_launches_per_call": graph_launches,
+            "graph_equals_eager": same, "grey_psnr_gain_db_min": min(gains), "grey_psnr_gain_db_mean": float(
+                np.mean(gains))}
 
 
 def run_ours(args):
@@ -444,12 +588,19 @@ def run_ours(args):
     form_opts = {f: dict(o_plain, form=f) for f in forms if f != "tuned"}
     tuning = None
     if "tuned" in forms:
-        # the autotuner searches strides, spin schedule, cycle spins and search
-        # size on its own calibration image (same size, another seed); the
+        # the 'tuned' profile: the autotuner's calibrated set for this size and
+        # sigma (gbm3d_b200/tuned_sets.json, calibrated on other seeds), or with
+        # --autotune a fresh search on a calibration image of this size; the
         # bench image only checks the result
         from gbm3d_b200 import autotune
         if args.tuned_opts:  # a known result (profiling runs): no search
             form_opts["tuned"] = dict(o_plain, **{**autotune.BASELINE, **json.loads(args.tuned_opts)})
+        elif not args.autotune and os.path.exists(_opt.TUNED_SETS):
+            form_opts["tuned"] = _opt.resolve_opts({"profile": "tuned"}, shape=(SIZE, SIZE), sigma=SIGMA)
+            tuning = {"source": "gbm3d_b200/tuned_sets.json (python -m gbm3d_b200.autotune --classes)",
+                      "opts": {k: form_opts["tuned"][k] for k in (
+                          "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin",
+                          "form")}}
         else:
             if rank == 0:
                 tuning = autotune.tune(size=SIZE, sigma=SIGMA, ctx=ctx, log=None)
@@ -534,15 +685,17 @@ def run_ours(args):
     roof, work = roofline(o, ktimes, peaks, sm_mhz)
     line = {"metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": FORM_DTYPE[form], "data": "synthetic",
+            "vs_baseline": None, "dtype": TUNED_DTYPE[o.get("form", "plain")] if form == "tuned" else FORM_DTYPE[form],
+            "data": "synthetic",
             "config": _config({"form": form, "form_opts": {k: o[k] for k in (
-                "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin", "form")}}),
-            "autotune": None if tuning is None else {
+                "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin", "form")},
+                "plain_workload": WORKLOADS[WL][0].format(n=SIZE)}, workload=describe(o, form)),
+            "autotune": None if tuning is None else (tuning if "source" in tuning else {
                 k: tuning[k] for k in ("opts", "size", "sigma", "seed", "budget_db", "margin_db", "evaluated",
                                        "timed", "seconds")} | {
                 "calibration_psnr_db": tuning["chosen"]["psnr"], "calibration_baseline_psnr_db":
                     tuning["baseline"]["psnr"], "calibration_ms": tuning["chosen"]["ms"],
-                "calibration_baseline_ms": tuning["baseline"]["ms"]},
+                "calibration_baseline_ms": tuning["baseline"]["ms"]}),
             "forms": {f: {"value": world * mpix / (r["ms"] / 1e3), "unit": "MPix/s", "ms_per_step": r["ms"],
                           "psnr_db": r["psnr"], "stages_ms": dict(zip(STAGES, r["stages"])),
                           "gate": r.get("gate"),
@@ -568,6 +721,12 @@ def run_ours(args):
             "kernels_ms": {f: {"launches": n, "ms": t} for f, (n, t) in ktimes.items()},
             "roofline": roof,
             "roofline_all": work}
+    if rank == 0 and getattr(args, "mixed_work", None) is not None:
+        line["batched"] = batched_block(ctx, stream, args.mixed_work)
+    if rank == 0 and have_pilot and args.form == "auto":
+        line["learned_pilot"] = learned_pilot_block(ctx)
+    if rank == 0 and "tuned" in res and not args.tuned_opts:
+        line["quality_by_size"] = quality_by_size(ctx, args.autotune and tuning)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"], line["parity"] = cpu_baseline(o, args.cpu_size)
     if world > 1:
@@ -592,6 +751,9 @@ def main():
     ap.add_argument("--form", default="auto", choices=["auto"] + sorted(FORM_DTYPE),
                     help="the form timed for `value` (auto: the fastest within 0.05 dB of plain); "
                          "the plain path is timed beside it")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched form's mixed submission")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the autotuner at this size instead of reading the calibrated 'tuned' profile")
     ap.add_argument("--tuned-opts", default=None,
                     help="JSON option overrides used as the tuned form instead of running the autotuner")
     args = ap.parse_args()
@@ -599,6 +761,12 @@ def main():
     if args.impl == "reference":
         run_reference(args)
     else:
+        args.mixed_work = None
+        if not args.no_batched and int(os.environ.get("RANK", "0")) == 0 and args.form == "auto":
+            # the batched form's workload is generated by a spawned process pool,
+            # before any CUDA work in this process
+            from gbm3d_b200 import mixed
+            args.mixed_work = mixed.workload()
         run_ours(args)
 
 

@@ -87,6 +87,7 @@ _SIGS = {
     "gbm3d_kernel_time": (C.c_int, [_P, C.c_char_p, _P]),
     "gbm3d_filters_from_bank": (C.c_int, [_P, _P, C.c_int, C.c_int, C.POINTER(gbm3d_filters)]),
     "gbm3d_tc_selfcheck": (C.c_int, [_P, _P, _P, _P]),
+    "gbm3d_tc_selfcheck_layout": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "gbm3d_ctx_synchronize": (C.c_int, [_P]),
     "gbm3d_denoise_rgb_device": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts),
                                            _P, _P, _P]),

@@ -1308,6 +1308,10 @@ int gbm3d_denoiseAndAggregateWie(gbm3d_ctx* c, const float* V1, const float* V2,
 }
 
 int gbm3d_tc_selfcheck(gbm3d_ctx* c, const uint16_t* A, const uint16_t* B, float* C) {
+  return gbm3d_tc_selfcheck_layout(c, 0, A, B, C);
+}
+
+int gbm3d_tc_selfcheck_layout(gbm3d_ctx* c, int mn_major, const uint16_t* A, const uint16_t* B, float* C) {
   return guarded(c, [&] {
     if (!A || !B || !C) argfail(c, "missing argument");
     uint16_t* dA = buf<uint16_t>(c, "tc.A", 128 * 64);
@@ -1316,7 +1320,10 @@ int gbm3d_tc_selfcheck(gbm3d_ctx* c, const uint16_t* A, const uint16_t* B, float
     ck(c, cudaMemcpyAsync(dA, A, 128 * 64 * 2, cudaMemcpyHostToDevice, c->st), "H2D");
     ck(c, cudaMemcpyAsync(dB, B, 256 * 64 * 2, cudaMemcpyHostToDevice, c->st), "H2D");
     ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
-    launched(c, launch_tc_gemm_check(dA, dB, dC, c->flag, c->st), "tc_gemm_check");
+    if (mn_major)
+      launched(c, launch_tc_gemm_check_mn(dA, dB, dC, c->flag, c->st), "tc_gemm_check");
+    else
+      launched(c, launch_tc_gemm_check(dA, dB, dC, c->flag, c->st), "tc_gemm_check");
     ck(c, cudaMemcpyAsync(C, dC, 128 * 256 * 4, cudaMemcpyDeviceToHost, c->st), "D2H");
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");

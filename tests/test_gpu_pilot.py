@@ -97,3 +97,43 @@ def test_pilot_deterministic(gpu):
     a, _ = pilot.train(steps=5, batch=4, data=data, log=None)
     b, _ = pilot.train(steps=5, batch=4, data=data, log=None)
     assert np.array_equal(a, b)
+
+
+def _wiener_on(pilot_img, noisy, sigma, o):
+    """Step 2 alone (matchBlocksWie + denoiseAndAggregateWieFast, one spin)
+    with the given image as its pilot: the method without a step-1 estimate
+    when the pilot is the noisy image itself."""
+    from gbm3d_b200 import api
+    S, V1, V2 = api.matchBlocksWie(pilot_img, noisy, sigma, o)
+    U, W = api.denoiseAndAggregateWieFast(V1, V2, S, sigma, o)
+    return U / W
+
+
+@pytest.mark.parametrize("sigma,seed", [(15.0, 61), (25.0, 62), (50.0, 63)])
+def test_trained_pilot_gains(gpu, sigma, seed):
+    """What the trained network adds, on a 512^2 image: the 2-step result with
+    its pilot against (a) Wiener filtering with the noisy image as the pilot
+    (no step-1 estimate at all) and (b) the same network untrained."""
+    import time
+    from gbm3d_b200 import api, options, pilot, synth
+    if not os.path.exists(pilot.WEIGHTS):
+        pytest.skip("no trained weights")
+    clean, noisy = synth.noisy_image(512, 512, sigma, seed=seed)
+    o = pilot.dense_opts(refStrideWie=8, matchSpinsWie=[0])
+    pilot.load()
+    t0 = time.perf_counter()
+    Ul, outl = api.GBM3D(noisy, sigma, dict(o, form="learned"))
+    t_learned = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Un = _wiener_on(noisy, noisy, sigma, dict(o, form="plain"))
+    t_nopilot = time.perf_counter() - t0
+    pilot.set_params(pilot.init_params(0))
+    Uu, _ = api.GBM3D(noisy, sigma, dict(o, form="learned"))
+    pilot.load()
+    pl, pn, pu = (options.myPSNR(clean, U, 255) for U in (Ul, Un, Uu))
+    p1 = options.myPSNR(clean, outl["U1"], 255)
+    print(f"sigma {sigma:g}: learned pilot {pl:.3f} dB (its step-1 estimate {p1:.3f} dB, {t_learned * 1e3:.0f} ms), "
+          f"Wiener on the noisy pilot {pn:.3f} dB ({t_nopilot * 1e3:.0f} ms), untrained network {pu:.3f} dB, "
+          f"noisy {options.myPSNR(clean, noisy, 255):.3f} dB")
+    assert pl > pn + 1.0, "the trained pilot does not improve on Wiener filtering without one"
+    assert pl > pu + 3.0, "training does not improve the pilot"

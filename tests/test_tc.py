@@ -34,3 +34,19 @@ def test_tcgen05_gemm_layouts(gpu, seed):
     ref = _f32(A).astype(np.float64) @ _f32(B).astype(np.float64).T
     err = np.abs(out - ref).max()
     assert err < 1e-4 * np.abs(ref).max(), f"max error {err}"
+
+
+@pytest.mark.parametrize("mn_major", [0, 1])
+def test_tcgen05_gemm_operand_majors(gpu, mn_major):
+    """K-major and MN-major operand staging give the same exact product."""
+    from gbm3d_b200._lib import context, lib
+    rng = np.random.default_rng(5 + mn_major)
+    A = _bf16(rng.normal(0, 1, (128, 64)))
+    B = _bf16(rng.normal(0, 1, (256, 64)))
+    out = np.zeros((128, 256), dtype=np.float32)
+    ctx = context()
+    ctx.check(lib().gbm3d_tc_selfcheck_layout(ctx.h, mn_major, A.ctypes.data_as(C.c_void_p),
+                                              B.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+    ref = _f32(A).astype(np.float64) @ _f32(B).astype(np.float64).T
+    err = np.abs(out - ref).max()
+    assert err < 1e-4 * np.abs(ref).max(), f"max error {err}"
