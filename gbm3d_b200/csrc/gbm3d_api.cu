@@ -1321,7 +1321,7 @@ int gbm3d_tc_selfcheck_layout(gbm3d_ctx* c, int mn_major, const uint16_t* A, con
     ck(c, cudaMemcpyAsync(dB, B, 256 * 64 * 2, cudaMemcpyHostToDevice, c->st), "H2D");
     ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
     if (mn_major)
-      launched(c, launch_tc_gemm_check_mn(dA, dB, dC, c->flag, c->st), "tc_gemm_check");
+      launched(c, launch_tc_gemm_check_mn(dA, dB, dC, c->flag, mn_major == 2, c->st), "tc_gemm_check");
     else
       launched(c, launch_tc_gemm_check(dA, dB, dC, c->flag, c->st), "tc_gemm_check");
     ck(c, cudaMemcpyAsync(C, dC, 128 * 256 * 4, cudaMemcpyDeviceToHost, c->st), "D2H");

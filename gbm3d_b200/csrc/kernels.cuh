@@ -179,6 +179,7 @@ cudaError_t pilot_adam(float* w, const float* g, float* m1, float* m2, int n, fl
 cudaError_t launch_tc_gemm_check(const uint16_t* A, const uint16_t* B, float* C, int* err, cudaStream_t st);
 // The same product with both operands staged MN-major (the layout the pilot's
 // weight gradient reads activations in).
-cudaError_t launch_tc_gemm_check_mn(const uint16_t* A, const uint16_t* B, float* C, int* err, cudaStream_t st);
+cudaError_t launch_tc_gemm_check_mn(const uint16_t* A, const uint16_t* B, float* C, int* err, int swap_offsets,
+                                    cudaStream_t st);
 
 }  // namespace gbm3d

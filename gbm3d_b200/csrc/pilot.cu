@@ -300,6 +300,147 @@ __global__ void __launch_bounds__(NT) k_dweight(const uint16_t* __restrict__ x, 
   }
 }
 
+// Weight and bias gradients of one layer on the tensor cores.  For tap
+// t = (dy, dx), dW_t[co][ci] = sum_p g[p][co] x[p + (dy-1, dx-1)][ci] is a
+// GEMM with M = co (padded to 128), N = ci and the pixels as K.  A CTA takes
+// tiles of 128 pixels of one row (persistent over tiles, fixed assignment):
+// g's tile and the input rows y-1, y, y+1 (with a one-pixel halo) sit in
+// shared memory in the forward's activation layout (pixel-major inside 8-channel
+// chunks), which read with pixels as K is the MN-major operand layout (core
+// matrix = 8 pixels x 8 channels; K-adjacent cores 128 bytes apart, channel-
+// adjacent ones a chunk apart), and tap dx is the row buffer read from pixel dx
+// (a 16-byte shift).  D of all 9 taps stays in TMEM over the CTA's tiles; the
+// centre tap also multiplies an all-ones channel, which gives the bias
+// gradient.  Each CTA writes its partial sums (bf16 products, fp32
+// accumulation) to part[blockIdx.x]; k_reduce_partials adds them in order, so
+// training stays deterministic.
+constexpr int WG_LBO_G = TP * 16;  // bytes of one 8-channel chunk of the gradient tile
+template <int CI_R, int CO_R, int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_dweight_tc(const uint16_t* __restrict__ x, const uint16_t* __restrict__ g,
+                                                    int nimg, int H, int W, float* __restrict__ part,
+                                                    int* __restrict__ err) {
+  constexpr int XCH = CIN / 8 + 2;           // input chunks + the ones chunk + a zero chunk
+  constexpr int ROWX = XCH * LBO_A;          // bytes of one input row buffer
+  constexpr int NCOL = 9 * CIN + 16;         // TMEM columns of the 9 taps (the centre one is 16 wider)
+  constexpr int TCOLS = NCOL <= 256 ? 256 : 512;
+  constexpr int E = 9 * CO_R * CI_R;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* sG = smem;                  // 16 chunks (M = 128)
+  unsigned char* sX = smem + 16 * WG_LBO_G;  // 3 row buffers
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sX + 3 * ROWX);
+  uint32_t* taddr_s = reinterpret_cast<uint32_t*>(mbar + 1);
+  int* fail_s = reinterpret_cast<int*>(taddr_s + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto col_of = [](int t) { return t <= 4 ? t * CIN : 5 * CIN + 16 + (t - 5) * CIN; };
+
+  if (warp == 0) tc::tmem_alloc(taddr_s, TCOLS);
+  if (tid == 0) {
+    tc::mbar_init(mbar, 1);
+    tc::fence_mbar_init();
+    *fail_s = 0;
+  }
+  // gradient chunks past COUT stay zero (rows co >= COUT of the M = 128 operand)
+  for (int e = tid; e < (16 - COUT / 8) * WG_LBO_G / 16; e += 128)
+    reinterpret_cast<uint4*>(sG + (COUT / 8) * WG_LBO_G)[e] = make_uint4(0, 0, 0, 0);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *taddr_s;
+  const int xt_n = (W + TP - 1) / TP;
+  const int ntiles = nimg * H * xt_n;
+  uint32_t phase = 0;
+  bool any = false;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int xt = tile % xt_n, y = (tile / xt_n) % H, n = tile / (xt_n * H);
+    const int x0 = xt * TP;
+    if (any) {  // the previous tile's MMAs read the buffers about to be rewritten
+      const bool ok = tc::mbar_wait(mbar, phase, PWAIT);
+      phase ^= 1u;
+      if (!ok) *fail_s = 1;
+      tc::fence_after_sync();
+      __syncthreads();
+      if (*fail_s) break;
+    }
+    for (int e = tid; e < TP * (COUT / 8); e += 128) {
+      const int j = e / TP, q = e % TP, xx = x0 + q;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (xx < W) v = *reinterpret_cast<const uint4*>(g + (((size_t)n * H + y) * W + xx) * COUT + 8 * j);
+      *reinterpret_cast<uint4*>(sG + j * WG_LBO_G + q * 16) = v;
+    }
+    for (int e = tid; e < 3 * NPX * XCH; e += 128) {
+      const int r = e / (NPX * XCH), j = (e / NPX) % XCH, q = e % NPX;
+      const int yy = y + r - 1, xx = x0 + q - 1;
+      const bool in = yy >= 0 && yy < H && xx >= 0 && xx < W;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (in && j < CIN / 8) v = *reinterpret_cast<const uint4*>(x + (((size_t)n * H + yy) * W + xx) * CIN + 8 * j);
+      else if (in && j == CIN / 8) v.x = 0x3F80u;  // bf16 1.0 in the first channel of the ones chunk
+      *reinterpret_cast<uint4*>(sX + r * ROWX + j * LBO_A + q * 16) = v;
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0) {
+      const uint32_t ga = tc::smem_u32(sG), xa = tc::smem_u32(sX);
+#pragma unroll 1
+      for (int t = 0; t < 9; ++t) {
+        const int dy = t / 3, dx = t % 3;
+        const uint32_t idesc = tc::idesc_bf16_f32(TP, t == 4 ? CIN + 16 : CIN) | (1u << 15) | (1u << 16);
+#pragma unroll
+        for (int ks = 0; ks < TP / 16; ++ks) {
+          const uint64_t ad = tc::desc_kmajor(ga + ks * 256, 128, WG_LBO_G);
+          const uint64_t bd = tc::desc_kmajor(xa + dy * ROWX + dx * 16 + ks * 256, 128, LBO_A);
+          tc::mma_bf16(tmem + (uint32_t)col_of(t), ad, bd, idesc, (any || ks > 0) ? 1u : 0u);
+        }
+      }
+      tc::commit(mbar);
+    }
+    any = true;
+  }
+  if (any && !*fail_s) {
+    if (!tc::mbar_wait(mbar, phase, PWAIT)) *fail_s = 1;
+    tc::fence_after_sync();
+  }
+  __syncthreads();
+  const bool failed = *fail_s != 0;
+  // ---- partial sums out: thread = co (TMEM lane), 32 columns at a time -------
+  float* out = part + (size_t)blockIdx.x * (E + CO_R);
+  const int co = warp * 32 + lane;
+  for (int c0 = 0; c0 < NCOL; c0 += 32) {
+    float v[32];
+    tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    if (co < CO_R) {
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        const int c = c0 + q;
+        const float val = (any && !failed) ? v[q] : 0.f;
+        int t, ci;
+        if (c < 4 * CIN) { t = c / CIN; ci = c % CIN; }
+        else if (c < 5 * CIN + 16) { t = 4; ci = c - 4 * CIN; }
+        else if (c < NCOL) { t = 5 + (c - 5 * CIN - 16) / CIN; ci = (c - 5 * CIN - 16) % CIN; }
+        else continue;
+        if (ci < CI_R) out[((size_t)t * CO_R + co) * CI_R + ci] = val;
+        else if (t == 4 && ci == CIN) out[E + co] = val;  // the ones channel: bias gradient
+      }
+    }
+  }
+  if (failed && tid == 0 && err) atomicOr(err, 2);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
+}
+
+template <int CI_R, int CO_R, int CIN, int COUT>
+cudaError_t launch_dweight_tc(const uint16_t* x, const uint16_t* g, int nimg, int H, int W, float* part, int grid,
+                              int* err, cudaStream_t st) {
+  const size_t sm = (size_t)16 * WG_LBO_G + (size_t)3 * (CIN / 8 + 2) * LBO_A + 64;
+  cudaError_t e = cudaFuncSetAttribute(k_dweight_tc<CI_R, CO_R, CIN, COUT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k_dweight_tc<CI_R, CO_R, CIN, COUT><<<grid, 128, sm, st>>>(x, g, nimg, H, W, part, err);
+  return cudaGetLastError();
+}
+
 __global__ void k_reduce_partials(const float* __restrict__ part, int nparts, int len, float* __restrict__ out) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < len; e += gridDim.x * blockDim.x) {
     float s = 0.f;
@@ -401,12 +542,14 @@ cudaError_t pilot_backward(const PilotNet& P, const float* pilot, const float* t
   for (int l = PILOT_LAYERS - 1; l >= 0; --l) {
     float* gl = grad + pilot_param_offset(l);
     const int len = 9 * kLayerCO[l] * kLayerCI[l] + kLayerCO[l];
+    cudaError_t ew;
     if (l == PILOT_LAYERS - 1)
-      k_dweight<48, 1, 48, 16><<<grid, NT, 0, st>>>(acts[l], g, nimg, H, W, part);
+      ew = launch_dweight_tc<48, 1, 48, 16>(acts[l], g, nimg, H, W, part, grid, err, st);
     else if (l == 0)
-      k_dweight<2, 48, 16, 48><<<grid, NT, 0, st>>>(acts[0], g, nimg, H, W, part);
+      ew = launch_dweight_tc<2, 48, 16, 48>(acts[0], g, nimg, H, W, part, grid, err, st);
     else
-      k_dweight<48, 48, 48, 48><<<grid, NT, 0, st>>>(acts[l], g, nimg, H, W, part);
+      ew = launch_dweight_tc<48, 48, 48, 48>(acts[l], g, nimg, H, W, part, grid, err, st);
+    if (ew != cudaSuccess) return ew;
     k_reduce_partials<<<64, 256, 0, st>>>(part, grid, len, gl);
     if (l == 0) break;
     // data gradient into the input of layer l, gated by that input's ReLU (acts[l])

@@ -72,11 +72,12 @@ __global__ void __launch_bounds__(128) k_tc_gemm_check(const uint16_t* __restric
 // consecutive M (or N) elements, K-adjacent ones 128 bytes apart (the
 // descriptor's leading byte offset), M-adjacent ones (K/8) * 128 bytes apart
 // (its stride byte offset); instruction descriptor bits 15 / 16 select
-// MN-major A / B.  Every address either reading of the two offsets implies
-// stays inside the operand buffers.
+// MN-major A / B.  With swap_offsets the two descriptor fields are exchanged
+// (the other reading of the MN-major canonical layout); every address either
+// reading implies stays inside the operand buffers.
 __global__ void __launch_bounds__(128) k_tc_gemm_check_mn(const uint16_t* __restrict__ A,
                                                           const uint16_t* __restrict__ B, float* __restrict__ C,
-                                                          int* __restrict__ err) {
+                                                          int* __restrict__ err, int swap_offsets) {
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* sA = smem;
   unsigned char* sB = smem + CM * CK * 2;
@@ -109,8 +110,10 @@ __global__ void __launch_bounds__(128) k_tc_gemm_check_mn(const uint16_t* __rest
     constexpr uint32_t idesc = tc::idesc_bf16_f32(CM, CN) | (1u << 15) | (1u << 16);
 #pragma unroll
     for (int ks = 0; ks < CK / 16; ++ks) {
-      const uint64_t ad = tc::desc_kmajor(a0 + ks * 256, 128, (CK / 8) * 128);
-      const uint64_t bd = tc::desc_kmajor(b0 + ks * 256, 128, (CK / 8) * 128);
+      const uint32_t kstr = 128, mstr = (CK / 8) * 128;  // K-adjacent, M-adjacent core strides
+      const uint32_t lbo = swap_offsets ? mstr : kstr, sbo = swap_offsets ? kstr : mstr;
+      const uint64_t ad = tc::desc_kmajor(a0 + ks * 256, lbo, sbo);
+      const uint64_t bd = tc::desc_kmajor(b0 + ks * 256, lbo, sbo);
       tc::mma_bf16(tmem, ad, bd, idesc, ks > 0);
     }
     tc::commit(mbar);
@@ -134,11 +137,12 @@ __global__ void __launch_bounds__(128) k_tc_gemm_check_mn(const uint16_t* __rest
 }
 }  // namespace
 
-cudaError_t launch_tc_gemm_check_mn(const uint16_t* A, const uint16_t* B, float* C, int* err, cudaStream_t st) {
+cudaError_t launch_tc_gemm_check_mn(const uint16_t* A, const uint16_t* B, float* C, int* err, int swap_offsets,
+                                    cudaStream_t st) {
   const size_t sm = (size_t)(CM + CN) * CK * 2 + 64;
   cudaError_t e = cudaFuncSetAttribute(k_tc_gemm_check_mn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  k_tc_gemm_check_mn<<<1, 128, sm, st>>>(A, B, C, err);
+  k_tc_gemm_check_mn<<<1, 128, sm, st>>>(A, B, C, err, swap_offsets);
   return cudaGetLastError();
 }
 

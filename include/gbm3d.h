@@ -310,9 +310,11 @@ int gbm3d_kernel_time(const gbm3d_ctx* ctx, const char* name, float* total_ms);
  * network use.  Host pointers. */
 int gbm3d_tc_selfcheck(gbm3d_ctx* ctx, const uint16_t* A, const uint16_t* B, float* C);
 /* The same product with the operand layout selected: mn_major = 0 stages A and
- * B K-major (as gbm3d_tc_selfcheck), 1 stages both MN-major (8 K-rows x 8
+ * B K-major (as gbm3d_tc_selfcheck); 1 stages both MN-major (8 K-rows x 8
  * consecutive M or N elements per core matrix), the layout the pilot's
- * weight gradient reads its activation tiles in. */
+ * weight gradient reads its activation tiles in, with the descriptor's leading
+ * byte offset the K-adjacent core stride and its stride byte offset the
+ * M-adjacent one; 2 the same with the two offsets exchanged. */
 int gbm3d_tc_selfcheck_layout(gbm3d_ctx* ctx, int mn_major, const uint16_t* A, const uint16_t* B, float* C);
 
 /* Step-1 block matching that allocates nothing.  No counterpart in the

@@ -38,7 +38,8 @@ def test_tcgen05_gemm_layouts(gpu, seed):
 
 @pytest.mark.parametrize("mn_major", [0, 1])
 def test_tcgen05_gemm_operand_majors(gpu, mn_major):
-    """K-major and MN-major operand staging give the same exact product."""
+    """K-major and MN-major operand staging give the same exact product (mode 1:
+    the descriptor offsets the pilot's weight gradient uses)."""
     from gbm3d_b200._lib import context, lib
     rng = np.random.default_rng(5 + mn_major)
     A = _bf16(rng.normal(0, 1, (128, 64)))
@@ -50,3 +51,22 @@ def test_tcgen05_gemm_operand_majors(gpu, mn_major):
     ref = _f32(A).astype(np.float64) @ _f32(B).astype(np.float64).T
     err = np.abs(out - ref).max()
     assert err < 1e-4 * np.abs(ref).max(), f"max error {err}"
+
+
+def test_tcgen05_mn_major_offset_reading(gpu):
+    """Which reading of the MN-major descriptor offsets the hardware follows:
+    exactly one of the two gives the product (reported; mode 1 must be it)."""
+    from gbm3d_b200._lib import context, lib
+    rng = np.random.default_rng(9)
+    A = _bf16(rng.normal(0, 1, (128, 64)))
+    B = _bf16(rng.normal(0, 1, (256, 64)))
+    ref = _f32(A).astype(np.float64) @ _f32(B).astype(np.float64).T
+    ctx = context()
+    errs = {}
+    for mode in (1, 2):
+        out = np.zeros((128, 256), dtype=np.float32)
+        ctx.check(lib().gbm3d_tc_selfcheck_layout(ctx.h, mode, A.ctypes.data_as(C.c_void_p),
+                                                  B.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+        errs[mode] = float(np.abs(out - ref).max() / np.abs(ref).max())
+    print(f"MN-major relative error: leading offset = K stride {errs[1]:.2e}, = MN stride {errs[2]:.2e}")
+    assert errs[1] < 1e-4
