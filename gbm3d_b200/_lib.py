@@ -88,6 +88,9 @@ _SIGS = {
     "gbm3d_filters_from_bank": (C.c_int, [_P, _P, C.c_int, C.c_int, C.POINTER(gbm3d_filters)]),
     "gbm3d_tc_selfcheck": (C.c_int, [_P, _P, _P, _P]),
     "gbm3d_tc_selfcheck_layout": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "gbm3d_tiles_device": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_double, _P, C.POINTER(gbm3d_opts), _P,
+                                     C.c_int, C.c_int, _P]),
+    "gbm3d_tiles_stitch_device": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P]),
     "gbm3d_ctx_synchronize": (C.c_int, [_P]),
     "gbm3d_denoise_rgb_device": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts),
                                            _P, _P, _P]),

@@ -2043,3 +2043,167 @@ int gbm3d_denoise_colored(gbm3d_ctx* c, const double* I, int m, int n, double si
 }
 
 }  // extern "C"
+
+// ---- GBM3D_distributed on the device (source/GBM3D_distributed.m:54-120) ----------------
+namespace {
+
+// out(r, c) = circshift(I(r0 + (0..ny-1), c0 + (0..nx-1)), [s, s])(r, c)
+//           = I(r0 + (r - s) mod ny, c0 + (c - s) mod nx)
+__global__ void k_tile_in(const double* __restrict__ I, int m, int r0, int c0, int ny, int nx, int s,
+                          double* __restrict__ out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= ny || c >= nx) return;
+  out[r + (size_t)c * ny] = I[(size_t)(r0 + pmod(r - s, ny)) + (size_t)(c0 + pmod(c - s, nx)) * m];
+}
+
+// circshift(U, [-s, -s]) and circshift(W, [-s, -s]) of an ny x nx tile, single -> double
+__global__ void k_tile_out(const float* __restrict__ U, const float* __restrict__ W, int ny, int nx, int s,
+                           double* __restrict__ outU, double* __restrict__ outW) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= ny || c >= nx) return;
+  const size_t src = (size_t)pmod(r + s, ny) + (size_t)pmod(c + s, nx) * ny;
+  outU[r + (size_t)c * ny] = (double)U[src];
+  outW[r + (size_t)c * ny] = (double)W[src];
+}
+
+// One item's stitch (GBM3D_distributed.m:69-71): U2 += U .* win, norm += win .* W
+// over its ny x nx tile at (r0, c0), win = makeInterpWindow(ny, nx, k) built
+// from the ramp linspace(0.01, 1, k) in makeInterpWindow.m's order.
+__global__ void k_tile_stitch(const double* __restrict__ U, const double* __restrict__ W, int ny, int nx, int r0,
+                              int c0, int k, const double* __restrict__ ramp, double* __restrict__ U2,
+                              double* __restrict__ nrm, int m) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= ny || c >= nx) return;
+  double w = 1.0;
+  if (r < k) w *= ramp[r];
+  if (c < k) w *= ramp[c];
+  if (r >= ny - k) w *= ramp[ny - 1 - r];
+  if (c >= nx - k) w *= ramp[nx - 1 - c];
+  const size_t t = r + (size_t)c * ny, o = (size_t)(r0 + r) + (size_t)(c0 + c) * m;
+  U2[o] = U2[o] + U[t] * w;
+  nrm[o] = nrm[o] + w * W[t];
+}
+
+__global__ void k_div(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = a[i] / b[i];
+}
+
+void check_items(gbm3d_ctx* c, const int* items, int n_items, int m, int n, int tile) {
+  if (!items || n_items < 0) argfail(c, "missing item table");
+  for (int ii = 0; ii < n_items; ++ii) {
+    const int* R = items + 5 * ii;
+    const int ny = R[1] - R[0] + 1, nx = R[3] - R[2] + 1;
+    if (R[0] < 1 || R[2] < 1 || R[1] > m || R[3] > n || ny < 1 || nx < 1 || ny > tile || nx > tile)
+      argfail(c, "item " + std::to_string(ii) + ": tile bounds outside the image or larger than the tile size");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int gbm3d_tiles_device(gbm3d_ctx* c, const double* I, const double* pilot, int m, int n, double sigma,
+                       const double* tau, const gbm3d_opts* o, const int* items, int n_items, int tile, double* out) {
+  return guarded(c, [&] {
+    check_opts(c, o);
+    if (!I || !out || (!pilot && !tau)) argfail(c, "missing argument");
+    if (m < 1 || n < 1 || tile < 1) argfail(c, "image size out of range");
+    check_items(c, items, n_items, m, n, tile);
+    const bool step2 = pilot != nullptr;
+    const int d = step2 ? o->blockSizeWie : o->blockSize, d2 = o->matchSize, K = o->numMax;
+    check_match(c, d, d2, K);
+    const int s = step2 ? stride2(o) : stride1(o);
+    gbm3d_filters fb;
+    bior(&fb);
+    const WaveletBank bk = step2 ? WaveletBank{} : make_bank(c, &fb);
+    const size_t slot = (size_t)tile * tile;
+    ck(c, cudaMemsetAsync(c->flag, 0, sizeof(int), c->st), "memset");
+    for (int ii = 0; ii < n_items; ++ii) {
+      const int* R = items + 5 * ii;
+      const int r0 = R[0] - 1, c0 = R[2] - 1, ny = R[1] - R[0] + 1, nx = R[3] - R[2] + 1, sp = R[4];
+      if (ny < d2 || nx < d2 || ny < d || nx < d) argfail(c, "tile smaller than matchSize");
+      const int M = grid_count(ny, d, s), N = grid_count(nx, d, s);
+      const int uy = (M - 1) * s + d, ux = (N - 1) * s + d;
+      if (uy != ny || ux != nx) argfail(c, "tile sides must be whole reference grids");
+      const size_t px = (size_t)ny * nx;
+      double* dT = buf<double>(c, "tl.I", px);
+      k_tile_in<<<grid2(ny, nx), 256, 0, c->st>>>(I, m, r0, c0, ny, nx, sp, dT);
+      launched(c, cudaGetLastError(), "tile_in");
+      float* Tf = buf<float>(c, "tl.If", px);
+      k_prep<<<grid2(ny, nx), 256, 0, c->st>>>(dT, ny, nx, Tf, ny, nx, c->flag);
+      launched(c, cudaGetLastError(), "prep");
+      uint32_t* dS = buf<uint32_t>(c, "tl.S", (size_t)K * M * N);
+      float* dU = buf<float>(c, "tl.U", px);
+      float* dW = buf<float>(c, "tl.W", px);
+      if (!step2) {
+        // [S, Volume] = matchBlocksCPU(Ilocal); [U, W] = denoiseAndAggregateGPU(...)
+        int32_t* dc = buf<int32_t>(c, "tl.cnt", (size_t)M * N);
+        const size_t vn = s == d ? px * K : (size_t)M * d * N * d * K;
+        float* dV = buf<float>(c, "tl.V", vn);
+        ck(c, cudaMemsetAsync(dV, 0, vn * sizeof(float), c->st), "memset");
+        run_match(c, Tf, nullptr, ny, nx, 0, d, d2, K, o->numMin, sigma, dS, dc, dV, nullptr, nullptr, "tl1", s,
+                  o->form);
+        run_ht(c, dV, dS, dc, M, N, d, d2, K, o->levels, o->cycleSpin, tau, bk, dU, dW, o->filtType, s);
+      } else {
+        // [S, V1, V2] = matchBlocksWie(pilot tile, noisy tile); denoiseAndAggregateWieFast
+        double* dP = buf<double>(c, "tl.P", px);
+        k_tile_in<<<grid2(ny, nx), 256, 0, c->st>>>(pilot, m, r0, c0, ny, nx, sp, dP);
+        launched(c, cudaGetLastError(), "tile_in");
+        float* Pf = buf<float>(c, "tl.Pf", px);
+        k_prep<<<grid2(ny, nx), 256, 0, c->st>>>(dP, ny, nx, Pf, ny, nx, c->flag);
+        launched(c, cudaGetLastError(), "prep");
+        const size_t gs = (size_t)d * d * K * M * N;
+        float* d1 = buf<float>(c, "tl.V1", gs);
+        float* d2p = buf<float>(c, "tl.V2", gs);
+        run_match(c, Pf, Tf, ny, nx, 0, d, d2, K, K, sigma, dS, nullptr, nullptr, d1, d2p, "tl2", s, o->form);
+        WienerArgs A{};
+        A.V1 = d1;
+        A.V2 = d2p;
+        A.S = dS;
+        A.M = M;
+        A.N = N;
+        A.K = K;
+        A.s = s;
+        A.d2 = d2;
+        fill_wiener_consts(A, d, &sigma, 0, 0);
+        run_wiener_agg(c, A, d, d2, dU, dW);
+      }
+      k_tile_out<<<grid2(ny, nx), 256, 0, c->st>>>(dU, dW, ny, nx, sp, out + 2 * slot * ii,
+                                                  out + 2 * slot * ii + slot);
+      launched(c, cudaGetLastError(), "tile_out");
+    }
+    int flag = 0;
+    ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+    report_flag(c, flag);
+  });
+}
+
+int gbm3d_tiles_stitch_device(gbm3d_ctx* c, const double* tiles, const int* items, int n_items, int tile, int m,
+                              int n, int k, const double* ramp, double* out) {
+  return guarded(c, [&] {
+    if (!tiles || !out || !ramp || k < 1 || k > 256) argfail(c, "missing argument");
+    check_items(c, items, n_items, m, n, tile);
+    const size_t px = (size_t)m * n, slot = (size_t)tile * tile;
+    double* U2 = buf<double>(c, "st.U2", px);
+    double* nrm = buf<double>(c, "st.norm", px);
+    double* dr = buf<double>(c, "st.ramp", (size_t)k);
+    ck(c, cudaMemcpyAsync(dr, ramp, (size_t)k * sizeof(double), cudaMemcpyHostToDevice, c->st), "H2D");
+    ck(c, cudaMemsetAsync(U2, 0, px * sizeof(double), c->st), "memset");
+    ck(c, cudaMemsetAsync(nrm, 0, px * sizeof(double), c->st), "memset");
+    for (int ii = 0; ii < n_items; ++ii) {  // item order: every pixel adds its tiles in table order
+      const int* R = items + 5 * ii;
+      const int ny = R[1] - R[0] + 1, nx = R[3] - R[2] + 1;
+      if (ny < 2 * k || nx < 2 * k) argfail(c, "tile shorter than two ramps");
+      k_tile_stitch<<<grid2(ny, nx), 256, 0, c->st>>>(tiles + 2 * slot * ii, tiles + 2 * slot * ii + slot, ny, nx,
+                                                     R[0] - 1, R[2] - 1, k, dr, U2, nrm, m);
+      launched(c, cudaGetLastError(), "tile_stitch");
+    }
+    k_div<<<(unsigned)std::min<size_t>((px + 255) / 256, 4096), 256, 0, c->st>>>(U2, nrm, out, px);
+    launched(c, cudaGetLastError(), "div");
+    ck(c, cudaStreamSynchronize(c->st), "sync");
+  });
+}
+
+}  // extern "C"

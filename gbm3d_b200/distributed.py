@@ -1,17 +1,25 @@
 """Tiled GBM3D (GBM3D_distributed) and its multi-GPU sharding.
 
-Host-side restatement of source/GBM3D_distributed.m:15-120 with
+Restatement of source/GBM3D_distributed.m:15-120 with
 utilities/getBM3D_distribution.m:10-48 and utilities/makeInterpWindow.m:8-13:
 the image is cut into (256+k) x (256+k) tiles overlapping by k = blockSize,
 each tile x match spin is denoised with the reference's four hot-path
 functions, and the tiles are stitched with linear ramp windows.
 
+Two drivers with the same result:
+  * on the device (the default with a GPU): one library call per step runs
+    this rank's tiles (gbm3d_tiles_device) and one call stitches them
+    (gbm3d_tiles_stitch_device); images and tiles stay in device memory;
+  * on the host through a Backend of per-tile functions (the CUDA drop-ins
+    with host copies, or the CPU oracle in the tests).
+
 Sharding: with torch.distributed initialised and world size N > 1, work item
 ii (a tile x spin row of the distribution table) runs on rank ii mod N.  The
-per-item results are all-gathered and every rank stitches all items in table
-order, so the result does not depend on N (bit-identical to one rank); the
-step-2 search needs the whole step-1 estimate, which every rank then holds.
-The all-gather is the only exchange; items are independent otherwise.
+per-item tiles are packed into fixed (2, tile, tile) float64 slots and
+all-gathered as one tensor (NCCL on the GPU, gloo on the CPU), and every rank
+stitches all items in table order, so the result does not depend on N
+(bit-identical to one rank); the step-2 search needs the whole step-1
+estimate, which every rank then holds.  The all-gather is the only exchange.
 """
 from __future__ import annotations
 
@@ -87,18 +95,42 @@ def _dist():
     return None
 
 
-def _run_items(items, fn, dist):
-    """Run fn(ii) for the work items of this rank and gather every item's result."""
+def _gather_slots(mine, n_items: int, dist, like):
+    """Every item's slot, in table order, from the slots each rank computed:
+    rank r holds items r, r + N, ... in order (mine: [n_mine, 2, tile, tile]).
+    One all_gather of equal-sized tensors (counts padded to the largest)."""
+    import torch
+    world = dist.get_world_size()
+    cap = -(-n_items // world)
+    buf = torch.zeros((cap,) + tuple(mine.shape[1:]), dtype=mine.dtype, device=mine.device)
+    buf[:mine.shape[0]] = mine
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf)
+    full = torch.empty((n_items,) + tuple(mine.shape[1:]), dtype=mine.dtype, device=mine.device)
+    for r in range(world):
+        idx = list(range(r, n_items, world))
+        if idx:
+            full[idx] = parts[r][:len(idx)]
+    return full
+
+
+def _run_items(items, fn, dist, tile):
+    """Run fn(ii) -> (U, W) for the work items of this rank and return every
+    item's (U, W) in table order (host arrays)."""
     if dist is None:
         return [fn(ii) for ii in items]
+    import torch
     rank, world = dist.get_rank(), dist.get_world_size()
-    mine = {ii: fn(ii) for ii in items if ii % world == rank}
-    gathered = [None] * world
-    dist.all_gather_object(gathered, mine)
-    out = {}
-    for part in gathered:
-        out.update(part)
-    return [out[ii] for ii in items]
+    res = {ii: fn(ii) for ii in items if ii % world == rank}
+    mine = torch.zeros((len(res), 2, tile, tile), dtype=torch.float64)
+    shapes = {}
+    for q, ii in enumerate(sorted(res)):
+        U, W = res[ii]
+        shapes[ii] = U.shape
+        mine[q, 0].view(-1)[:U.size] = torch.from_numpy(np.asfortranarray(U).ravel(order="F"))
+        mine[q, 1].view(-1)[:W.size] = torch.from_numpy(np.asfortranarray(W).ravel(order="F"))
+    full = _gather_slots(mine, len(items), dist, mine).numpy()
+    return full, shapes
 
 
 def _stitch(R, results, m, n, d0, k):
@@ -118,8 +150,25 @@ def _shift(a, s):
     return np.roll(a, (s, s), axis=(0, 1))
 
 
-def GBM3D_distributed(I, sigma, opts: dict | None = None, backend: Backend | None = None):
-    """[U, out] = GBM3D_distributed(I, sigma, opts) (source/GBM3D_distributed.m:1)."""
+def _unpack(full, R, ii):
+    r1, r2, r3, r4 = (int(v) for v in R[ii, :4])
+    ny, nx = r2 - r1 + 1, r4 - r3 + 1
+    U = full[ii, 0].reshape(-1)[:ny * nx].reshape((ny, nx), order="F")
+    W = full[ii, 1].reshape(-1)[:ny * nx].reshape((ny, nx), order="F")
+    return U, W
+
+
+def _host_items(R, fn, dist, d0):
+    out = _run_items(list(range(len(R))), fn, dist, d0)
+    if dist is None:
+        return out
+    full, _ = out
+    return [_unpack(full, R, ii) for ii in range(len(R))]
+
+
+def GBM3D_distributed(I, sigma, opts: dict | None = None, backend: Backend | None = None, ctx=None):
+    """[U, out] = GBM3D_distributed(I, sigma, opts) (source/GBM3D_distributed.m:1).
+    Without a backend the tiles run on the device (gbm3d_tiles_device)."""
     o = _opt.resolve_opts(opts)
     I = np.asarray(I, dtype=np.float64)
     m, n = I.shape
@@ -127,8 +176,10 @@ def GBM3D_distributed(I, sigma, opts: dict | None = None, backend: Backend | Non
     if m < 256 + k or n < 256 + k:  # GBM3D_distributed.m:24-27
         from . import api
         return api.GBM3D(I, sigma, o)
-    be = backend or cuda_backend()
     dist = _dist()
+    if backend is None:
+        return _device_driver(I, sigma, o, dist, ctx)
+    be = backend
     tau = sigma * _opt.getTau(int(o["levels"]), int(o["tauMode"]))
     R, d0, _ = getBM3D_distribution(m, n, o["matchSpins"], k)
     RW, _, _ = getBM3D_distribution(m, n, o["matchSpinsWie"], k)
@@ -138,7 +189,7 @@ def GBM3D_distributed(I, sigma, opts: dict | None = None, backend: Backend | Non
         U, W = be.step1(_shift(I[r1 - 1:r2, r3 - 1:r4], s), sigma, tau, o)
         return _shift(U, -s), _shift(W, -s)
 
-    res1 = _run_items(list(range(len(R))), step1, dist)
+    res1 = _host_items(R, step1, dist, d0)
     U2, norm = _stitch(R, res1, m, n, d0, k)
     U2 = U2 / norm
     out = {"U2": U2}
@@ -150,6 +201,52 @@ def GBM3D_distributed(I, sigma, opts: dict | None = None, backend: Backend | Non
         U, W = be.step2(_shift(U2[r1 - 1:r2, r3 - 1:r4], s), _shift(I[r1 - 1:r2, r3 - 1:r4], s), sigma, o)
         return _shift(U, -s), _shift(W, -s)
 
-    res2 = _run_items(list(range(len(RW))), step2, dist)
+    res2 = _host_items(RW, step2, dist, d0)
     Uf, norm2 = _stitch(RW, res2, m, n, d0, k)
     return Uf / norm2, out
+
+
+def _device_driver(I, sigma, o, dist, ctx=None):
+    """The tiled driver on the device: per step one gbm3d_tiles_device call over
+    this rank's items, one all_gather of the item slots (N > 1), one
+    gbm3d_tiles_stitch_device call in table order."""
+    import ctypes as C
+
+    import torch
+
+    from . import api
+    from ._lib import context, lib
+    ctx = ctx or context()
+    dev = torch.device("cuda", ctx.device)
+    m, n = I.shape
+    k = int(o["blockSize"])
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist is not None else (0, 1)
+    tau = np.asfortranarray(sigma * _opt.getTau(int(o["levels"]), int(o["tauMode"])))
+    ramp = np.ascontiguousarray(np.linspace(0.01, 1, k))
+    co = api.c_opts(o)
+    dI = torch.from_numpy(np.asfortranarray(I).ravel(order="F").copy()).to(dev)
+    torch.cuda.synchronize(dev)
+
+    def step(spins, pilot):
+        R, d0, _ = getBM3D_distribution(m, n, spins, k)
+        table = np.ascontiguousarray(R, dtype=np.int32)
+        mine = np.ascontiguousarray(table[rank::world])
+        slots = torch.empty((mine.shape[0], 2, d0, d0), dtype=torch.float64, device=dev)
+        ctx.check(lib().gbm3d_tiles_device(
+            ctx.h, C.c_void_p(dI.data_ptr()), C.c_void_p(pilot.data_ptr()) if pilot is not None else None, m, n,
+            float(sigma), tau.ctypes.data_as(C.c_void_p), C.byref(co), mine.ctypes.data_as(C.c_void_p),
+            mine.shape[0], d0, C.c_void_p(slots.data_ptr())))
+        full = _gather_slots(slots, len(table), dist, slots) if dist is not None else slots
+        torch.cuda.synchronize(dev)
+        U = torch.empty_like(dI)
+        ctx.check(lib().gbm3d_tiles_stitch_device(
+            ctx.h, C.c_void_p(full.data_ptr()), table.ctypes.data_as(C.c_void_p), len(table), d0, m, n, k,
+            ramp.ctypes.data_as(C.c_void_p), C.c_void_p(U.data_ptr())))
+        return U
+
+    U2 = step(o["matchSpins"], None)
+    out = {"U2": U2.cpu().numpy().reshape((m, n), order="F")}
+    if not o["Wiener"]:
+        return out["U2"], out
+    U = step(o["matchSpinsWie"], U2)
+    return U.cpu().numpy().reshape((m, n), order="F"), out

@@ -281,6 +281,30 @@ int gbm3d_denoise_mixed(gbm3d_ctx* ctx, const gbm3d_mixed_batch* batch, const gb
 int gbm3d_denoise_async(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma, const gbm3d_opts* opts,
                         double* U);
 
+/* ---- U = GBM3D_distributed(I,sigma,opts) on the device ----------------------------
+ * source/GBM3D_distributed.m:54-120: the image is cut into overlapping tiles
+ * (items from getBM3D_distribution: n_items rows of r1, r2, r3, r4, spin with
+ * 1-based inclusive bounds, int32), each item is denoised on its own and the
+ * tiles are stitched with ramp windows.  Device pointers (float64 column-major
+ * images), results as the reference computes them tile by tile.
+ * gbm3d_tiles_device: step 1 (pilot NULL) runs matchBlocksCPU +
+ * denoiseAndAggregateGPU on circshift(I(r1:r2,r3:r4),[s s]) with tau (host,
+ * levels x 7) and the bior1.5 x Haar bank; step 2 (pilot = the step-1
+ * estimate) runs matchBlocksWie on the pilot tile + denoiseAndAggregateWieFast
+ * at sigma.  Item ii writes circshift(U,[-s -s]) then circshift(W,[-s -s])
+ * (column-major ny x nx each) at out + 2 tile^2 ii; every tile side is at most
+ * `tile` and a whole reference grid.  The item table is host memory.
+ * gbm3d_tiles_stitch_device: out = (sum over items, in table order, of
+ * U .* win) ./ (sum of win .* W) (GBM3D_distributed.m:62-72, :103-113),
+ * win = makeInterpWindow(ny, nx, k) built from ramp = linspace(0.01, 1, k)
+ * (host).  Not in the reference: the reference runs these loops as parfor
+ * over MATLAB workers. */
+int gbm3d_tiles_device(gbm3d_ctx* ctx, const double* I, const double* pilot, int m, int n, double sigma,
+                       const double* tau, const gbm3d_opts* opts, const int* items, int n_items, int tile,
+                       double* out);
+int gbm3d_tiles_stitch_device(gbm3d_ctx* ctx, const double* tiles, const int* items, int n_items, int tile, int m,
+                              int n, int k, const double* ramp, double* out);
+
 /* Same as gbm3d_denoise with device pointers; no host copies.  Asynchronous on
  * the context stream (synchronise before reading U). */
 int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,

@@ -232,6 +232,18 @@ def test_GBM3D_distributed_cuda_matches_oracle_tiles(gpu):
     assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255) + 5
 
 
+def test_GBM3D_distributed_device_matches_host_driver(gpu):
+    """The device tile driver (one call per step, device-side stitching) equals
+    the host driver over the CUDA drop-ins bit for bit, on an image whose edge
+    tiles are pulled back (getBM3D_distribution.m:29-36)."""
+    from gbm3d_b200 import distributed as D
+    clean, noisy = synth.noisy_image(600, 540, 25.0, seed=43)
+    U, out = D.GBM3D_distributed(noisy, 25.0, {"profile": "default"})
+    Uh, outh = D.GBM3D_distributed(noisy, 25.0, {"profile": "default"}, backend=D.cuda_backend())
+    assert np.array_equal(out["U2"], outh["U2"]) and np.array_equal(U, Uh)
+    assert options.myPSNR(clean, U, 255) > options.myPSNR(clean, noisy, 255) + 5
+
+
 @pytest.mark.parametrize("m,n,sigma,omega,seed", [(64, 64, 25.0, 1.0, 31), (96, 80, 40.0, 2.0, 32)])
 def test_GBM3D_colored_noise(gpu, oracle, m, n, sigma, omega, seed):
     """GBM3D.m:33-35: matrix sigma (sigma^2 * PSD) -> getColoredTau / getColoredWie."""
