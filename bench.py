@@ -500,6 +500,31 @@ def batched_block(ctx, stream, work, reps=3):
                 np.mean(gains))}
 
 
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The step time of the whole job: the slowest rank's (an all-reduce MAX of
+    one value, on the device the backend needs: a GPU for NCCL, the CPU for gloo)."""
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def bcast_from_rank0(obj, dist):
+    """Rank 0's value of a small picklable object on every rank (the chosen
+    form and options, so every rank takes the same collective steps)."""
+    if dist is None:
+        return obj
+    box = [obj]
+    dist.broadcast_object_list(box, src=0)
+    return box[0]
+
+
+def replica_value(world: int, mpix_per_rank: float, ms: float) -> float:
+    """Whole-job MPix/s of N replicas, each denoising its own image: all
+    ranks' pixels over the slowest rank's step time."""
+    return world * mpix_per_rank / (ms / 1e3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -516,12 +541,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
 
     def bcast(obj):
-        """rank 0's value of a small picklable object, on every rank"""
-        if world == 1:
-            return obj
-        box = [obj]
-        dist.broadcast_object_list(box, src=0)
-        return box[0]
+        return bcast_from_rank0(obj, dist if world > 1 else None)
 
     from gbm3d_b200 import _lib, api, build, synth
     build.build()
@@ -570,9 +590,7 @@ def run_ours(args):
         clk = clocks.stop() if sample_clocks else None
         ms = e0.elapsed_time(e1) / args.steps
         if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dist, dev)
             dist.barrier()
         U = dU.cpu().numpy().reshape(SIZE, SIZE, order="F")
         return {"ms": ms, "stages": stages, "ktimes": kt, "launches": launches, "clk": clk,
@@ -630,7 +648,7 @@ def run_ours(args):
     if form != forms[-1]:  # leave the chosen form's output in dU for the end-to-end check
         measure(o, False)
     ms, stages, ktimes, launches, clk = (chosen[k] for k in ("ms", "stages", "ktimes", "launches", "clk"))
-    value = world * mpix / (ms / 1e3)
+    value = replica_value(world, mpix, ms)
 
     # end to end through the public host API, pinned host buffers, the H2D copy
     # of the input and the D2H copy of the result in every step: (1) one
@@ -661,9 +679,7 @@ def run_ours(args):
             ctx.synchronize()
         ms = (time.perf_counter() - t0) * 1e3 / args.steps
         if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dist, dev)
         return ms
 
     Uref = dU.cpu().numpy().reshape(SIZE, SIZE, order="F")

@@ -68,3 +68,40 @@ def test_measured_hbm_peak_is_used_when_present():
     assert work["wiener"]["peak"] == 7000.0 and work["wiener"]["unit"] == "GB/s"
     _, work = bench.roofline(o, {"wiener": (1, 1.0)}, {}, 1965.0)
     assert work["wiener"]["peak"] == 6650.0
+
+
+def _replica_rank(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    ms = bench.max_over_ranks(10.0 + 5.0 * rank, dist, "cpu")      # rank 1 is the slower one
+    form = bench.bcast_from_rank0("tuned" if rank == 0 else "plain", dist)
+    value = bench.replica_value(world, 16.777216, ms)
+    with open(os.path.join(out, f"r{rank}.txt"), "w") as f:
+        f.write(f"{ms} {form} {value}")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_mode_two_ranks(tmp_path):
+    """bench.py --gpus 2 as two gloo ranks on the CPU: every rank reports the
+    slowest rank's time, takes rank 0's choice of form, and the whole-job
+    value counts both ranks' images."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_replica_rank, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for r in range(2):
+        ms, form, value = open(tmp_path / f"r{r}.txt").read().split()
+        assert float(ms) == 15.0 and form == "tuned"
+        assert abs(float(value) - 2 * 16.777216 / 0.015) < 1e-9
