@@ -358,7 +358,7 @@ def quality_by_size(ctx, fresh=None, sizes=(512, 1024, 2048, 4096)):
         Ut, _ = api.GBM3D(noisy, SIGMA, tuned, ctx=ctx)
         pd, pt = float(_opt.myPSNR(clean, Ud, 255)), float(_opt.myPSNR(clean, Ut, 255))
         out.append({"size": sz, "seed": 7000 + sz, "psnr_dense_db": pd, "psnr_tuned_db": pt, "delta_db": pt - pd,
-                    "within_0.05dB": pt >= pd - 0.05, "tuned_opts": {k: tuned[k] for k in (
+                    "within_0.05dB": pt >= pd - 0.05, "tuned_opts": {k: tuned.get(k, "plain") for k in (
                         "refStride", "refStrideWie", "matchSpins", "matchSpinsWie", "cycleSpin", "form")}})
     return out
 
@@ -491,8 +491,8 @@ def batched_block(ctx, stream, work, reps=3):
         gains.append(float(_opt.myPSNR(clean, U, 255) - _opt.myPSNR(clean, x, 255)))
     return {"workload": "64 grey (200x300 .. 2048x1536, sigma 5-50) + 8 RGB 1024^2 (opponent colour, luma "
                         "matching) + 32-frame 1280x720 video (+-1 frame), one gbm3d_denoise_mixed submission",
-            "megapixels": mpix, "opts": {k: o[k] for k in ("refStride", "refStrideWie", "matchSize", "matchSpins",
-                                                           "matchSpinsWie", "cycleSpin", "form")},
+            "megapixels": mpix, "opts": {k: o.get(k, "plain") for k in (
+                "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin", "form")},
             "eager_ms": eager_ms, "graph_ms": graph_ms, "value": mpix / (min(eager_ms, graph_ms) / 1e3),
             "unit": "MPix/s", "eager_mpix_s": mpix / (eager_ms / 1e3), "graph_mpix_s": mpix / (graph_ms / 1e3),
             "launches_eager": eager_launches, "graph_launches_per_call": graph_launches,
@@ -616,7 +616,7 @@ def run_ours(args):
         elif not args.autotune and os.path.exists(_opt.TUNED_SETS):
             form_opts["tuned"] = _opt.resolve_opts({"profile": "tuned"}, shape=(SIZE, SIZE), sigma=SIGMA)
             tuning = {"source": "gbm3d_b200/tuned_sets.json (python -m gbm3d_b200.autotune --classes)",
-                      "opts": {k: form_opts["tuned"][k] for k in (
+                      "opts": {k: form_opts["tuned"].get(k, "plain") for k in (
                           "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin",
                           "form")}}
         else:
@@ -703,7 +703,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": TUNED_DTYPE[o.get("form", "plain")] if form == "tuned" else FORM_DTYPE[form],
             "data": "synthetic",
-            "config": _config({"form": form, "form_opts": {k: o[k] for k in (
+            "config": _config({"form": form, "form_opts": {k: o.get(k, "plain") for k in (
                 "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin", "form")},
                 "plain_workload": WORKLOADS[WL][0].format(n=SIZE)}, workload=describe(o, form)),
             "autotune": None if tuning is None else (tuning if "source" in tuning else {
