@@ -8,8 +8,10 @@
 // (it is the candidate at offset (d2/2, d2/2)) by warp-uniform broadcasts.
 //
 // Distances are exact FP32 sums of squared differences, row-major over the
-// block: t = x - y; acc = fmaf(t, t, acc), two candidates per paired
-// instruction.  The K best candidates are the K
+// block: t = x - y; acc = fmaf(t, t, acc), in scalar instructions, which the
+// scheduler spreads over both FP32 pipes (fmaheavy and fmalite); the paired
+// f32x2 form of the same operations issues half as many instructions but runs
+// on fmaheavy alone and measured 23 % slower.  The K best candidates are the K
 // smallest (distance, column-major window index) pairs — the stable order of
 // MATLAB's mink — found by a bitwise radix search for the K-th smallest
 // distance with warp reductions, then an index-ordered pick among ties.
@@ -19,29 +21,6 @@
 #include "kernels.cuh"
 
 namespace gbm3d {
-
-typedef unsigned long long u64;
-
-// Paired single-precision arithmetic of sm_100 (two IEEE round-to-nearest
-// operations per instruction on a 64-bit register pair).
-__device__ __forceinline__ u64 pack2(float lo, float hi) {
-  u64 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void unpack2(u64 v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
-  u64 d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
-  u64 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
 
 // Ipad of the reference for a circularly shifted image: rows (m+d2), cols
 // (n+d2), column pitch P floats.  spin is the circshift applied to the image.
@@ -82,54 +61,31 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float
   __syncwarp();
 
   // ---- exact SSD for the lane's candidates (a = lane, b = 0..D2-1) ----------
-  // Accumulators are held in pairs (acc[b], acc[b+1]) and updated with the
-  // paired FP32 instructions of sm_100 (sub.rn.f32x2, fma.rn.f32x2), which
-  // round each component exactly as the scalar sub/fmaf would: candidate b
-  // still sees t = x(r, c) - y, acc = fmaf(t, t, acc) in (r, c) order.  At
-  // window column xw the pair needs x(r, xw-b) and x(r, xw-b-1), kept packed
-  // per row as xp[c] = (x(r,c), x(r,c-1)).
-  u64 acc2[D2 / 2];
+  // Candidate b sees t = x(r, c) - y, acc = fmaf(t, t, acc) in (r, c) order
+  // (c = xw - b ascends with the window column xw).
+  float acc[D2];
 #pragma unroll
-  for (int p = 0; p < D2 / 2; ++p) acc2[p] = 0ull;
+  for (int b = 0; b < D2; ++b) acc[b] = 0.f;
   const int a = lane < D2 ? lane : 0;
 #pragma unroll 1
   for (int r = 0; r < D; ++r) {
     float xr[D];
 #pragma unroll
     for (int c = 0; c < D; ++c) xr[c] = win[(H + r) + (H + c) * WD];
-    u64 xp[D];
-#pragma unroll
-    for (int c = 1; c < D; ++c) xp[c] = pack2(xr[c], xr[c - 1]);
     const float* wrow = win + (a + r);
 #pragma unroll
     for (int xw = 0; xw < WD; ++xw) {
       const float w = wrow[xw * WD];
-      const u64 w2 = pack2(w, w);
 #pragma unroll
-      for (int p = 0; p < D2 / 2; ++p) {
-        const int c = xw - 2 * p;  // column of candidate b = 2p; b+1 uses c-1
-        if (c >= 1 && c <= D - 1) {
-          const u64 t2 = sub2(xp[c], w2);
-          acc2[p] = fma2(t2, t2, acc2[p]);
-        } else if (c == 0) {
-          float lo, hi;
-          unpack2(acc2[p], lo, hi);
-          const float t = xr[0] - w;
-          lo = fmaf(t, t, lo);
-          acc2[p] = pack2(lo, hi);
-        } else if (c == D) {
-          float lo, hi;
-          unpack2(acc2[p], lo, hi);
-          const float t = xr[D - 1] - w;
-          hi = fmaf(t, t, hi);
-          acc2[p] = pack2(lo, hi);
+      for (int b = 0; b < D2; ++b) {
+        const int c = xw - b;
+        if (c >= 0 && c < D) {
+          const float t = xr[c] - w;
+          acc[b] = fmaf(t, t, acc[b]);
         }
       }
     }
   }
-  float acc[D2];
-#pragma unroll
-  for (int p = 0; p < D2 / 2; ++p) unpack2(acc2[p], acc[2 * p], acc[2 * p + 1]);
 
   // ---- selection -------------------------------------------------------------
   const unsigned FULL = 0xffffffffu;
