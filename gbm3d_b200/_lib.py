@@ -82,6 +82,8 @@ _SIGS = {
     "gbm3d_denoise_device": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise_async": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P]),
     "gbm3d_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
+    "gbm3d_ctx_set_tc_wait": (C.c_int, [_P, C.c_longlong]),
+    "gbm3d_ctx_tc_stats": (C.c_int, [_P, C.c_int, _P]),
     "gbm3d_stage_times": (C.c_int, [_P, _P, C.c_int]),
     "gbm3d_last_launch_count": (C.c_int, [_P]),
     "gbm3d_kernel_time": (C.c_int, [_P, C.c_char_p, _P]),
@@ -170,6 +172,20 @@ class Context:
 
     def enable_timing(self, on: bool = True) -> None:
         self.check(lib().gbm3d_ctx_enable_timing(self.h, 1 if on else 0))
+
+    def set_tc_wait(self, cycles: int = 0) -> None:
+        """Limit (SM clocks) of each wait in the tensor-core matcher; 0 = about
+        two seconds.  Negative: a probe of the give-up path (every CTA waits
+        -cycles clocks on a barrier that nothing completes, then gives up)."""
+        self.check(lib().gbm3d_ctx_set_tc_wait(self.h, int(cycles)))
+
+    def tc_stats(self, enable: bool = True, read: bool = True) -> list[int] | None:
+        """Candidates per reference left by the tensor-core matcher's bound:
+        33 buckets of 8 (the last: 256 or more).  Returns the counts since the
+        last read (and resets them) when ``read``."""
+        buf = (C.c_int32 * 33)()
+        self.check(lib().gbm3d_ctx_tc_stats(self.h, 1 if enable else 0, buf if read else None))
+        return [int(x) for x in buf] if read else None
 
     def stage_times(self) -> list[float]:
         buf = (C.c_float * 8)()

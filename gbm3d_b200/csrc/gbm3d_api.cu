@@ -56,6 +56,9 @@ struct gbm3d_ctx {
   int slot = 0;
   bool async_pending = false;
   int* sticky = nullptr;  // OR of the status words of the asynchronous calls since the last synchronisation
+  long long tc_wait = 0;  // wait limit of the tensor-core matcher in SM clocks (0: about two seconds; < 0: probe)
+  bool tc_stats = false;  // accumulate the tensor-core matcher's candidate histogram
+  int* tc_hist = nullptr; // 33 buckets on the device
 };
 
 namespace {
@@ -81,10 +84,10 @@ void argfail(gbm3d_ctx* c, const std::string& s, int code = GBM3D_ERR_ARG) {
 }
 
 // Device status word: bit 0 non-finite input (k_prep), bit 1 a tensor-core
-// MMA that did not complete within its wait limit (the kernel gave up).
+// matcher wait (TMA copy or MMA) that ran out of its limit (the kernel gave up).
 void report_flag(gbm3d_ctx* c, int flag) {
   if (flag & 1) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
-  if (flag & 2) argfail(c, "tensor-core MMA did not complete in time", GBM3D_ERR_CUDA);
+  if (flag & 2) argfail(c, "tensor-core matcher: a TMA copy or MMA did not complete within its wait limit", GBM3D_ERR_CUDA);
 }
 
 template <class T>
@@ -498,7 +501,11 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
     if (!V1 && !V2 && !img2) {
       A.ovf_list = buf<int>(c, "mtc.ovf", (size_t)A.M * A.N);
       A.ovf_count = buf<int>(c, "mtc.novf", 1);
-      launched(c, launch_match_tc(d, d2, A, c->st), "match_tc");
+      A.work = buf<int>(c, "mtc.work", 1);
+      A.wait_cycles = c->tc_wait;
+      A.cand_hist = c->tc_stats ? c->tc_hist : nullptr;
+      // precision form: bf16 operands; tensor form: f16 (a tighter bound, the same match sets)
+      launched(c, launch_match_tc(d, d2, A, form == 3, c->st), "match_tc");
       // references whose candidate list overflowed: the exhaustive search
       MatchArgs L = A;
       L.list = A.ovf_list;
@@ -904,6 +911,7 @@ void gbm3d_ctx_destroy(gbm3d_ctx* c) {
         if (e) cudaEventDestroy(e);
   }
   if (c->sticky) cudaFree(c->sticky);
+  if (c->tc_hist) cudaFree(c->tc_hist);
   for (auto& kv : c->bufs) cudaFree(kv.second.first);
   for (auto& e : c->evpool) cudaEventDestroy(e);
   for (auto& e : c->kpool) cudaEventDestroy(e);
@@ -920,6 +928,27 @@ int gbm3d_ctx_set_stream(gbm3d_ctx* c, void* s) {
 }
 
 const char* gbm3d_last_error(const gbm3d_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int gbm3d_ctx_set_tc_wait(gbm3d_ctx* c, long long cycles) {
+  if (!c) return GBM3D_ERR_ARG;
+  c->tc_wait = cycles;
+  return GBM3D_OK;
+}
+
+int gbm3d_ctx_tc_stats(gbm3d_ctx* c, int enable, int32_t* hist) {
+  return guarded(c, [&] {
+    if (!c->tc_hist) {
+      ck(c, cudaMalloc(&c->tc_hist, 33 * sizeof(int)), "tc_hist");
+      ck(c, cudaMemsetAsync(c->tc_hist, 0, 33 * sizeof(int), c->st), "memset");
+    }
+    if (hist) {
+      ck(c, cudaMemcpyAsync(hist, c->tc_hist, 33 * sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
+      ck(c, cudaMemsetAsync(c->tc_hist, 0, 33 * sizeof(int), c->st), "memset");
+      ck(c, cudaStreamSynchronize(c->st), "synchronize");
+    }
+    c->tc_stats = enable != 0;
+  });
+}
 
 int gbm3d_ctx_enable_timing(gbm3d_ctx* c, int on) {
   if (!c) return GBM3D_ERR_ARG;
@@ -964,7 +993,7 @@ int gbm3d_ctx_synchronize(gbm3d_ctx* c) {
       return GBM3D_ERR_NONFINITE;
     }
     if (flag & 2) {
-      c->err = "tensor-core MMA did not complete in time";
+      c->err = "tensor-core matcher: a TMA copy or MMA did not complete within its wait limit";
       return GBM3D_ERR_CUDA;
     }
   }
@@ -1328,7 +1357,7 @@ int gbm3d_tc_selfcheck_layout(gbm3d_ctx* c, int mn_major, const uint16_t* A, con
     int flag = 0;
     ck(c, cudaMemcpyAsync(&flag, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->st), "D2H");
     ck(c, cudaStreamSynchronize(c->st), "sync");
-    if (flag) argfail(c, "tensor-core MMA did not complete in time", GBM3D_ERR_CUDA);
+    if (flag) argfail(c, "tensor-core matcher: a TMA copy or MMA did not complete within its wait limit", GBM3D_ERR_CUDA);
   });
 }
 

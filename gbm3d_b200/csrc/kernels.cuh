@@ -29,6 +29,12 @@ struct MatchArgs {
   // list mode of the exhaustive matcher: only the references list[0 .. *list_count)
   const int* list;
   const int* list_count;
+  // tensor-core matcher: work queue counter (zeroed by the launch), limit of
+  // every wait in SM clocks (0: about two seconds), and an optional histogram
+  // of candidates per reference (33 buckets of 8, the last for >= 256)
+  int* work;
+  long long wait_cycles;
+  int* cand_hist;
 };
 bool match_supported(int d, int d2);
 size_t match_smem_bytes(int d, int d2);
@@ -46,7 +52,8 @@ cudaError_t launch_match_list(int d, int d2, const MatchArgs& A, cudaStream_t st
 // d = 8, K <= 16, stride 1..8.  References whose candidate list overflows go
 // to A.ovf_list; launch_match_list(A with list = ovf_list) finishes them.
 bool match_tc_supported(int d, int d2, int s, int K, bool tol_branch);
-cudaError_t launch_match_tc(int d, int d2, const MatchArgs& A, cudaStream_t st);
+// f16 selects f16 operands (tensor form) instead of bf16 (precision form).
+cudaError_t launch_match_tc(int d, int d2, const MatchArgs& A, bool f16, cudaStream_t st);
 
 // ---- step 1: global 3D wavelet hard thresholding (wavelet.cu) ----------------
 struct WaveletBank {

@@ -239,67 +239,6 @@ __global__ void k_loss_grad(const float* __restrict__ pilot, const float* __rest
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-// Weight and bias gradients of one layer on the FP32 cores:
-//   dW[t][co][ci] = sum_p g[p][co] x[p + tap t][ci],  db[co] = sum_p g[p][co]
-// over the rows of every image.  Each CTA takes rows r = blockIdx.x, +gridDim.x
-// ... and writes its partial sums to part[blockIdx.x][.]; k_reduce_partials
-// adds the CTAs' partials in index order.  Thread b owns entries
-// (t, co, ci) = b + NT k (and, past the weights, the biases).
-constexpr int NT = 512;
-template <int CI_R, int CO_R, int CIN, int COUT>
-__global__ void __launch_bounds__(NT) k_dweight(const uint16_t* __restrict__ x, const uint16_t* __restrict__ g,
-                                                int nimg, int H, int W, float* __restrict__ part) {
-  constexpr int E = 9 * CO_R * CI_R;
-  constexpr int PER = (E + CO_R + NT - 1) / NT;  // entries (+ biases) per thread
-  constexpr int SEG = 32;                      // pixels per smem segment
-  __shared__ float sx[3][SEG + 2][CI_R];
-  __shared__ float sg[SEG][CO_R];
-  float acc[PER];
-#pragma unroll
-  for (int k = 0; k < PER; ++k) acc[k] = 0.f;
-  const int tid = threadIdx.x;
-  const int rows = nimg * H;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-    const int n = row / H, y = row % H;
-    for (int x0 = 0; x0 < W; x0 += SEG) {
-      __syncthreads();
-      for (int e = tid; e < 3 * (SEG + 2) * CI_R; e += NT) {
-        const int r = e / ((SEG + 2) * CI_R), q = (e / CI_R) % (SEG + 2), c = e % CI_R;
-        const int yy = y + r - 1, xx = x0 + q - 1;
-        float v = 0.f;
-        if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = bf2f(x[(((size_t)n * H + yy) * W + xx) * CIN + c]);
-        sx[r][q][c] = v;
-      }
-      for (int e = tid; e < SEG * CO_R; e += NT) {
-        const int q = e / CO_R, c = e % CO_R;
-        const int xx = x0 + q;
-        sg[q][c] = xx < W ? bf2f(g[(((size_t)n * H + y) * W + xx) * COUT + c]) : 0.f;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < PER; ++k) {
-        const int b = tid + NT * k;
-        if (b < E) {
-          const int t = b / (CO_R * CI_R), co = (b / CI_R) % CO_R, ci = b % CI_R;
-          const int dy = t / 3, dx = t % 3;
-          float a = acc[k];
-          for (int q = 0; q < SEG; ++q) a = fmaf(sg[q][co], sx[dy][q + dx][ci], a);
-          acc[k] = a;
-        } else if (b < E + CO_R) {
-          float a = acc[k];
-          for (int q = 0; q < SEG; ++q) a += sg[q][b - E];
-          acc[k] = a;
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int b = tid + NT * k;
-    if (b < E + CO_R) part[(size_t)blockIdx.x * (E + CO_R) + b] = acc[k];
-  }
-}
-
 // Weight and bias gradients of one layer on the tensor cores.  For tap
 // t = (dy, dx), dW_t[co][ci] = sum_p g[p][co] x[p + (dy-1, dx-1)][ci] is a
 // GEMM with M = co (padded to 128), N = ci and the pixels as K.  A CTA takes

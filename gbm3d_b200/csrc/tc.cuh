@@ -80,13 +80,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-blocking test of the phase with the given parity.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(mbar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Wait for the phase with the given parity, giving up after about `cycles`
-// SM clocks (returns false then).
+// SM clocks (returns false then).  The limit is checked before every
+// (potentially suspending) try_wait, so even a limit of one clock is honoured.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, long long cycles) {
   const long long t0 = clock64();
-  while (!mbar_try_wait(mbar, parity))
+  for (;;) {
+    if (mbar_test_wait(mbar, parity)) return true;
     if (clock64() - t0 > cycles) return false;
-  return true;
+    if (mbar_try_wait(mbar, parity)) return true;
+  }
 }
 
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -161,6 +176,19 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
   for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// The same read without the conversion: the registers r hold the values only
+// after tmem_wait_ld() followed by reg_fence4(r), so that several reads can be
+// in flight and no use of r is scheduled before the wait.
+__device__ __forceinline__ void tmem_ld4_async(uint32_t taddr, uint32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void reg_fence4(uint32_t* r) {
+  asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])::"memory");
+}
 
 // Whole warp: thread t writes the value x into 16 consecutive fp32 columns of
 // lane (taddr lane) + t.

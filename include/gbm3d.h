@@ -318,6 +318,24 @@ int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double s
 int gbm3d_ctx_enable_timing(gbm3d_ctx* ctx, int on);
 int gbm3d_stage_times(const gbm3d_ctx* ctx, float* ms, int n);
 
+/* Tensor-core matcher (forms 1 and 3): the limit of each of its waits for a
+ * TMA copy or its MMAs, in SM clocks (0, the default: about two seconds).  A
+ * wait that runs out ends the kernel's work after its own copies and MMAs in
+ * flight have landed, and the call reports GBM3D_ERR_CUDA ("... did not
+ * complete within its wait limit").  A negative value is a probe of that
+ * path: every CTA first waits, with the limit -cycles, on a barrier that
+ * nothing completes, so the next matching call fails that way.  Not in the
+ * reference. */
+int gbm3d_ctx_set_tc_wait(gbm3d_ctx* ctx, long long cycles);
+
+/* Tensor-core matcher statistics: with enable = 1 the following calls count,
+ * per reference block, the candidates its bound leaves for the exact re-rank
+ * (hist[b] = references with 8 b .. 8 b + 7 candidates, hist[32] = 256 or
+ * more; references with more than 64 are finished by the exhaustive matcher).  With hist non-null the counts
+ * so far are copied out (the context stream is synchronised) and reset.  Not
+ * in the reference. */
+int gbm3d_ctx_tc_stats(gbm3d_ctx* ctx, int enable, int32_t* hist);
+
 /* Number of kernels the last pipeline call launched. */
 int gbm3d_last_launch_count(const gbm3d_ctx* ctx);
 
