@@ -261,40 +261,39 @@ __global__ void __launch_bounds__(NT, 1) k_match_tc(const __grid_constant__ CUte
       const float* cand = reg + pxx * RP + py;
       float acc = 0.f;
 #pragma unroll
-      for (int r = 0; r < TD; ++r)
+      for (int h2 = 0; h2 < 2; ++h2) {  // block rows 4 h2 .. 4 h2 + 3: 32 loads in flight, then their sums
+        float cv[32];
 #pragma unroll
-        for (int c = 0; c < TD; ++c) {
-          const float tt = xr[r * TD + c] - cand[r + c * RP];
+        for (int q = 0; q < 32; ++q) cv[q] = cand[(4 * h2 + (q >> 3)) + (q & 7) * RP];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {  // element (r, c) = (4 h2 + q / 8, q % 8): row-major order
+          const float tt = xr[32 * h2 + q] - cv[q];
           acc = fmaf(tt, tt, acc);
         }
+      }
       const uint32_t ix = (uint32_t)((py - wy) + (pxx - wx) * D2);
       return ((u64)__float_as_uint(acc) << 32) | ix;
     };
-    // keys (distance bits, window index) are distinct; the K smallest in order
+    // keys (distance bits, window index) are distinct: a key's rank is the
+    // number of keys below it (independent broadcasts, no sorting network)
     if (C <= 32) {
-      u64 k0 = lane < C ? exact_key(lane) : ~0ull;
-      k0 = warp_sort_asc(k0, lane);
-      if (k0 != ~0ull && lane < K) sel[lane] = lane == 0 ? center : (uint32_t)k0 + 1u;
-    } else {  // C <= CAP = 64
-      // two sorted halves of up to 32 keys; an element's rank is its place in
-      // its own half plus the other half's keys below it
-      u64 k0 = exact_key(lane);
-      u64 k1 = lane + 32 < C ? exact_key(lane + 32) : ~0ull;
-      k0 = warp_sort_asc(k0, lane);
-      k1 = warp_sort_asc(k1, lane);
-      auto below = [&](u64 x, u64 other) {  // keys of the sorted `other` half below x
-        int lo = 0;
+      const u64 k0 = lane < C ? exact_key(lane) : ~0ull;
+      int r0 = 0;
 #pragma unroll
-        for (int bb = 16; bb >= 1; bb >>= 1) {
-          const u64 o = __shfl_sync(FULL, other, lo + bb - 1);
-          if (o < x) lo += bb;
-        }
-        const u64 o = __shfl_sync(FULL, other, lo & 31);
-        return lo + ((lo < 32 && o < x) ? 1 : 0);
-      };
-      const int r0 = lane + below(k0, k1), r1 = lane + below(k1, k0);
+      for (int i = 0; i < 32; ++i) r0 += __shfl_sync(FULL, k0, i) < k0 ? 1 : 0;
+      if (lane < C && r0 < K) sel[r0] = r0 == 0 ? center : (uint32_t)k0 + 1u;
+    } else {  // C <= CAP = 64: two keys per lane
+      const u64 k0 = exact_key(lane);
+      const u64 k1 = lane + 32 < C ? exact_key(lane + 32) : ~0ull;
+      int r0 = 0, r1 = 0;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const u64 o0 = __shfl_sync(FULL, k0, i), o1 = __shfl_sync(FULL, k1, i);
+        r0 += (o0 < k0 ? 1 : 0) + (o1 < k0 ? 1 : 0);
+        r1 += (o0 < k1 ? 1 : 0) + (o1 < k1 ? 1 : 0);
+      }
       if (r0 < K) sel[r0] = r0 == 0 ? center : (uint32_t)k0 + 1u;
-      if (k1 != ~0ull && r1 < K) sel[r1] = r1 == 0 ? center : (uint32_t)k1 + 1u;
+      if (lane + 32 < C && r1 < K) sel[r1] = r1 == 0 ? center : (uint32_t)k1 + 1u;
     }
     __syncwarp();
     if (lane < K) Sg[lane] = sel[lane];
