@@ -50,8 +50,9 @@ WL = "dense"
 STAGES = ["glue", "match1", "wavelet1", "agg1", "match2", "wiener2", "agg2", "total"]
 # arithmetic of each form: plain FP32; precision: bf16 tensor-core distances (+ exact FP32 re-rank)
 FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32", "tuned": "f32"}
-# a tuned set that takes tensor-core matching computes its distances' bound in bf16
-TUNED_DTYPE = {"plain": "f32", "tensor": "bf16+f32", "precision": "bf16+f32", "learned": "bf16+f32"}
+# a tuned set that takes tensor-core matching computes its distances' bound in f16
+# (tensor form) or bf16 (precision form); the ranking is always exact FP32
+TUNED_DTYPE = {"plain": "f32", "tensor": "f16+f32", "precision": "bf16+f32", "learned": "bf16+f32"}
 FAMILIES = ["match", "match_tc", "match_redo", "wav_analysis", "wav_synthesis", "aggregate", "wiener", "ht_weights", "make_pad",
             "accum", "ratio", "prep", "medfilt3"]
 
@@ -60,7 +61,7 @@ def describe(o: dict, name: str) -> str:
     """The timed option set in words (the line's config.workload)."""
     from gbm3d_b200 import options as _opt
     s1, s2 = _opt.strides(o)
-    matcher = {"plain": "exhaustive FP32 matching", "tensor": "tensor-core matching (bf16 distance bound, exact "
+    matcher = {"plain": "exhaustive FP32 matching", "tensor": "tensor-core matching (f16 distance bound, exact "
                "FP32 re-rank: the exhaustive matcher's match sets)", "precision": "tensor-core matching and "
                "Kahan-compensated aggregation", "learned": "learned pilot in place of step 1"}[o.get("form", "plain")]
     wav = "3D Haar" if o.get("wname") == "haar" else "bior1.5 x Haar"
@@ -212,8 +213,8 @@ REFS_1024 = 340 * 340
 TRAFFIC_TUNED_2048 = {
     (8, 6, (0,), (0,), 1, 32): (2048, {"match": 125.1e6, "wav_analysis": 177.0e6, "wav_synthesis": 177.6e6,
                                        "ht_weights": 269.2e6, "aggregate": 419.8e6, "wiener": 488.1e6}),
-    (8, 7, (0,), (0,), 1, 32): (2080, {"match": 129.9e6, "wav_analysis": 183.5e6, "wav_synthesis": 183.3e6,
-                                       "ht_weights": 277.5e6, "aggregate": 363.0e6, "wiener": 365.1e6}),
+    (8, 7, (0,), (0,), 1, 32): (2080, {"match": 131.6e6, "wav_analysis": 183.3e6, "wav_synthesis": 183.8e6,
+                                       "ht_weights": 277.5e6, "aggregate": 363.9e6, "wiener": 365.3e6}),
 }
 
 
@@ -278,8 +279,9 @@ def roofline(o, ktimes, peaks, sm_mhz):
         side, table = TRAFFIC_TUNED_2048[key]
         traffic = table.get(top)
         traffic = None if traffic is None else traffic * (Mp / side) ** 2
-        tsrc = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this option set on a 2048x2048 image, "
-                "averaged over the family's launches of one call and scaled by the padded area (bytes per launch)")
+        tsrc = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this option set on a 2048x2048 image "
+                "(capture restricted to the six pipeline kernels, one call), averaged over the family's launches "
+                "and scaled by the padded area (bytes per launch)")
     else:
         traffic = TRAFFIC_1024[top] * G1 / REFS_1024 if top in TRAFFIC_1024 else None
         tsrc = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one step-1 launch of the dense workload on "
