@@ -84,10 +84,12 @@ void argfail(gbm3d_ctx* c, const std::string& s, int code = GBM3D_ERR_ARG) {
 }
 
 // Device status word: bit 0 non-finite input (k_prep), bit 1 a tensor-core
-// matcher wait (TMA copy or MMA) that ran out of its limit (the kernel gave up).
+// matcher wait (TMA copy or MMA) that ran out of its limit (the kernel gave up),
+// bit 2 the exhaustive matcher's wait for a search-window copy (likewise).
 void report_flag(gbm3d_ctx* c, int flag) {
   if (flag & 1) argfail(c, "input image holds NaN or Inf", GBM3D_ERR_NONFINITE);
   if (flag & 2) argfail(c, "tensor-core matcher: a TMA copy or MMA did not complete within its wait limit", GBM3D_ERR_CUDA);
+  if (flag & 4) argfail(c, "matcher: a search-window TMA copy did not complete within its wait limit", GBM3D_ERR_CUDA);
 }
 
 template <class T>
@@ -994,6 +996,10 @@ int gbm3d_ctx_synchronize(gbm3d_ctx* c) {
     }
     if (flag & 2) {
       c->err = "tensor-core matcher: a TMA copy or MMA did not complete within its wait limit";
+      return GBM3D_ERR_CUDA;
+    }
+    if (flag & 4) {
+      c->err = "matcher: a search-window TMA copy did not complete within its wait limit";
       return GBM3D_ERR_CUDA;
     }
   }

@@ -1,5 +1,7 @@
 // Launch interfaces of the GBM3D kernels (host side of each .cu file).
 #pragma once
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace gbm3d {
@@ -20,7 +22,8 @@ struct MatchArgs {
   int m, n;           // volume rows/cols: the image for s = d, (M d) x (N d) otherwise
   float* V1;          // d x d x K x M x N gathers (may be null)
   float* V2;
-  int* err;           // bit 1 set by the tensor-core matcher when a wait times out (may be null)
+  int* err;           // status word (may be null): bit 1 a tensor-core matcher wait ran out, bit 2
+                      // the exhaustive matcher's wait for its search-window copy ran out
   int R, Q;           // rows and columns of the search image (m + d2, n + d2)
   // tensor-core matcher: references whose candidate set overflowed its list
   // are appended here (count first zeroed) and searched exhaustively after it
@@ -37,6 +40,11 @@ struct MatchArgs {
   int* cand_hist;
 };
 bool match_supported(int d, int d2);
+// 2-D fp32 tensor map of a search image (R rows, the inner dimension, of
+// pitch P floats; Q columns) with a box of box_rows x box_cols, zero fill past
+// its end, no multicast.  False when the driver's encoder is unavailable or
+// the image is not TMA-addressable (16-byte aligned base, P a multiple of 4).
+bool encode_search_map(CUtensorMap* tm, const float* pad, int R, int Q, int P, int box_rows, int box_cols);
 size_t match_smem_bytes(int d, int d2);
 cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st);
 cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,

@@ -15,12 +15,45 @@
 // smallest (distance, column-major window index) pairs — the stable order of
 // MATLAB's mink — found by a bitwise radix search for the K-th smallest
 // distance with warp reductions, then an index-ordered pick among ties.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tc.cuh"
 
 namespace gbm3d {
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+}  // namespace
+
+bool encode_search_map(CUtensorMap* tm, const float* pad, int R, int Q, int P, int box_rows, int box_cols) {
+  auto encode = encode_fn();
+  if (!encode || (reinterpret_cast<uintptr_t>(pad) & 15) || (P & 3) || R < 1 || Q < 1 || P < R) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)R, (cuuint64_t)Q};
+  const cuuint64_t strides[1] = {(cuuint64_t)P * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)box_rows, (cuuint32_t)box_cols};
+  const cuuint32_t es[2] = {1, 1};
+  return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(pad), dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 // Ipad of the reference for a circularly shifted image: rows (m+d2), cols
 // (n+d2), column pitch P floats.  spin is the circshift applied to the image.
@@ -43,22 +76,44 @@ __global__ void k_make_pad(const float* __restrict__ img, int m, int n, int h, i
   pad[y + (size_t)x * P] = img[src(y, m) + (size_t)src(x, n) * m];
 }
 
-// The search of reference g by one warp: win holds (D + D2 - 1)^2 floats of
-// shared memory, lst 224 words (keys, indices, S and the bounded set).
+// Column pitch of a staged search window of WD rows: its first row sits up to
+// 3 rows into a TMA box that starts on a 16-byte boundary.
+__host__ __device__ constexpr int win_pitch(int wd) { return (wd + 3 + 3) & ~3; }
+// Floats of one warp's window buffer (a multiple of 32: 128-byte aligned buffers).
+__host__ __device__ constexpr int win_floats(int wd) { return (win_pitch(wd) * wd + 31) & ~31; }
+constexpr long long MATCH_WAIT_CYCLES = 4000000000LL;  // ~2 s at 2 GHz
+
+// The search of reference g by one warp: win holds win_floats(D + D2 - 1)
+// floats of shared memory (128-byte aligned), lst 224 words (keys, indices, S
+// and the bounded set), mbar the warp's mbarrier (phase: its parity).
 template <int D, int D2>
-__device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float* win, uint32_t* lst,
-                                          const int lane) {
+__device__ __forceinline__ void match_ref(const MatchArgs& A, const CUtensorMap* tmap, const int g, float* win,
+                                          uint32_t* lst, uint64_t* mbar, uint32_t& phase, const int lane) {
   constexpr int WD = D + D2 - 1;  // window rows/cols that candidates touch
+  constexpr int WP = win_pitch(WD);
   constexpr int H = D2 / 2;
   const int i = g % A.M, j = g / A.M;
 
-  // ---- stage the search window (column-major, stride WD) --------------------
-  const float* src = A.pad + (size_t)i * A.s + (size_t)j * A.s * A.P;
-  for (int t = lane; t < WD * WD; t += 32) {  // flat over the window: every lane busy
-    const int c = t / WD, r = t - c * WD;
-    win[t] = src[r + (size_t)c * A.P];
+  // ---- stage the search window: one TMA copy (this GPU's search image, no
+  // multicast) of a WP x WD box whose first row i s is rounded down to a
+  // multiple of 4 (a 16-byte aligned coordinate); the window starts o rows
+  // into each staged column.  Rows past the search image read as zero.
+  const int y0 = i * A.s, o = y0 & 3;
+  if (lane == 0) {
+    tc::fence_proxy_async();  // this warp's earlier reads of the buffer come first
+    tc::mbar_expect_tx(mbar, WP * WD * (int)sizeof(float));
+    tc::tma_load_2d(win, tmap, y0 - o, j * A.s, mbar);
   }
-  __syncwarp();
+  if (!tc::mbar_wait(mbar, phase, MATCH_WAIT_CYCLES)) {
+    // the copy did not land in time: give it the full limit again before the
+    // buffer is reused, report, and leave this reference's S unwritten
+    tc::mbar_wait(mbar, phase, MATCH_WAIT_CYCLES);
+    phase ^= 1u;
+    if (lane == 0 && A.err) atomicOr(A.err, 4);
+    return;
+  }
+  phase ^= 1u;
+  const float* wv = win + o;
 
   // ---- exact SSD for the lane's candidates (a = lane, b = 0..D2-1) ----------
   // Candidate b sees t = x(r, c) - y, acc = fmaf(t, t, acc) in (r, c) order
@@ -71,11 +126,11 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float
   for (int r = 0; r < D; ++r) {
     float xr[D];
 #pragma unroll
-    for (int c = 0; c < D; ++c) xr[c] = win[(H + r) + (H + c) * WD];
-    const float* wrow = win + (a + r);
+    for (int c = 0; c < D; ++c) xr[c] = wv[(H + r) + (H + c) * WP];
+    const float* wrow = wv + (a + r);
 #pragma unroll
     for (int xw = 0; xw < WD; ++xw) {
-      const float w = wrow[xw * WD];
+      const float w = wrow[xw * WP];
 #pragma unroll
       for (int b = 0; b < D2; ++b) {
         const int c = xw - b;
@@ -102,7 +157,7 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float
     float nR = 0.f;
     for (int c = 0; c < D; ++c)
       for (int r = 0; r < D; ++r) {
-        const float xv = win[(H + r) + (H + c) * WD];
+        const float xv = wv[(H + r) + (H + c) * WP];
         nR = fmaf(xv, xv, nR);
       }
     int nf = 0;
@@ -247,13 +302,13 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float
         const int e = (int)lS[k] - 1;
         if ((unsigned)e < (unsigned)(D2 * D2)) { aa = e % D2; bb = e / D2; }
       }
-      const float* wsrc = win + aa + bb * WD;
+      const float* wsrc = wv + aa + bb * WP;
 #pragma unroll
       for (int u = 0; u < (D * D + 31) / 32; ++u) {
         const int t = lane + 32 * u;
         if (t < D * D) {
           const int r = t % D, c = t / D;
-          vol0[(size_t)r + (size_t)A.m * c + mn * k] = wsrc[r + c * WD];
+          vol0[(size_t)r + (size_t)A.m * c + mn * k] = wsrc[r + c * WP];
         }
       }
     }
@@ -268,47 +323,76 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const int g, float
       float* o2 = A.V2 ? A.V2 + (size_t)D * D * (k + (size_t)K * g) : nullptr;
       for (int t = lane; t < D * D; t += 32) {
         const int r = t % D, c = t / D;
-        if (o1) o1[t] = win[(aa + r) + (bb + c) * WD];
+        if (o1) o1[t] = wv[(aa + r) + (bb + c) * WP];
         if (o2) o2[t] = src2[(aa + r) + (size_t)(bb + c) * A.P];
       }
     }
   }
 }
 
+// Shared memory of a 4-warp CTA: the warps' window buffers, their lst words,
+// their mbarriers.
 template <int D, int D2>
-__global__ void __launch_bounds__(128) k_match(MatchArgs A) {
-  constexpr int WD = D + D2 - 1;
-  extern __shared__ float smem[];
+struct MatchSmem {
+  static constexpr int WF = win_floats(D + D2 - 1);
+  static constexpr size_t LST = (size_t)4 * WF * sizeof(float);
+  static constexpr size_t MBAR = LST + (size_t)4 * 224 * sizeof(uint32_t);
+  static constexpr size_t BYTES = MBAR + 4 * sizeof(uint64_t);
+};
+
+template <int D, int D2>
+__global__ void __launch_bounds__(128) k_match(const __grid_constant__ CUtensorMap tmap, MatchArgs A) {
+  using SM = MatchSmem<D, D2>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = blockIdx.x * 4 + warp;
   if (g >= A.M * A.N) return;  // warp-uniform
-  match_ref<D, D2>(A, g, smem + warp * (WD * WD), reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 224, lane);
+  float* win = reinterpret_cast<float*>(smem_raw) + warp * SM::WF;
+  uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw + SM::LST) + warp * 224;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + SM::MBAR) + warp;
+  if (lane == 0) {
+    tc::mbar_init(mbar, 1);
+    tc::fence_mbar_init();
+  }
+  __syncwarp();
+  uint32_t phase = 0;
+  match_ref<D, D2>(A, &tmap, g, win, lst, mbar, phase, lane);
 }
 
 // List mode: the references A.list[0 .. *A.list_count), grid-stride over the list.
 template <int D, int D2>
-__global__ void __launch_bounds__(128) k_match_list(MatchArgs A) {
-  constexpr int WD = D + D2 - 1;
-  extern __shared__ float smem[];
+__global__ void __launch_bounds__(128) k_match_list(const __grid_constant__ CUtensorMap tmap, MatchArgs A) {
+  using SM = MatchSmem<D, D2>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* win = smem + warp * (WD * WD);
-  uint32_t* lst = reinterpret_cast<uint32_t*>(smem + 4 * WD * WD) + warp * 224;
+  float* win = reinterpret_cast<float*>(smem_raw) + warp * SM::WF;
+  uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw + SM::LST) + warp * 224;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + SM::MBAR) + warp;
+  if (lane == 0) {
+    tc::mbar_init(mbar, 1);
+    tc::fence_mbar_init();
+  }
+  __syncwarp();
+  uint32_t phase = 0;
   const int n = *A.list_count;
   for (int t = blockIdx.x * 4 + warp; t < n; t += gridDim.x * 4) {
     const int g = A.list[t];
-    if ((unsigned)g < (unsigned)(A.M * A.N)) match_ref<D, D2>(A, g, win, lst, lane);
+    if ((unsigned)g < (unsigned)(A.M * A.N)) match_ref<D, D2>(A, &tmap, g, win, lst, mbar, phase, lane);
     __syncwarp();  // the next reference restages win and lst
   }
 }
 
 size_t match_smem_bytes(int d, int d2) {
   const int wd = d + d2 - 1;
-  return (size_t)4 * wd * wd * sizeof(float) + 4 * 224 * sizeof(uint32_t);
+  return (size_t)4 * win_floats(wd) * sizeof(float) + 4 * 224 * sizeof(uint32_t) + 4 * sizeof(uint64_t);
 }
 
 template <int D, int D2>
 static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
-  const size_t sm = match_smem_bytes(D, D2);
+  constexpr int WD = D + D2 - 1;
+  const size_t sm = MatchSmem<D, D2>::BYTES;
+  CUtensorMap tm;
+  if (!encode_search_map(&tm, A.pad, A.R, A.Q, A.P, win_pitch(WD), WD)) return cudaErrorInvalidValue;
   // The attribute belongs to the current device, so it is set before every
   // launch (a host-side call that costs well under a microsecond) rather than
   // remembered once per process: a second device, or another host thread on
@@ -316,19 +400,22 @@ static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   cudaError_t e = cudaFuncSetAttribute(k_match<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
-  k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(A);
+  k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(tm, A);
   return cudaGetLastError();
 }
 
 template <int D, int D2>
 static cudaError_t launch_match_list_t(const MatchArgs& A, cudaStream_t st) {
-  const size_t sm = match_smem_bytes(D, D2);
+  constexpr int WD = D + D2 - 1;
+  const size_t sm = MatchSmem<D, D2>::BYTES;
+  CUtensorMap tm;
+  if (!encode_search_map(&tm, A.pad, A.R, A.Q, A.P, win_pitch(WD), WD)) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_match_list<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.M * A.N;
   // enough warps for the rare references a list holds; the rest exit at once
   const int blocks = std::min((G + 3) / 4, 2 * 148);
-  k_match_list<D, D2><<<blocks, 128, sm, st>>>(A);
+  k_match_list<D, D2><<<blocks, 128, sm, st>>>(tm, A);
   return cudaGetLastError();
 }
 

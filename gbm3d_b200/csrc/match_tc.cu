@@ -60,10 +60,8 @@
 // and ends the CTA's work, after letting its own copies and MMAs in flight
 // land with the full limit; TMEM is always released.
 #include <cuda.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -642,34 +640,11 @@ __global__ void __launch_bounds__(NT, 1) k_match_tc(const __grid_constant__ CUte
   if (warp == 0) tc::tmem_dealloc(tmem, 512);
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  });
-  return fn;
-}
-
 template <int D2, bool HALF>
 cudaError_t launch_tc_t(const MatchArgs& A, cudaStream_t st) {
-  auto encode = encode_fn();
-  if (!encode) return cudaErrorNotSupported;
   // the search image: rows (inner) R of pitch P floats, columns Q; box RP x RC
   CUtensorMap tm;
-  const cuuint64_t dims[2] = {(cuuint64_t)A.R, (cuuint64_t)A.Q};
-  const cuuint64_t strides[1] = {(cuuint64_t)A.P * sizeof(float)};
-  const cuuint32_t box[2] = {RP, RC};
-  const cuuint32_t es[2] = {1, 1};
-  if (encode(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(A.pad), dims, strides, box, es,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return cudaErrorInvalidValue;
+  if (!encode_search_map(&tm, A.pad, A.R, A.Q, A.P, RP, RC)) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_match_tc<D2, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(A.ovf_count, 0, sizeof(int), st);

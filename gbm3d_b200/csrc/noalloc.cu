@@ -80,6 +80,8 @@ extern "C" int gbm3d_matchBlocks_noalloc(const float* I, int m, int n, double si
   A.cnt = S_count;
   A.m = m;
   A.n = n;
+  A.R = m + d2;  // the search image's rows and columns (the matcher's TMA tensor map)
+  A.Q = n + d2;
   if (gbm3d::launch_match(d, d2, A, st) != cudaSuccess) return GBM3D_ERR_CUDA;
   return GBM3D_OK;
 }
