@@ -293,9 +293,24 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const CUtensorMap*
 
   // ---- optional gathers: Volume (matchBlocksCPU.m:107-114), V1/V2 (matchBlocksWie.m:85-89)
   if (A.volume) {
-    // lane-parallel over the block: element t = lane + 32 u is row t % D, column t / D
     const size_t mn = (size_t)A.m * A.n;
     float* vol0 = A.volume + (size_t)(i * D) + (size_t)A.m * (j * D);
+    if (D == 8 && (A.m & 3) == 0 && (reinterpret_cast<uintptr_t>(A.volume) & 15) == 0) {
+      // two slots per pass: lane = (slot parity, column c, half-column r0); each
+      // lane stores four rows of one column as one 16-byte store (a block
+      // column is 32 contiguous bytes of the volume, 16-byte aligned here)
+      const int q = lane & 15, c = q >> 1, r0 = 4 * (q & 1);
+      for (int k = lane >> 4; k < K; k += 2) {
+        int aa = H, bb = H;
+        if (k < count) {
+          const int e = (int)lS[k] - 1;
+          if ((unsigned)e < (unsigned)(D2 * D2)) { aa = e % D2; bb = e / D2; }
+        }
+        const float* ws = wv + aa + r0 + (bb + c) * WP;
+        *reinterpret_cast<float4*>(vol0 + r0 + (size_t)A.m * c + mn * k) = make_float4(ws[0], ws[1], ws[2], ws[3]);
+      }
+    } else {
+    // lane-parallel over the block: element t = lane + 32 u is row t % D, column t / D
     for (int k = 0; k < K; ++k) {
       int aa = H, bb = H;
       if (k < count) {
@@ -311,6 +326,7 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const CUtensorMap*
           vol0[(size_t)r + (size_t)A.m * c + mn * k] = wsrc[r + c * WP];
         }
       }
+    }
     }
   }
   if (A.V1 || A.V2) {
