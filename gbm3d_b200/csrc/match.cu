@@ -57,11 +57,13 @@ bool encode_search_map(CUtensorMap* tm, const float* pad, int R, int Q, int P, i
 
 // Ipad of the reference for a circularly shifted image: rows (m+d2), cols
 // (n+d2), column pitch P floats.  spin is the circshift applied to the image.
+// A thread writes rows 4 t .. 4 t + 3 of column x as one 16-byte store (P is a
+// multiple of 4; rows R .. P-1 of the pitch are never read as image rows).
 __global__ void k_make_pad(const float* __restrict__ img, int m, int n, int h, int spin,
                            float* __restrict__ pad, int P, int R, int Q) {
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int x = blockIdx.y;
-  if (y >= R || x >= Q) return;
+  if (y0 >= P || x >= Q) return;
   // (pad_index(r) - spin) mod L without divisions when h <= L and 0 <= spin <= L
   // (r < L + 2h, so pad_index needs at most one wrap); the general form otherwise
   auto src = [&](int r, int L) {
@@ -73,7 +75,9 @@ __global__ void k_make_pad(const float* __restrict__ img, int m, int n, int h, i
     }
     return pmod(pad_index(r, L, h) - spin, L);
   };
-  pad[y + (size_t)x * P] = img[src(y, m) + (size_t)src(x, n) * m];
+  const float* col = img + (size_t)src(x, n) * m;
+  const float4 v = make_float4(col[src(y0, m)], col[src(y0 + 1, m)], col[src(y0 + 2, m)], col[src(y0 + 3, m)]);
+  *reinterpret_cast<float4*>(pad + y0 + (size_t)x * P) = v;
 }
 
 // Column pitch of a staged search window of WD rows: its first row sits up to
@@ -490,7 +494,8 @@ cudaError_t launch_gather_volume(const float* pad, int P, int M, int N, int s, i
 cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
                             cudaStream_t st) {
   const int R = m + d2, Q = n + d2;
-  dim3 grid((R + 255) / 256, Q);
+  dim3 grid((P / 4 + 255) / 256, Q);
+  if ((P & 3) || P < R || (reinterpret_cast<uintptr_t>(pad) & 15)) return cudaErrorInvalidValue;
   k_make_pad<<<grid, 256, 0, st>>>(img, m, n, d2 / 2, spin, pad, P, R, Q);
   return cudaGetLastError();
 }
