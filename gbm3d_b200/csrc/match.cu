@@ -197,11 +197,43 @@ __device__ __forceinline__ void match_ref(const MatchArgs& A, const CUtensorMap*
         const bool up = ((lane & k2) == 0), lower = ((lane & j2) == 0);
         v = (lower == up) ? min(v, o) : max(v, o);
       }
-    const uint32_t T = __shfl_sync(FULL, v, want - 1);
+    uint32_t T = __shfl_sync(FULL, v, want - 1);
     int cl = 0;
 #pragma unroll
     for (int b = 0; b < D2; ++b) cl += key[b] <= T ? 1 : 0;
-    const int C = __reduce_add_sync(FULL, cl);
+    int C = __reduce_add_sync(FULL, cl);
+    if (T != 0xffffffffu && C > 64) {
+      // Tighter bound (smooth images, where many keys tie with the lane
+      // minima): T2 = the want-th smallest of the 64 values {lane minimum,
+      // lane second minimum}, still >= the want-th smallest key.  With A the
+      // sorted minima and B the sorted second minima, the want-th smallest of
+      // A u B is the smallest max(A[i-1], B[want-1-i]) over i = 0..want.
+      uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu;
+#pragma unroll
+      for (int b = 0; b < D2; ++b) {
+        const uint32_t kb = key[b];
+        if (kb < m1) { m2 = m1; m1 = kb; } else if (kb < m2) m2 = kb;
+      }
+      uint32_t vb = m2;
+#pragma unroll
+      for (int k2 = 2; k2 <= 32; k2 <<= 1)
+#pragma unroll
+        for (int j2 = k2 >> 1; j2 > 0; j2 >>= 1) {
+          const uint32_t o = __shfl_xor_sync(FULL, vb, j2);
+          const bool up = ((lane & k2) == 0), lower = ((lane & j2) == 0);
+          vb = (lower == up) ? min(vb, o) : max(vb, o);
+        }
+      const uint32_t a_prev = __shfl_sync(FULL, v, (lane + 31) & 31);          // A[lane - 1]
+      const uint32_t b_pair = __shfl_sync(FULL, vb, (want - 1 - lane) & 31);  // B[want - 1 - lane]
+      uint32_t cand = 0xffffffffu;
+      if (lane <= want - 1)  // i = lane in 0 .. want - 1 (i = want is T itself)
+        cand = max(lane == 0 ? 0u : a_prev, b_pair);
+      T = min(T, __reduce_min_sync(FULL, cand));
+      cl = 0;
+#pragma unroll
+      for (int b = 0; b < D2; ++b) cl += key[b] <= T ? 1 : 0;
+      C = __reduce_add_sync(FULL, cl);
+    }
     if (T != 0xffffffffu && C <= 64) {
       int pos = cl;
 #pragma unroll
@@ -361,7 +393,7 @@ struct MatchSmem {
 };
 
 template <int D, int D2>
-__global__ void __launch_bounds__(128) k_match(const __grid_constant__ CUtensorMap tmap, MatchArgs A) {
+__global__ void __launch_bounds__(128, 7) k_match(const __grid_constant__ CUtensorMap tmap, MatchArgs A) {
   using SM = MatchSmem<D, D2>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

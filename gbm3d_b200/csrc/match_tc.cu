@@ -51,7 +51,7 @@
 //
 // Schedule: one persistent CTA of 16 warps per SM takes tiles from a device
 // work queue.  Per tile t: tables, E and the reference operand; TMEM
-// initialisation and the 112 MMAs (one thread issues, one commit); while they
+// initialisation and the 112 MMAs (lane 0 of 8 warps issues, one commit each); while they
 // run, the exact re-rank of tile t-1; then pass 1, thresholds and pass 2.  The
 // region of tile t+2 is loaded by TMA meanwhile (three region buffers).
 //
