@@ -68,6 +68,8 @@ __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
   const int j_lo = max(0, ceil_div(PC0 - D - D2 + 2, s)), j_hi = min(A.N - 1, floor_div(PC0 + CC - 1, s));
   const int NI = i_hi - i_lo + 1, NJ = j_hi - j_lo + 1;
   const int total = (NI > 0 && NJ > 0) ? NI * NJ * K : 0;
+  const unsigned invK = K > 1 ? (unsigned)(0xFFFFFFFFu / (unsigned)K) + 1u : 0u;  // ceil(2^32 / K)
+  const unsigned invNJ = NJ > 1 ? (unsigned)(0xFFFFFFFFu / (unsigned)NJ) + 1u : 0u;
   const size_t mn = (size_t)mv * (A.N * D);
   const unsigned FULL = 0xffffffffu;
 
@@ -183,8 +185,10 @@ __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
     bool hit = false;
     int4 ent = make_int4(0, 0, 0, 0);
     if (q < total) {
-      const int r2 = q / K, k = q - r2 * K;
-      const int i2 = r2 / NJ;
+      // q / K and r2 / NJ by multiply-high with ceil(2^32 / divisor): exact
+      // for dividends below 2^32 / divisor (here below NI NJ K < 2^20)
+      const int r2 = K > 1 ? (int)__umulhi((unsigned)q, invK) : q, k = q - r2 * K;
+      const int i2 = NJ > 1 ? (int)__umulhi((unsigned)r2, invNJ) : r2;
       const int i = i_lo + i2, j = j_lo + (r2 - i2 * NJ);
       const int g = i + A.M * j;
       const int nm = A.cnt ? A.cnt[g] : K;
