@@ -45,7 +45,6 @@ bool match_supported(int d, int d2);
 // its end, no multicast.  False when the driver's encoder is unavailable or
 // the image is not TMA-addressable (16-byte aligned base, P a multiple of 4).
 bool encode_search_map(CUtensorMap* tm, const float* pad, int R, int Q, int P, int box_rows, int box_cols);
-size_t match_smem_bytes(int d, int d2);
 cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st);
 cudaError_t launch_make_pad(const float* img, int m, int n, int d2, int spin, float* pad, int P,
                             cudaStream_t st);

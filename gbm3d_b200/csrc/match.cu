@@ -434,11 +434,6 @@ __global__ void __launch_bounds__(128) k_match_list(const __grid_constant__ CUte
   }
 }
 
-size_t match_smem_bytes(int d, int d2) {
-  const int wd = d + d2 - 1;
-  return (size_t)4 * win_floats(wd) * sizeof(float) + 4 * 224 * sizeof(uint32_t) + 4 * sizeof(uint64_t);
-}
-
 template <int D, int D2>
 static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   constexpr int WD = D + D2 - 1;
