@@ -49,7 +49,8 @@ WORKLOADS = {
 WL = "dense"
 STAGES = ["glue", "match1", "wavelet1", "agg1", "match2", "wiener2", "agg2", "total"]
 # arithmetic of each form: plain FP32; precision: bf16 tensor-core distances (+ exact FP32 re-rank)
-FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32", "tuned": "f32"}
+FORM_DTYPE = {"plain": "f32", "precision": "bf16+f32", "learned": "bf16+f32", "tuned": "f32",
+              "tuned_tensor": "f16+f32", "tuned_precision": "bf16+f32"}
 # a tuned set that takes tensor-core matching computes its distances' bound in f16
 # (tensor form) or bf16 (precision form); the ranking is always exact FP32
 TUNED_DTYPE = {"plain": "f32", "tensor": "f16+f32", "precision": "bf16+f32", "learned": "bf16+f32"}
@@ -626,6 +627,12 @@ def run_ours(args):
                 tuning = autotune.tune(size=SIZE, sigma=SIGMA, ctx=ctx, log=None)
             tuning = bcast(tuning)  # every rank runs rank 0's choice
             form_opts["tuned"] = dict(o_plain, **tuning["opts"])
+    if "tuned" in forms and args.form == "auto" and autotune._tensor_ok(form_opts["tuned"]):
+        # the tuned option set with tensor-core matching: the tensor form (the
+        # same output) and the precision form (Kahan aggregation) at those strides
+        for f, fo in (("tuned_tensor", "tensor"), ("tuned_precision", "precision")):
+            forms.append(f)
+            form_opts[f] = dict(form_opts["tuned"], form=fo)
     res = {f: measure(form_opts[f], True) for f in forms}
     plain = res["plain"]
     if "learned" in res:
