@@ -213,6 +213,20 @@ def test_denoiseAndAggregateGPU_median(gpu, oracle):
     assert np.array_equal(U, Uo) and np.array_equal(W, Wo)
 
 
+@pytest.mark.parametrize("K,s", [(8, 8), (8, 5), (32, 8)])
+def test_GBM3D_pipeline_group_sizes(gpu, oracle, K, s):
+    """Groups of 8 and 32 slots (the aggregation's enumeration divides by K
+    with a multiply-high; the wavelet and Wiener passes run 8 or 32 slots).
+    NaN compares equal: with fewer than 15 slots an all-zero pilot group gets
+    an infinite Wiener weight in the reference's arithmetic too."""
+    clean, noisy = synth.noisy_image(120, 136, 25.0, seed=40 + K + s)
+    o = _opts(blockSize=8, blockSizeWie=8, numMax=K, numMin=K, refStride=s, refStrideWie=s)
+    U, out = gpu.GBM3D(noisy, 25.0, o)
+    Uo, U1o = oracle.GBM3D(noisy, 25.0, o, prec=32)
+    assert np.array_equal(out["U1"], U1o, equal_nan=True), "step-1 estimate not bit-identical"
+    assert np.array_equal(U, Uo, equal_nan=True), "final estimate not bit-identical"
+
+
 def test_GBM3D_pipeline_median(gpu, oracle):
     clean, noisy = synth.noisy_image(96, 96, 25.0, seed=32)
     o = dict(_opts(), filtType="median")
