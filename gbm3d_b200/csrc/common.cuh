@@ -26,6 +26,15 @@ __host__ __device__ __forceinline__ int pad_index(int r, int L, int h) {
   return r < h ? r + h : (r - h) % L;
 }
 
+// 4-byte asynchronous global -> shared copy: no register round trip, so all of
+// a tile's or a group's loads are in flight together.  The copying thread calls
+// cp_async_wait_all() before the barrier (or __syncwarp) that publishes them.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // One axis of a separable filter bank with its nonzero taps in ascending order.
 struct Taps {
   int n;

@@ -388,10 +388,11 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restri
 #pragma unroll
       for (int t = 0; t < QT; ++t) {
         const int qyl = lane + 32 * t;
-        if (qyl < NQY) dst[qyl] = __ldg(src + qyv[t]);
+        if (qyl < NQY) cp_async4(dst + qyl, src + qyv[t]);
       }
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   // y-pass: item = (comb, run, qx); outputs py = 16 run .. 16 run + 15 of column qx
   constexpr int NRUN = FSY / 16;

@@ -137,11 +137,12 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
       for (int u = 0; u < NU; ++u) {
         const int t = lane + 32 * u;
         if (t < DD) {
-          b1[k * PG + t] = __ldg(A.padP + o + toff[u]);
-          b2[k * PG + t] = __ldg(A.padN + o + toff[u]);
+          cp_async4(b1 + k * PG + t, A.padP + o + toff[u]);
+          cp_async4(b2 + k * PG + t, A.padN + o + toff[u]);
         }
       }
     }
+    cp_async_wait_all();
   } else {
     const float* v1 = A.V1 + (size_t)g * GS;
     const float* v2 = A.V2 + (size_t)g * GS;
