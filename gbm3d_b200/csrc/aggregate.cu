@@ -191,9 +191,14 @@ __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
       const int i2 = NJ > 1 ? (int)__umulhi((unsigned)r2, invNJ) : r2;
       const int i = i_lo + i2, j = j_lo + (r2 - i2 * NJ);
       const int g = i + A.M * j;
-      const int nm = A.cnt ? A.cnt[g] : K;
+      // the count, the match index and the group weight are independent
+      // loads: all three in flight before the count test (S holds K entries
+      // per group whatever the count)
+      const int nm = A.cnt ? __ldg(A.cnt + g) : K;
+      const int eS = (int)__ldg(A.S + (size_t)g * K + k) - 1;
+      const float gwv = WIE ? 0.f : __ldg(A.gw + g);
       if (k < nm) {
-        const int e = (int)A.S[(size_t)g * K + k] - 1;
+        const int e = eS;
         const int r0 = i * s + e % D2 - PR0, c0 = j * s + e / D2 - PC0;
         hit = r0 < CR && r0 + D > 0 && c0 < CC && c0 + D > 0;
         if (hit) {
@@ -203,7 +208,7 @@ __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
             ent.z = g * (D * D);
           } else {
             ent.y = (int)((size_t)i * D + (size_t)mv * (j * D) + mn * k);
-            ent.z = __float_as_int(A.gw[g]);
+            ent.z = __float_as_int(gwv);
           }
         }
       }

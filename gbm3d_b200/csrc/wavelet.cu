@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
   int gy[RT];
 #pragma unroll
   for (int t = 0; t < RT; ++t) gy[t] = wrap1(y0 + lane + 32 * t, Ly);
-#pragma unroll 2
+#pragma unroll 3
   for (int xx = w; xx < NX; xx += 8) {
     const float* col = in + (size_t)Ly * wrap1(x0 + xx, Lx);
 #pragma unroll
