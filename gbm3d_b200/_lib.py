@@ -81,6 +81,9 @@ _SIGS = {
     "gbm3d_denoise": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise_device": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P, _P]),
     "gbm3d_denoise_async": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), _P]),
+    "gbm3d_denoise_strip_device": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_double, C.POINTER(gbm3d_opts), C.c_int,
+                                             C.c_int, _P]),
+    "gbm3d_strip_work": (C.c_int, [C.POINTER(gbm3d_opts), C.c_int, C.c_int, C.c_int, C.c_int, _P]),
     "gbm3d_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "gbm3d_ctx_set_tc_wait": (C.c_int, [_P, C.c_longlong]),
     "gbm3d_ctx_tc_stats": (C.c_int, [_P, C.c_int, _P]),

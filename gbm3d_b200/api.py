@@ -286,6 +286,30 @@ def GBM3D_device(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dic
                                          C.c_void_p(U_ptr), C.c_void_p(U1_ptr or 0)))
 
 
+def GBM3D_strip_device(I_ptr: int, m: int, n: int, sigma: float, col_lo: int, col_hi: int, U_ptr: int,
+                       opts: dict | None = None, ctx: Context | None = None) -> None:
+    """Strip form: columns [col_lo, col_hi) of GBM3D_device's result (bit-identical
+    to them) into U_ptr (float64, column-major m x (col_hi - col_lo)) from the
+    whole image I_ptr (m x n), asynchronous on the context stream.  The options
+    resolve for the whole image's size, as the whole-image call does."""
+    ctx = ctx or context()
+    co = c_opts(_opt.resolve_opts(opts, shape=(m, n), sigma=sigma))
+    ctx.check(lib().gbm3d_denoise_strip_device(ctx.h, C.c_void_p(I_ptr), m, n, float(sigma), C.byref(co),
+                                               int(col_lo), int(col_hi), C.c_void_p(U_ptr)))
+
+
+def strip_work(m: int, n: int, col_lo: int, col_hi: int, opts: dict | None = None,
+               sigma: float | None = None) -> tuple[float, float]:
+    """Share of the whole image's references that the strip [col_lo, col_hi)
+    matches in step 1 and step 2 (host only, no GPU)."""
+    co = c_opts(_opt.resolve_opts(opts, shape=(m, n), sigma=sigma))
+    frac = (C.c_double * 2)()
+    rc = lib().gbm3d_strip_work(C.byref(co), m, n, int(col_lo), int(col_hi), frac)
+    if rc != 0:
+        raise GBM3DError(rc, "gbm3d_strip_work: invalid arguments")
+    return float(frac[0]), float(frac[1])
+
+
 def GBM3D_async(I_ptr: int, m: int, n: int, sigma: float, U_ptr: int, opts: dict | None = None,
                 ctx: Context | None = None) -> None:
     """Enqueue one whole denoise of a host image (I_ptr: pinned float64,

@@ -58,8 +58,9 @@ __global__ void __launch_bounds__(NTC) k_aggregate_cta(AggArgs A) {
   int4* lst = lstC + CAPC + warp * LCAP;
   if (!WIE)
     for (int t = tid; t < D * D; t += NTC) win[t] = A.win[t];
-  const int tiles_r = (A.m + CR - 1) / CR;
-  const int R0 = (blockIdx.x % tiles_r) * CR, C0 = (blockIdx.x / tiles_r) * CC;
+  const int tiles_r = (A.m + CR - 1) / CR, tiles_c = (A.n + CC - 1) / CC;
+  const int tcol = (int)(blockIdx.x / tiles_r) + A.ct0;  // the window's column tiles, modulo the count
+  const int R0 = (blockIdx.x % tiles_r) * CR, C0 = (tcol >= tiles_c ? tcol - tiles_c : tcol) * CC;
   const int K = A.K, s = A.s;
   const int mv = A.M * D;
   constexpr int H = D2 / 2;
@@ -248,8 +249,12 @@ static cudaError_t launch_px_cap(const AggArgs& A, cudaStream_t st) {
   cudaError_t e = cudaFuncSetAttribute(k_aggregate_cta<D, D2, WIE, KAHAN, CAPC>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int tiles = ((A.m + CR - 1) / CR) * ((A.n + CC - 1) / CC);
-  k_aggregate_cta<D, D2, WIE, KAHAN, CAPC><<<tiles, NTC, sm, st>>>(A);
+  AggArgs B = A;
+  int nt;
+  tile_span(A.cols, A.n, CC, B.ct0, nt);
+  if (nt == 0) return cudaSuccess;
+  const int tiles = ((A.m + CR - 1) / CR) * nt;
+  k_aggregate_cta<D, D2, WIE, KAHAN, CAPC><<<tiles, NTC, sm, st>>>(B);
   return cudaGetLastError();
 }
 

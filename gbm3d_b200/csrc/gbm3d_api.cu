@@ -462,7 +462,7 @@ void check_match_set(gbm3d_ctx* c, const uint32_t* S, const int32_t* cnt, size_t
 // the reference's layout) and (M d) x (N d) x K otherwise.
 void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, int spin, int d, int d2,
                int K, int numMin, double sigma, uint32_t* S, int32_t* cnt, float* volume, float* V1,
-               float* V2, const char* tag, int s, int form) {
+               float* V2, const char* tag, int s, int form, const ColRange& jcols = ColRange()) {
   const int P = pitch4(m + d2);
   const std::string t(tag);
   float* pad = buf<float>(c, (t + ".pad").c_str(), (size_t)P * (n + d2));
@@ -493,6 +493,7 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
   A.err = c->flag;
   A.R = m + d2;
   A.Q = n + d2;
+  group_span(jcols, A.M, A.N, A.g0, A.gn);  // the exhaustive matcher's window (strip form)
   if (form == 1 || form == 3) {
     // tensor-core distances (precision and tensor forms): the V1/V2 gathers of
     // matchBlocksWie are not produced by the tensor-core matcher, so that
@@ -523,8 +524,17 @@ void run_match(gbm3d_ctx* c, const float* img, const float* img2, int m, int n, 
 // U, W are float ((M-1) s + d) x ((N-1) s + d).
 // The cycle-spun 3D wavelet hard threshold (or medfilt3) of an m x n x K
 // volume: Vavg = max(mean over cycle spins, 0), returned in "ht.vsum".
+// Strip form: the columns each stage of one step-1 spin produces.
+struct Spin1Cols {
+  ColRange match, weights, agg;  // group columns matched and weighed; pixel columns aggregated
+  std::vector<ColRange> an, sy;  // per level: analysis coefficient columns, synthesis output columns
+};
+struct Spin2Cols {
+  ColRange groups, agg;  // group columns matched and filtered; pixel columns aggregated
+};
+
 float* run_wavelet_ht(gbm3d_ctx* c, const float* vol, int m, int n, int K, int levels, int cycleSpin,
-                      const double* tau, const WaveletBank& bk, int filtType) {
+                      const double* tau, const WaveletBank& bk, int filtType, const Spin1Cols* w = nullptr) {
   float* vsum = buf<float>(c, "ht.vsum", (size_t)m * n * K);
   if (filtType == 1) {  // medfilt3 instead of the wavelet (denoiseAndAggregateGPU.m:49-52)
     StageTimer tw(c, 2);
@@ -551,7 +561,8 @@ float* run_wavelet_ht(gbm3d_ctx* c, const float* vol, int m, int n, int K, int l
   for (int s = 0; s < cycleSpin; ++s) {
     for (int lv = 0; lv < levels; ++lv) {
       const float* in = lv == 0 ? vol : coef[lv - 1];
-      launched(c, launch_wav_analysis(in, m >> lv, n >> lv, K >> lv, lv == 0 ? s : 0, coef[lv], bk, th[lv], c->st),
+      launched(c, launch_wav_analysis(in, m >> lv, n >> lv, K >> lv, lv == 0 ? s : 0, coef[lv], bk, th[lv], c->st,
+                                      w ? w->an[lv] : ColRange()),
                "wav_analysis");
     }
     for (int lv = levels - 1; lv >= 0; --lv) {
@@ -570,7 +581,9 @@ float* run_wavelet_ht(gbm3d_ctx* c, const float* vol, int m, int n, int K, int l
         o.last = 0;
         o.cycles = 1.f;
       }
-      launched(c, launch_wav_synthesis(coef[lv], approx, m >> lv, n >> lv, K >> lv, o, bk, c->st), "wav_synthesis");
+      launched(c, launch_wav_synthesis(coef[lv], approx, m >> lv, n >> lv, K >> lv, o, bk, c->st,
+                                       w ? w->sy[lv] : ColRange()),
+               "wav_synthesis");
     }
   }
   }
@@ -580,12 +593,12 @@ float* run_wavelet_ht(gbm3d_ctx* c, const float* vol, int m, int n, int K, int l
 
 void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cnt, int M, int N, int d,
             int d2, int K, int levels, int cycleSpin, const double* tau, const WaveletBank& bk, float* U,
-            float* W, int filtType, int s) {
+            float* W, int filtType, int s, const Spin1Cols* w = nullptr) {
   const int m = M * d, n = N * d;
-  float* vsum = run_wavelet_ht(c, vol, m, n, K, levels, cycleSpin, tau, bk, filtType);
+  float* vsum = run_wavelet_ht(c, vol, m, n, K, levels, cycleSpin, tau, bk, filtType, w);
   StageTimer tagg(c, 3);
   float* wgt = buf<float>(c, "ht.wgt", (size_t)M * N);
-  launched(c, launch_ht_weights(vsum, m, n, M, N, d, K, cnt, wgt, c->st), "ht_weights");
+  launched(c, launch_ht_weights(vsum, m, n, M, N, d, K, cnt, wgt, c->st, w ? w->weights : ColRange()), "ht_weights");
   AggArgs A{};
   A.S = S;
   A.cnt = cnt;
@@ -606,6 +619,7 @@ void run_ht(gbm3d_ctx* c, const float* vol, const uint32_t* S, const int32_t* cn
   A.n = (N - 1) * s + d;
   A.U = U;
   A.W = W;
+  if (w) A.cols = w->agg;
   launched(c, launch_aggregate(A, c->st), "aggregate");
 }
 
@@ -623,7 +637,10 @@ void fill_wiener_consts(WienerArgs& A, int d, const double* sigma, int is_matrix
   A.clamp_one = variant == 1;
 }
 
-void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float* W) {
+// Strip form: cols the aggregated pixel columns and cnt the per-group counts
+// (K inside the filtered window, 0 outside); A.g0 / A.gn set the window.
+void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float* W,
+                    const ColRange& cols = ColRange(), const int32_t* cnt = nullptr) {
   const int M = A.M, N = A.N, K = A.K;
   if (!wiener_supported(d, K))
     argfail(c, "unsupported (blockSizeWie, numMax) pair for the Wiener step", GBM3D_ERR_UNSUPPORTED);
@@ -637,7 +654,7 @@ void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float*
   StageTimer t(c, 6);
   AggArgs G{};
   G.S = A.S;
-  G.cnt = nullptr;
+  G.cnt = cnt;
   G.M = M;
   G.N = N;
   G.d = d;
@@ -652,6 +669,7 @@ void run_wiener_agg(gbm3d_ctx* c, WienerArgs& A, int d, int d2, float* U, float*
   G.n = (N - 1) * A.s + d;
   G.U = U;
   G.W = W;
+  G.cols = cols;
   launched(c, launch_aggregate(G, c->st), "aggregate");
 }
 
@@ -731,11 +749,194 @@ __global__ void k_crop_f2d(const float* __restrict__ v, int Mp, double* __restri
 
 __global__ void k_fill_f(float* __restrict__ p, float v) { p[0] = v; }
 
+// Strip form, step 2: count K for the groups of the filtered window (group
+// columns lo .. lo + len - 1 modulo N), 0 elsewhere, so that the aggregation
+// takes nothing from groups this call did not match.
+__global__ void k_window_counts(int32_t* __restrict__ cnt, int M, int N, int lo, int len, int K) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= M * N) return;
+  const int dj = g / M - lo;
+  cnt[g] = (dj < 0 ? dj + N : dj) < len ? K : 0;
+}
+
+// ---- the strip form: which columns each stage must produce ---------------------------
+//
+// A caller that wants output columns [c_lo, c_hi) only (one GPU's share of a
+// single image) runs every stage on the full-size buffers but restricted to the
+// columns its consumers read, walking the dependencies back from the output:
+// spin shifts (GBM3D.m:53-57,78-83), aggregation reach (a group's blocks land
+// within its search window, denoiseAndAggregateGPU.m:70-89), search windows
+// (matchBlocksCPU.m:57-79), and the 3D wavelet's circular filters per level
+// and cycle spin (denoiseAndAggregateGPU.m:27-47).  Every produced column is
+// computed from the same inputs as in the whole-image call, so the strip is
+// bit-identical to the same columns of that call.  Sets are circular column
+// masks; each stage gets the smallest circular range that covers its mask.
+using ColMask = std::vector<char>;
+
+ColRange cover(const ColMask& m) {
+  const int L = (int)m.size();
+  bool any = false;
+  int best = 0, best_end = 0, run = 0;  // longest circular run of unneeded columns
+  for (int t = 0; t < 2 * L; ++t) {
+    if (m[t % L]) {
+      any = true;
+      run = 0;
+    } else if (++run > best && run <= L) {
+      best = run;
+      best_end = t + 1;
+    }
+  }
+  if (!any) return ColRange{0, 0};
+  if (best == 0) return ColRange{0, -1};
+  return ColRange{best_end % L, L - best};
+}
+// mark [a, b] (inclusive, any integers) modulo the mask length
+void mark(ColMask& m, int a, int b) {
+  const int L = (int)m.size();
+  if (b - a + 1 >= L) {
+    std::fill(m.begin(), m.end(), 1);
+    return;
+  }
+  for (int x = a; x <= b; ++x) m[pmod(x, L)] = 1;
+}
+ColMask shifted(const ColMask& m, int s) {  // {(c + s) mod L : c in m}
+  const int L = (int)m.size();
+  ColMask o(L, 0);
+  for (int c = 0; c < L; ++c)
+    if (m[c]) o[pmod(c + s, L)] = 1;
+  return o;
+}
+// Groups (of N, stride s, patch D) whose blocks can land on a needed pixel
+// column: a block of group j starts at column j s - h + b, b in 0 .. d2 - 1.
+ColMask groups_reaching(const ColMask& px, int N, int s, int D, int d2) {
+  const int L = (int)px.size(), h = d2 / 2;
+  std::vector<int> pre(L + 1, 0);
+  for (int c = 0; c < L; ++c) pre[c + 1] = pre[c] + (px[c] ? 1 : 0);
+  ColMask g(N, 0);
+  for (int j = 0; j < N; ++j) {
+    const int a = std::max(0, j * s - h - 1), b = std::min(L, j * s - h + d2 + D);
+    g[j] = b > a && pre[b] > pre[a];
+  }
+  return g;
+}
+
+struct StripCols {
+  std::vector<Spin1Cols> s1;
+  std::vector<Spin2Cols> s2;
+};
+
+// Columns per stage for output columns [c_lo, c_hi) of the Mp x Np padded grid.
+StripCols strip_cols(const gbm3d_opts* o, int Mp, int Np, int d, int dw, int d2, int st1, int st2, int c_lo,
+                     int c_hi, const WaveletBank& bk) {
+  (void)Mp;
+  const int nS = o->nMatchSpins, nW = o->Wiener ? o->nMatchSpinsWie : 0, h = d2 / 2;
+  const bool stale = o->form != 2 && o->Wiener && o->staleWeights && nW < nS;
+  StripCols P;
+  ColMask out(Np, 0);
+  for (int x = c_lo; x < c_hi; ++x) out[x] = 1;
+  ColMask u1 = out;  // step-1 estimate columns needed (its own strip, and the step-2 search windows)
+  // step 2: spin shift -> aggregation -> groups -> pilot search windows
+  const int N2 = grid_count(Np, dw, st2);
+  for (int ii = 0; ii < nW; ++ii) {
+    const int sp = o->matchSpinsWie[ii];
+    const ColMask a2 = shifted(out, sp);
+    const ColMask g2 = groups_reaching(a2, N2, st2, dw, d2);
+    P.s2.push_back(Spin2Cols{cover(g2), cover(a2)});
+    for (int j = 0; j < N2; ++j) {
+      if (!g2[j]) continue;
+      for (int q = std::max(0, j * st2 - 1); q < std::min(Np + d2, j * st2 + d2 + dw + 1); ++q)
+        u1[pmod(pad_index(q, Np, h) - sp, Np)] = 1;
+    }
+  }
+  if (o->form == 2) return P;  // the learned pilot runs on the whole image
+  // step 1: spin shift -> aggregation -> groups -> denoised volume -> wavelet -> matched volume
+  const int N1 = grid_count(Np, d, st1), n0 = N1 * d, levels = o->levels;
+  for (int ii = 0; ii < nS; ++ii) {
+    const int sp = o->matchSpins[ii];
+    ColMask a1 = shifted(u1, sp);
+    if (stale && ii >= nW) {  // this spin's weights also join the step-2 denominator
+      const ColMask extra = shifted(out, sp);
+      for (int x = 0; x < Np; ++x) a1[x] |= extra[x];
+    }
+    const ColMask g1 = groups_reaching(a1, N1, st1, d, d2);
+    ColMask vs(n0, 0);  // denoised-volume (mosaic) columns the weights and the aggregation read
+    for (int j = 0; j < N1; ++j)
+      if (g1[j]) mark(vs, j * d, j * d + d - 1);
+    ColMask vol(n0, 0);  // matched-volume columns
+    Spin1Cols w;
+    if (o->filtType == 1) {
+      for (int x = 0; x < n0; ++x)
+        if (vs[x]) mark(vol, x - 2, x + 2);
+    } else {
+      std::vector<ColMask> an(levels), sy(levels);
+      for (int lv = 0; lv < levels; ++lv) {
+        an[lv].assign(n0 >> (lv + 1), 0);
+        sy[lv].assign(n0 >> lv, 0);
+      }
+      const int RS = bk.reach_s + 1, RA = bk.reach_a + 1;
+      for (int sc = 0; sc < o->cycleSpin; ++sc) {
+        // synthesis, level 0 up: outputs computed at p land at p - shift (shift sc at level 0)
+        std::vector<ColMask> coef(levels);
+        ColMask p = shifted(vs, sc);
+        for (int lv = 0; lv < levels; ++lv) {
+          for (int x = 0; x < (int)p.size(); ++x) sy[lv][x] |= p[x];
+          ColMask q(n0 >> (lv + 1), 0);
+          for (int x = 0; x < (int)p.size(); ++x)
+            if (p[x]) mark(q, x / 2 - 2, (x + RS) / 2 + 2);
+          coef[lv] = q;  // bands of level lv (and, at the top, the approximation)
+          p = q;         // the approximation rec[lv + 1] the level below needs
+        }
+        // analysis, top level down: coefficient q reads inputs 2q - reach - shift .. 2q + 1 - shift
+        ColMask need = coef[levels - 1];
+        for (int lv = levels - 1; lv >= 0; --lv) {
+          for (int x = 0; x < (int)need.size(); ++x) an[lv][x] |= need[x];
+          const int sh = lv == 0 ? sc : 0;
+          ColMask in(n0 >> lv, 0);
+          for (int x = 0; x < (int)need.size(); ++x)
+            if (need[x]) mark(in, 2 * x - RA - sh - 1, 2 * x + 2 - sh);
+          if (lv == 0) {
+            for (int x = 0; x < n0; ++x) vol[x] |= in[x];
+          } else {
+            need = coef[lv - 1];
+            for (int x = 0; x < (int)in.size(); ++x) need[x] |= in[x];
+          }
+        }
+      }
+      for (int lv = 0; lv < levels; ++lv) {
+        w.an.push_back(cover(an[lv]));
+        w.sy.push_back(cover(sy[lv]));
+      }
+    }
+    ColMask gm = g1;  // matched groups: the aggregated ones and every one the wavelet reads
+    for (int x = 0; x < n0; ++x)
+      if (vol[x]) gm[x / d] = 1;
+    w.match = cover(gm);
+    w.weights = cover(g1);
+    w.agg = cover(a1);
+    P.s1.push_back(w);
+  }
+  return P;
+}
+
+// Padded size along an axis of L pixels.  GBM3D.m:21-25 pads to a multiple of
+// blockSize; with other strides, to the smallest size whose references of both
+// steps end exactly at the border.  Such a size exists iff d = dw modulo
+// gcd(st1, st2); then the search ends within lcm(st1, st2) steps.
+int padded_size(const gbm3d_opts* o, int L, int d, int dw, int st1, int st2) {
+  if (st1 == d && (!o->Wiener || (st2 == dw && d % dw == 0))) return (L + d - 1) / d * d;
+  int p = std::max(L, std::max(d, dw));
+  while ((p - d) % st1 != 0 || (o->Wiener && (p - dw) % st2 != 0)) ++p;
+  return p;
+}
+
 // tau_in (levels x 7) and sigwie_in (blockSizeWie^2) replace sigma * getTau
 // and the scalar Wiener sigma on the coloured-noise path (GBM3D.m:30-36);
 // sigma is then what the matchers use, mean(sqrt(sigmaPSD)).
+// strip (c_lo < c_hi): only output columns [c_lo, c_hi) of dU are exact (the
+// strip form); the rest of dU holds whatever the restricted stages left there.
 void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const gbm3d_opts* o, double* dU,
-              double* dU1, const double* tau_in = nullptr, const double* sigwie_in = nullptr) {
+              double* dU1, const double* tau_in = nullptr, const double* sigwie_in = nullptr, int c_lo = 0,
+              int c_hi = 0) {
   check_opts(c, o);
   int d, dw, d2, K;
   opts_dims(o, d, dw, d2, K);
@@ -744,20 +945,10 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
   if (!(sigma >= 0) || !std::isfinite(sigma)) argfail(c, "sigma must be a finite non-negative scalar");
   const int st1 = stride1(o), st2 = stride2(o);
-  // GBM3D.m:21-25 pads to a multiple of blockSize; with other strides, to the
-  // smallest size whose references of both steps end exactly at the border.
-  // Such a size exists iff d = dw modulo gcd(st1, st2); then the search below
-  // ends within lcm(st1, st2) steps.
   if (o->Wiener && (d - dw) % std::gcd(st1, st2) != 0)
     argfail(c, "no padded size lets both reference grids end at the border: blockSize - blockSizeWie must be "
                "a multiple of gcd(refStride, refStrideWie)", GBM3D_ERR_UNSUPPORTED);
-  auto padded = [&](int L) {
-    if (st1 == d && (!o->Wiener || (st2 == dw && d % dw == 0))) return (L + d - 1) / d * d;
-    int p = std::max(L, std::max(d, dw));
-    while ((p - d) % st1 != 0 || (o->Wiener && (p - dw) % st2 != 0)) ++p;
-    return p;
-  };
-  const int Mp = padded(m), Np = padded(n);
+  const int Mp = padded_size(o, m, d, dw, st1, st2), Np = padded_size(o, n, d, dw, st1, st2);
   if (Mp - m > m || Np - n > n) argfail(c, "image smaller than the padding it needs");
   if (Mp < d2 || Np < d2) argfail(c, "image smaller than matchSize");
   const int nS = o->nMatchSpins, nW = o->Wiener ? o->nMatchSpinsWie : 0;
@@ -770,6 +961,14 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
   tau_table(o->levels, o->tauMode, tau.data());
   for (auto& t : tau) t *= sigma;
   if (tau_in) std::copy(tau_in, tau_in + o->levels * 7, tau.begin());
+  const bool strip = c_lo < c_hi;
+  StripCols plan;
+  if (strip) {
+    if (o->form == 1 || o->form == 3)
+      argfail(c, "the strip form runs the exhaustive matcher (forms 0 and 2)", GBM3D_ERR_UNSUPPORTED);
+    if (c_lo < 0 || c_hi > n) argfail(c, "strip columns out of range");
+    plan = strip_cols(o, Mp, Np, d, dw, d2, st1, st2, c_lo, c_hi, bk);
+  }
 
   StageTimer tall(c, 7);
   float* If = buf<float>(c, "p.If", px);
@@ -817,9 +1016,13 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     const int s = o->matchSpins[ii];
     {
       StageTimer t(c, 1);
-      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1", st1, o->form);
+      // strip form: groups this spin does not match count 0, so the aggregation skips them
+      if (strip) ck(c, cudaMemsetAsync(cnt1, 0, sizeof(int32_t) * M1 * N1, c->st), "memset");
+      run_match(c, If, nullptr, Mp, Np, s, d, d2, K, o->numMin, sigma, S1, cnt1, vol, nullptr, nullptr, "m1", st1,
+                o->form, strip ? plan.s1[ii].match : ColRange());
     }
-    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType, st1);
+    run_ht(c, vol, S1, cnt1, M1, N1, d, d2, K, o->levels, o->cycleSpin, tau.data(), bk, Us, Ws, o->filtType, st1,
+           strip ? &plan.s1[ii] : nullptr);
     k_accum2<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Ws, Mp, Np, s, Ua, Wa, ii == 0);
     launched(c, cudaGetLastError(), "accum");
     if (stale && ii >= nW) {
@@ -843,7 +1046,8 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     const int s = o->matchSpinsWie[ii];
     {
       StageTimer t(c, 4);
-      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2", st2, o->form);
+      run_match(c, U1f, nullptr, Mp, Np, s, dw, d2, K, K, sigma, S2, nullptr, nullptr, nullptr, nullptr, "m2", st2,
+                o->form, strip ? plan.s2[ii].groups : ColRange());
     }
     float* padP = buf<float>(c, "m2.pad", 1);  // the pilot search image run_match just built
     float* padN = buf<float>(c, "m2.padN", (size_t)pitch4(Mp + d2) * (Np + d2));
@@ -860,7 +1064,16 @@ void pipeline(gbm3d_ctx* c, const double* dI, int m, int n, double sigma, const 
     A.s = st2;
     double sg = sigma;
     fill_wiener_consts(A, dw, sigwie_in ? sigwie_in : &sg, sigwie_in ? 1 : 0, 0);
-    run_wiener_agg(c, A, dw, d2, Us, Ws);
+    int32_t* cnt2 = nullptr;
+    if (strip) {
+      const ColRange& gr = plan.s2[ii].groups;
+      group_span(gr, M2, N2, A.g0, A.gn);
+      cnt2 = buf<int32_t>(c, "p.cnt2", (size_t)M2 * N2);
+      k_window_counts<<<(M2 * N2 + 255) / 256, 256, 0, c->st>>>(cnt2, M2, N2, pmod(gr.lo, N2),
+                                                                 gr.all(N2) ? N2 : gr.len, K);
+      launched(c, cudaGetLastError(), "window_counts");
+    }
+    run_wiener_agg(c, A, dw, d2, Us, Ws, strip ? plan.s2[ii].agg : ColRange(), cnt2);
     k_accum2<<<grid2(Mp, Np), 256, 0, c->st>>>(Us, Ws, Mp, Np, s, Ua, Wa, ii == 0);
     launched(c, cudaGetLastError(), "accum");
   }
@@ -1905,6 +2118,49 @@ int gbm3d_denoise_device(gbm3d_ctx* c, const double* I, int m, int n, double sig
     if (!I || !U) argfail(c, "missing argument");
     pipeline(c, I, m, n, sigma, o, U, U1);
   });
+}
+
+int gbm3d_denoise_strip_device(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o,
+                               int col_lo, int col_hi, double* U) {
+  return guarded(c, [&] {
+    if (!I || !U) argfail(c, "missing argument");
+    if (m < 1 || n < 1 || m > 32000 || n > 32000) argfail(c, "image size out of range");
+    if (col_lo < 0 || col_hi > n || col_lo >= col_hi) argfail(c, "strip columns must satisfy 0 <= col_lo < col_hi <= n");
+    double* full = buf<double>(c, "strip.U", (size_t)m * n);
+    pipeline(c, I, m, n, sigma, o, full, nullptr, nullptr, nullptr, col_lo, col_hi);
+    ck(c, cudaMemcpyAsync(U, full + (size_t)col_lo * m, (size_t)m * (col_hi - col_lo) * sizeof(double),
+                          cudaMemcpyDeviceToDevice, c->st),
+       "D2D");
+  });
+}
+
+int gbm3d_strip_work(const gbm3d_opts* o, int m, int n, int col_lo, int col_hi, double* frac) {
+  if (!o || !frac || m < 1 || n < 1 || m > 32000 || n > 32000 || col_lo < 0 || col_hi > n || col_lo >= col_hi)
+    return GBM3D_ERR_ARG;
+  try {
+    int d, dw, d2, K;
+    opts_dims(o, d, dw, d2, K);
+    const int st1 = stride1(o), st2 = stride2(o);
+    if (!match_supported(d, d2) || o->levels < 1 || o->levels > GBM3D_MAX_LEVELS || o->cycleSpin < 1 ||
+        o->nMatchSpins < 1 || o->nMatchSpins > 8 || (o->Wiener && (o->nMatchSpinsWie < 1 || o->nMatchSpinsWie > 8)) ||
+        st1 < 1 || st1 > d || st2 < 1 || st2 > dw || (o->Wiener && (d - dw) % std::gcd(st1, st2) != 0))
+      return GBM3D_ERR_ARG;
+    const int Mp = padded_size(o, m, d, dw, st1, st2), Np = padded_size(o, n, d, dw, st1, st2);
+    gbm3d_filters f;
+    bank_of_opts(o, &f);
+    const WaveletBank bk = make_bank(nullptr, &f);
+    const StripCols P = strip_cols(o, Mp, Np, d, dw, d2, st1, st2, col_lo, col_hi, bk);
+    const int N1 = grid_count(Np, d, st1), N2 = grid_count(Np, dw, st2);
+    auto span = [](const ColRange& r, int N) { return r.all(N) ? N : r.len; };
+    double a = 0, b = 0;
+    for (const auto& w : P.s1) a += (double)span(w.match, N1) / N1;
+    for (const auto& w : P.s2) b += (double)span(w.groups, N2) / N2;
+    frac[0] = P.s1.empty() ? 0.0 : a / P.s1.size();
+    frac[1] = P.s2.empty() ? 0.0 : b / P.s2.size();
+    return GBM3D_OK;
+  } catch (const Fail& e) {
+    return e.code;
+  }
 }
 
 static int denoise_host(gbm3d_ctx* c, const double* I, int m, int n, double sigma, const gbm3d_opts* o, double* U,

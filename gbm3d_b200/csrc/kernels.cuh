@@ -6,6 +6,53 @@
 
 namespace gbm3d {
 
+// ---- column windows (the strip form) ------------------------------------------
+// A circular range of columns [lo, lo + len) of an axis of length L, every
+// index taken modulo L; len < 0 (or >= L): the whole axis; len 0: none.  The
+// strip form restricts each stage to the columns its consumers read.
+struct ColRange {
+  int lo = 0, len = -1;
+  bool all(int L) const { return len < 0 || len >= L; }
+};
+// The tiles of T columns (the last one partial) that hold every column of r:
+// tiles t0, t0 + 1, ..., nt of them, modulo the tile count.  Whole axis: 0, count.
+inline void tile_span(const ColRange& r, int L, int T, int& t0, int& nt) {
+  const int ntile = (L + T - 1) / T;
+  if (r.all(L)) {
+    t0 = 0;
+    nt = ntile;
+    return;
+  }
+  if (r.len == 0) {
+    t0 = nt = 0;
+    return;
+  }
+  const int lo = ((r.lo % L) + L) % L, last = lo + r.len - 1;  // last may pass L: it wraps
+  t0 = lo / T;
+  nt = last < L ? last / T - t0 + 1 : (ntile - t0) + (last - L) / T + 1;
+  if (nt >= ntile) t0 = 0, nt = ntile;
+}
+// Groups g = i + M j of the group columns r (N of them): g0 and the count gn
+// (0: every group; -1: none).
+inline void group_span(const ColRange& r, int M, int N, int& g0, int& gn) {
+  if (r.all(N)) {
+    g0 = gn = 0;
+    return;
+  }
+  if (r.len == 0) {
+    g0 = 0, gn = -1;
+    return;
+  }
+  g0 = (((r.lo % N) + N) % N) * M;
+  gn = r.len * M;
+}
+// Group of window slot gl (g0 + gl modulo G), or -1 past the window.
+__host__ __device__ __forceinline__ int window_group(int gl, int g0, int gn, int G) {
+  if (gl >= (gn > 0 ? gn : G)) return -1;
+  const int g = gl + g0;
+  return g >= G ? g - G : g;
+}
+
 // ---- block matching (match.cu) ----------------------------------------------
 struct MatchArgs {
   const float* pad;   // padded search image of the matched image, pitch P
@@ -38,6 +85,8 @@ struct MatchArgs {
   int* work;
   long long wait_cycles;
   int* cand_hist;
+  // exhaustive matcher: only the groups g0 .. g0 + gn - 1 (modulo M N); gn 0: all
+  int g0, gn;
 };
 bool match_supported(int d, int d2);
 // 2-D fp32 tensor map of a search image (R rows, the inner dimension, of
@@ -74,8 +123,10 @@ struct LevelBands {
 // Analysis of one level + hard threshold.  in: Ly x Lx x Lz, read at
 // ((y-shift) mod Ly, (x-shift) mod Lx, (z-shift) mod Lz).  out: 8 bands, band
 // code fy + 2 fx + 4 fz, each (Ly/2)(Lx/2)(Lz/2) floats.
+// qcols: the coefficient columns (of Lx / 2) to produce.
 cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
-                                const WaveletBank& bk, const LevelBands& th, cudaStream_t st);
+                                const WaveletBank& bk, const LevelBands& th, cudaStream_t st,
+                                const ColRange& qcols = ColRange());
 // Synthesis of one level: bands (codes 1..7) + approx -> out (Oy x Ox x Oz).
 // mode 0: out[p] = v; with shift_out, the value for p lands at p - shift_out.
 // Level-1 cycle-spin accumulation: first (store) / middle (add) / last
@@ -86,13 +137,16 @@ struct SynthOut {
   int first, last;
   float cycles;
 };
+// cols: the output columns (values computed for p, before the shift) to produce.
 cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy, int Ox, int Oz,
-                                 const SynthOut& o, const WaveletBank& bk, cudaStream_t st);
+                                 const SynthOut& o, const WaveletBank& bk, cudaStream_t st,
+                                 const ColRange& cols = ColRange());
 // medfilt3 of the volume (filtType 'median').
 cudaError_t launch_medfilt3(const float* V, int m, int n, int K, float* out, cudaStream_t st);
 // Aggregation weight 1/(TV(group)+eps) per group of the image-shaped Vavg.
+// jcols: the group columns (of N) to weigh.
 cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int d, int K,
-                              const int32_t* cnt, float* wgt, cudaStream_t st);
+                              const int32_t* cnt, float* wgt, cudaStream_t st, const ColRange& jcols = ColRange());
 
 // ---- step 2: empirical Wiener (wiener.cu) --------------------------------------
 struct WienerArgs {
@@ -114,6 +168,7 @@ struct WienerArgs {
   float* out;         // weighted filtered groups fl(wv .* block), d x d x K x M x N
   float* wt;          // per-group weights wv = fl(w / n2), d x d x M x N
   float* n2;          // ||filt||^2 per group (sqrt then square, single)
+  int g0, gn;         // only the groups g0 .. g0 + gn - 1 (modulo M N); gn 0: all
 };
 bool wiener_supported(int d, int K);
 cudaError_t launch_wiener(int d, const WienerArgs& A, cudaStream_t st);
@@ -132,6 +187,8 @@ struct AggArgs {
   int m, n;             // output size (m = (M-1) s + d, n = (N-1) s + d)
   float* U;             // m x n
   float* W;
+  ColRange cols;        // output columns to produce (whole CTA tiles; the rest of U, W is left as it is)
+  int ct0;              // first CTA column tile (set by the launcher from cols)
 };
 cudaError_t launch_aggregate(const AggArgs& A, cudaStream_t st);
 

@@ -397,8 +397,8 @@ __global__ void __launch_bounds__(128, 7) k_match(const __grid_constant__ CUtens
   using SM = MatchSmem<D, D2>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * 4 + warp;
-  if (g >= A.M * A.N) return;  // warp-uniform
+  const int g = window_group(blockIdx.x * 4 + warp, A.g0, A.gn, A.M * A.N);
+  if (g < 0) return;  // warp-uniform
   float* win = reinterpret_cast<float*>(smem_raw) + warp * SM::WF;
   uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw + SM::LST) + warp * 224;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + SM::MBAR) + warp;
@@ -446,7 +446,8 @@ static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   // it, would otherwise launch without it.
   cudaError_t e = cudaFuncSetAttribute(k_match<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int G = A.M * A.N;
+  const int G = A.gn > 0 ? A.gn : A.M * A.N;
+  if (A.gn < 0) return cudaSuccess;  // an empty window
   k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(tm, A);
   return cudaGetLastError();
 }

@@ -28,14 +28,15 @@ constexpr int TP = 32;  // synthesis output tile (samples per axis)
 
 __global__ void __launch_bounds__(256) k_wav_analysis(const float* __restrict__ in, int Ly, int Lx,
                                                       int Lz, int shift, float* __restrict__ out,
-                                                      WaveletBank bk, LevelBands th) {
+                                                      WaveletBank bk, LevelBands th, int tx0) {
   extern __shared__ float sm[];
   const int R = bk.reach_a;
   const int NY = 2 * TQ + R;
   float* tz = sm;                // [2][NY(x)][NY(y)]
   float* tx = sm + 2 * NY * NY;  // [4][TQ(qx)][NY(y)]
   const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
-  const int qy0 = blockIdx.x * TQ, qx0 = blockIdx.y * TQ, qz = blockIdx.z;
+  const int ntx = (Ox + TQ - 1) / TQ, bx = blockIdx.y + tx0;  // column tile: the window's, modulo the count
+  const int qy0 = blockIdx.x * TQ, qx0 = (bx >= ntx ? bx - ntx : bx) * TQ, qz = blockIdx.z;
   const int y0 = 2 * qy0 - R, x0 = 2 * qx0 - R;
   const size_t plane = (size_t)Ly * Lx;
 
@@ -93,14 +94,15 @@ __global__ void __launch_bounds__(256) k_wav_analysis(const float* __restrict__ 
 
 __global__ void __launch_bounds__(256) k_wav_synthesis(const float* __restrict__ bands,
                                                        const float* __restrict__ approx, int Oy,
-                                                       int Ox, int Oz, SynthOut o, WaveletBank bk) {
+                                                       int Ox, int Oz, SynthOut o, WaveletBank bk, int tx0) {
   extern __shared__ float sm[];
   const int Iy = Oy >> 1, Ix = Ox >> 1, Iz = Oz >> 1;
   const int NQ = (TP - 1 + bk.reach_s) / 2 + 1;
   float* B = sm;                  // [8][NQ(qx)][NQ(qy)]
   float* Y = B + 8 * NQ * NQ;     // [4][NQ(qx)][TP(py)]
   float* X = Y + 4 * NQ * TP;     // [2][TP(px)][TP(py)]
-  const int py0 = blockIdx.x * TP, px0 = blockIdx.y * TP, qz = blockIdx.z;
+  const int ntx = (Ox + TP - 1) / TP, bx = blockIdx.y + tx0;
+  const int py0 = blockIdx.x * TP, px0 = (bx >= ntx ? bx - ntx : bx) * TP, qz = blockIdx.z;
   const int qy0 = py0 >> 1, qx0 = px0 >> 1;
   const size_t bsz = (size_t)Iy * Ix * Iz;
 
@@ -189,10 +191,10 @@ __device__ __forceinline__ float warp_sum(float v) {
 
 __global__ void __launch_bounds__(128) k_ht_weights(const float* __restrict__ V, int m, int n, int M,
                                                     int N, int d, int K, const int32_t* __restrict__ cnt,
-                                                    float* __restrict__ wgt) {
+                                                    float* __restrict__ wgt, int g0, int gn) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * 4 + warp;
-  if (g >= M * N) return;
+  const int g = window_group(blockIdx.x * 4 + warp, g0, gn, M * N);
+  if (g < 0) return;
   const int i = g % M, j = g / M;
   const int nm = cnt ? cnt[g] : K;
   const size_t sz = (size_t)m * n;
@@ -249,7 +251,7 @@ constexpr int FQY = 32, FQX = 16;  // fast analysis tile: coefficients along y (
 template <int LA, int HA0>
 __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restrict__ in, int Ly, int Lx, int Lz,
                                                            int shift, float* __restrict__ out, FastBank fb,
-                                                           LevelBands th) {
+                                                           LevelBands th, int tx0) {
   constexpr int HALO = LA - 1;
   constexpr int NY = 2 * FQY + HALO;  // staged rows
   constexpr int NX = 2 * FQX + HALO;  // staged columns
@@ -260,7 +262,8 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
   float* tz = sm;                     // [2 fz][NX x][NY y]
   float* tx = sm + 2 * NX * NY;       // [4 comb][FQX qx][2 parity][NYHP]
   const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
-  const int qy0 = blockIdx.x * FQY, qx0 = blockIdx.y * FQX, qz = blockIdx.z;
+  const int ntx = (Ox + FQX - 1) / FQX, bx = blockIdx.y + tx0;
+  const int qy0 = blockIdx.x * FQY, qx0 = (bx >= ntx ? bx - ntx : bx) * FQX, qz = blockIdx.z;
   const int y0 = 2 * qy0 - HALO - shift, x0 = 2 * qx0 - HALO - shift;
   const size_t zA = (size_t)Ly * Lx * pmod(2 * qz - shift, Lz), zB = (size_t)Ly * Lx * pmod(2 * qz - 1 - shift, Lz);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -356,7 +359,7 @@ constexpr int FSY = 64, FSX = 32;  // fast synthesis tile: samples along y and x
 template <int SL0, int SH>
 __global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restrict__ bands,
                                                            const float* __restrict__ approx, int Oy, int Ox,
-                                                           int Oz, SynthOut o, FastBank fb) {
+                                                           int Oz, SynthOut o, FastBank fb, int tx0) {
   constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
   constexpr int NQY = (FSY - 1 + REACH) / 2 + 1;  // staged coefficients along y
   constexpr int NQX = (FSX - 1 + REACH) / 2 + 1;  // and along x
@@ -369,7 +372,8 @@ __global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restri
   float* B = sm;                    // [8 code][NQX qx][BQ]
   float* Y = sm + 8 * NQX * BQ;     // [4 comb][NQX qx][YS]
   const int Iy = Oy >> 1, Ix = Ox >> 1, Iz = Oz >> 1;
-  const int py0 = blockIdx.x * FSY, px0 = blockIdx.y * FSX, qz = blockIdx.z;
+  const int ntx = (Ox + FSX - 1) / FSX, bx = blockIdx.y + tx0;
+  const int py0 = blockIdx.x * FSY, px0 = (bx >= ntx ? bx - ntx : bx) * FSX, qz = blockIdx.z;
   const int qy0 = py0 >> 1, qx0 = px0 >> 1;
   const size_t bsz = (size_t)Iy * Ix * Iz, zoff = (size_t)Iy * Ix * qz;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -525,27 +529,35 @@ static FastBank fast_bank(const WaveletBank& bk) {
 
 template <int LA, int HA0>
 static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
-                                        const FastBank& fb, const LevelBands& th, cudaStream_t st) {
+                                        const FastBank& fb, const LevelBands& th, cudaStream_t st,
+                                        const ColRange& qcols) {
   constexpr int NY = 2 * FQY + LA - 1, NX = 2 * FQX + LA - 1, NYH = (NY + 1) / 2;
   constexpr int NYHP = ((NYH + 15) / 32) * 32 + 16;
   const size_t sm = (size_t)(2 * NX * NY + 4 * FQX * 2 * NYHP) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_fast<LA, HA0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((Ly / 2 + FQY - 1) / FQY, (Lx / 2 + FQX - 1) / FQX, Lz / 2);
-  k_wav_analysis_fast<LA, HA0><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, fb, th);
+  int t0, nt;
+  tile_span(qcols, Lx / 2, FQX, t0, nt);
+  if (nt == 0) return cudaSuccess;
+  dim3 grid((Ly / 2 + FQY - 1) / FQY, nt, Lz / 2);
+  k_wav_analysis_fast<LA, HA0><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, fb, th, t0);
   return cudaGetLastError();
 }
 
 template <int SL0, int SH>
 static cudaError_t launch_synthesis_fast(const float* bands, const float* approx, int Oy, int Ox, int Oz,
-                                         const SynthOut& o, const FastBank& fb, cudaStream_t st) {
+                                         const SynthOut& o, const FastBank& fb, cudaStream_t st,
+                                         const ColRange& cols) {
   constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
   constexpr int NQY = (FSY - 1 + REACH) / 2 + 1, NQX = (FSX - 1 + REACH) / 2 + 1;
   const size_t sm = ((size_t)8 * NQX * (NQY | 1) + (size_t)4 * NQX * (FSY + 1)) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_win<SL0, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((Oy + FSY - 1) / FSY, (Ox + FSX - 1) / FSX, Oz / 2);
-  k_wav_synthesis_win<SL0, SH><<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, fb);
+  int t0, nt;
+  tile_span(cols, Ox, FSX, t0, nt);
+  if (nt == 0) return cudaSuccess;
+  dim3 grid((Oy + FSY - 1) / FSY, nt, Oz / 2);
+  k_wav_synthesis_win<SL0, SH><<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, fb, t0);
   return cudaGetLastError();
 }
 
@@ -557,12 +569,12 @@ static cudaError_t launch_synthesis_fast(const float* bands, const float* approx
 template <int D>
 __global__ void __launch_bounds__(128) k_ht_weights_t(const float* __restrict__ V, int m, int n, int M, int N,
                                                       int K, const int32_t* __restrict__ cnt,
-                                                      float* __restrict__ wgt) {
+                                                      float* __restrict__ wgt, int g0, int gn) {
   constexpr int DM = D - 3, SL = D * D, SX = D * DM;  // slice size, per-slot elements of the x/y terms
   __shared__ float sl[4][2][SL];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * 4 + warp;
-  if (g >= M * N) return;
+  const int g = window_group(blockIdx.x * 4 + warp, g0, gn, M * N);
+  if (g < 0) return;
   const int i = g % M, j = g / M;
   const int nm = cnt ? cnt[g] : K;
   const size_t sz = (size_t)m * n;
@@ -650,36 +662,44 @@ static size_t synthesis_smem(int reach) {
 }
 
 cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
-                                const WaveletBank& bk, const LevelBands& th, cudaStream_t st) {
+                                const WaveletBank& bk, const LevelBands& th, cudaStream_t st,
+                                const ColRange& qcols) {
   const int kind = fast_kind(bk);
   // the fast kernel wraps each halo coordinate at most once
   if (kind && Ly > 2 * TQ + 16 && Lx > 2 * TQ + 16 && Lz >= 2) {
     const FastBank fb = fast_bank(bk);
-    if (kind == 1) return launch_analysis_fast<10, 4>(in, Ly, Lx, Lz, shift, out, fb, th, st);
-    return launch_analysis_fast<2, 0>(in, Ly, Lx, Lz, shift, out, fb, th, st);
+    if (kind == 1) return launch_analysis_fast<10, 4>(in, Ly, Lx, Lz, shift, out, fb, th, st, qcols);
+    return launch_analysis_fast<2, 0>(in, Ly, Lx, Lz, shift, out, fb, th, st, qcols);
   }
   const size_t sm = analysis_smem(bk.reach_a);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((Ly / 2 + TQ - 1) / TQ, (Lx / 2 + TQ - 1) / TQ, Lz / 2);
-  k_wav_analysis<<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, bk, th);
+  int t0, nt;
+  tile_span(qcols, Lx / 2, TQ, t0, nt);
+  if (nt == 0) return cudaSuccess;
+  dim3 grid((Ly / 2 + TQ - 1) / TQ, nt, Lz / 2);
+  k_wav_analysis<<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, bk, th, t0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy, int Ox, int Oz,
-                                 const SynthOut& o, const WaveletBank& bk, cudaStream_t st) {
+                                 const SynthOut& o, const WaveletBank& bk, cudaStream_t st,
+                                 const ColRange& cols) {
   const int kind = fast_kind(bk);
   // coefficient tiles of 37 per axis must wrap at most once; shifts below the size
   if (kind && Oy >= 128 && Ox >= 128 && Oz >= 2 && o.shift >= 0 && o.shift < Oy && o.shift < Ox) {
     const FastBank fb = fast_bank(bk);
-    if (kind == 1) return launch_synthesis_fast<4, 10>(bands, approx, Oy, Ox, Oz, o, fb, st);
-    return launch_synthesis_fast<0, 2>(bands, approx, Oy, Ox, Oz, o, fb, st);
+    if (kind == 1) return launch_synthesis_fast<4, 10>(bands, approx, Oy, Ox, Oz, o, fb, st, cols);
+    return launch_synthesis_fast<0, 2>(bands, approx, Oy, Ox, Oz, o, fb, st, cols);
   }
   const size_t sm = synthesis_smem(bk.reach_s);
   cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((Oy + TP - 1) / TP, (Ox + TP - 1) / TP, Oz / 2);
-  k_wav_synthesis<<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, bk);
+  int t0, nt;
+  tile_span(cols, Ox, TP, t0, nt);
+  if (nt == 0) return cudaSuccess;
+  dim3 grid((Oy + TP - 1) / TP, nt, Oz / 2);
+  k_wav_synthesis<<<grid, 256, sm, st>>>(bands, approx, Oy, Ox, Oz, o, bk, t0);
   return cudaGetLastError();
 }
 
@@ -691,12 +711,12 @@ cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy
 // index arithmetic goes away.
 __global__ void __launch_bounds__(128) k_ht_weights_8(const float* __restrict__ V, int m, int n, int M, int N,
                                                       int K, const int32_t* __restrict__ cnt,
-                                                      float* __restrict__ wgt) {
+                                                      float* __restrict__ wgt, int g0, int gn) {
   constexpr int D = 8, DM = D - 3, SL = D * D, SX = D * DM;
   extern __shared__ float shw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * 4 + warp;
-  if (g >= M * N) return;
+  const int g = window_group(blockIdx.x * 4 + warp, g0, gn, M * N);
+  if (g < 0) return;
   float* sg = shw + warp * K * SL;
   const int i = g % M, j = g / M;
   const int nm = cnt ? cnt[g] : K;
@@ -750,24 +770,27 @@ __global__ void __launch_bounds__(128) k_ht_weights_8(const float* __restrict__ 
 }
 
 cudaError_t launch_ht_weights(const float* Vavg, int m, int n, int M, int N, int d, int K,
-                              const int32_t* cnt, float* wgt, cudaStream_t st) {
-  const int G = M * N;
+                              const int32_t* cnt, float* wgt, cudaStream_t st, const ColRange& jcols) {
+  int g0, gn;
+  group_span(jcols, M, N, g0, gn);
+  if (gn < 0) return cudaSuccess;
+  const int G = gn > 0 ? gn : M * N;
   if (d == 16) {
-    k_ht_weights_t<16><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    k_ht_weights_t<16><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt, g0, gn);
     return cudaGetLastError();
   }
   if (d == 8) {
     const size_t smb = (size_t)4 * K * 64 * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k_ht_weights_8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
     if (e != cudaSuccess) return e;
-    k_ht_weights_8<<<(G + 3) / 4, 128, smb, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    k_ht_weights_8<<<(G + 3) / 4, 128, smb, st>>>(Vavg, m, n, M, N, K, cnt, wgt, g0, gn);
     return cudaGetLastError();
   }
   if (d == 32) {
-    k_ht_weights_t<32><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt);
+    k_ht_weights_t<32><<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, K, cnt, wgt, g0, gn);
     return cudaGetLastError();
   }
-  k_ht_weights<<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, d, K, cnt, wgt);
+  k_ht_weights<<<(G + 3) / 4, 128, 0, st>>>(Vavg, m, n, M, N, d, K, cnt, wgt, g0, gn);
   return cudaGetLastError();
 }
 

@@ -98,8 +98,8 @@ __global__ void __launch_bounds__(128) k_wiener(WienerArgs A) {
     s2[t] = A.s2[t];
   }
   __syncthreads();
-  const int g = blockIdx.x * 4 + warp;
-  if (g >= A.M * A.N) return;
+  const int g = window_group(blockIdx.x * 4 + warp, A.g0, A.gn, A.M * A.N);
+  if (g < 0) return;
   const float cc = 0.70710678118654752440f;
   // every task a lane runs has row r = lane % D (rounds of 32 tasks hold whole pages)
   const int r = lane % D, kq = lane / D;
@@ -285,7 +285,8 @@ static cudaError_t launch_wiener_t(const WienerArgs& A, cudaStream_t st) {
   const size_t sm = (size_t)(3 * D * D + 4 * 2 * (D * D + D) * K + 4 * D * D) * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_wiener<D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int G = A.M * A.N;
+  const int G = A.gn > 0 ? A.gn : A.M * A.N;
+  if (A.gn < 0) return cudaSuccess;  // an empty window
   k_wiener<D, K><<<(G + 3) / 4, 128, sm, st>>>(A);
   return cudaGetLastError();
 }

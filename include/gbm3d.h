@@ -310,6 +310,23 @@ int gbm3d_tiles_stitch_device(gbm3d_ctx* ctx, const double* tiles, const int* it
 int gbm3d_denoise_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
                          const gbm3d_opts* opts, double* U, double* U1);
 
+/* The strip form: output columns [col_lo, col_hi) of gbm3d_denoise_device's
+ * result, bit-identical to those columns of the whole-image call, into U
+ * (m x (col_hi - col_lo), column-major, device).  I is the whole m x n image on
+ * the device.  Every stage runs on the columns its consumers read (the strip
+ * plus the halo that spin shifts, the search windows and the wavelet filters
+ * reach), so one GPU per strip splits a single image with no exchange before
+ * the final gather.  Forms 0 (plain) and 2 (learned pilot); the tensor-core
+ * forms return GBM3D_ERR_UNSUPPORTED.  Replaces nothing in the reference: its
+ * GBM3D.m:22-83 runs the whole image on one GPU.  Asynchronous on the context
+ * stream. */
+int gbm3d_denoise_strip_device(gbm3d_ctx* ctx, const double* I, int m, int n, double sigma,
+                               const gbm3d_opts* opts, int col_lo, int col_hi, double* U);
+/* Host only (no GPU needed): the share of the whole image's references that the
+ * strip [col_lo, col_hi) matches, averaged over the spins of each step:
+ * frac[0] step 1, frac[1] step 2 (0 without a Wiener step). */
+int gbm3d_strip_work(const gbm3d_opts* opts, int m, int n, int col_lo, int col_hi, double* frac);
+
 /* Per-stage device times (ms) of the last pipeline call, by CUDA events:
  * [0] prepare, [1] step-1 matching, [2] step-1 wavelet, [3] step-1 aggregation,
  * [4] step-2 matching, [5] step-2 Wiener, [6] step-2 aggregation, [7] total.
