@@ -392,13 +392,15 @@ struct MatchSmem {
   static constexpr size_t BYTES = MBAR + 4 * sizeof(uint64_t);
 };
 
-template <int D, int D2>
+// WIN: the group window of the strip form (A.g0, A.gn); without it the grid
+// covers every group in order.
+template <int D, int D2, bool WIN>
 __global__ void __launch_bounds__(128, 7) k_match(const __grid_constant__ CUtensorMap tmap, MatchArgs A) {
   using SM = MatchSmem<D, D2>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = window_group(blockIdx.x * 4 + warp, A.g0, A.gn, A.M * A.N);
-  if (g < 0) return;  // warp-uniform
+  const int g = WIN ? window_group(blockIdx.x * 4 + warp, A.g0, A.gn, A.M * A.N) : blockIdx.x * 4 + warp;
+  if (WIN ? g < 0 : g >= A.M * A.N) return;  // warp-uniform
   float* win = reinterpret_cast<float*>(smem_raw) + warp * SM::WF;
   uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw + SM::LST) + warp * 224;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + SM::MBAR) + warp;
@@ -434,7 +436,7 @@ __global__ void __launch_bounds__(128) k_match_list(const __grid_constant__ CUte
   }
 }
 
-template <int D, int D2>
+template <int D, int D2, bool WIN>
 static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   constexpr int WD = D + D2 - 1;
   const size_t sm = MatchSmem<D, D2>::BYTES;
@@ -444,11 +446,11 @@ static cudaError_t launch_match_t(const MatchArgs& A, cudaStream_t st) {
   // launch (a host-side call that costs well under a microsecond) rather than
   // remembered once per process: a second device, or another host thread on
   // it, would otherwise launch without it.
-  cudaError_t e = cudaFuncSetAttribute(k_match<D, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = cudaFuncSetAttribute(k_match<D, D2, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int G = A.gn > 0 ? A.gn : A.M * A.N;
   if (A.gn < 0) return cudaSuccess;  // an empty window
-  k_match<D, D2><<<(G + 3) / 4, 128, sm, st>>>(tm, A);
+  k_match<D, D2, WIN><<<(G + 3) / 4, 128, sm, st>>>(tm, A);
   return cudaGetLastError();
 }
 
@@ -483,7 +485,7 @@ bool match_supported(int d, int d2) {
 cudaError_t launch_match(int d, int d2, const MatchArgs& A, cudaStream_t st) {
   if (A.s < 1 || A.s > d) return cudaErrorInvalidValue;
 #define GBM3D_MATCH_CASE(DD, DD2) \
-  if (d == DD && d2 == DD2) return launch_match_t<DD, DD2>(A, st);
+  if (d == DD && d2 == DD2) return A.gn ? launch_match_t<DD, DD2, true>(A, st) : launch_match_t<DD, DD2, false>(A, st);
   GBM3D_MATCH_CASE(8, 16) GBM3D_MATCH_CASE(8, 24) GBM3D_MATCH_CASE(8, 32)
   GBM3D_MATCH_CASE(16, 16) GBM3D_MATCH_CASE(16, 24) GBM3D_MATCH_CASE(16, 32)
   GBM3D_MATCH_CASE(32, 16) GBM3D_MATCH_CASE(32, 24) GBM3D_MATCH_CASE(32, 32)

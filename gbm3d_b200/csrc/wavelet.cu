@@ -248,7 +248,9 @@ __device__ __forceinline__ int wrap1(int v, int L) { return v < 0 ? v + L : (v >
 
 constexpr int FQY = 32, FQX = 16;  // fast analysis tile: coefficients along y (fast axis) and x
 
-template <int LA, int HA0>
+// WIN: the column-tile window of the strip form (tx0); without it the grid
+// covers every tile in order.
+template <int LA, int HA0, bool WIN>
 __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restrict__ in, int Ly, int Lx, int Lz,
                                                            int shift, float* __restrict__ out, FastBank fb,
                                                            LevelBands th, int tx0) {
@@ -262,8 +264,8 @@ __global__ void __launch_bounds__(256) k_wav_analysis_fast(const float* __restri
   float* tz = sm;                     // [2 fz][NX x][NY y]
   float* tx = sm + 2 * NX * NY;       // [4 comb][FQX qx][2 parity][NYHP]
   const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
-  const int ntx = (Ox + FQX - 1) / FQX, bx = blockIdx.y + tx0;
-  const int qy0 = blockIdx.x * FQY, qx0 = (bx >= ntx ? bx - ntx : bx) * FQX, qz = blockIdx.z;
+  const int ntx = (Ox + FQX - 1) / FQX, bx = WIN ? blockIdx.y + tx0 : blockIdx.y;
+  const int qy0 = blockIdx.x * FQY, qx0 = (WIN && bx >= ntx ? bx - ntx : bx) * FQX, qz = blockIdx.z;
   const int y0 = 2 * qy0 - HALO - shift, x0 = 2 * qx0 - HALO - shift;
   const size_t zA = (size_t)Ly * Lx * pmod(2 * qz - shift, Lz), zB = (size_t)Ly * Lx * pmod(2 * qz - 1 - shift, Lz);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -355,9 +357,10 @@ constexpr int FSY = 64, FSX = 32;  // fast synthesis tile: samples along y and x
 //           slot bands, then the slot pass and the write/accumulate, in
 //           registers.
 // Row strides of the staged arrays are odd, so lanes that walk neighbouring
-// rows hit distinct banks.
+// rows hit distinct banks.  Four CTAs fit an SM by shared memory (46.7 KB
+// each), so the register budget is that of four: up to 64 per thread.
 template <int SL0, int SH>
-__global__ void __launch_bounds__(256) k_wav_synthesis_win(const float* __restrict__ bands,
+__global__ void __launch_bounds__(256, 4) k_wav_synthesis_win(const float* __restrict__ bands,
                                                            const float* __restrict__ approx, int Oy, int Ox,
                                                            int Oz, SynthOut o, FastBank fb, int tx0) {
   constexpr int REACH = SH - 1 > SL0 + 1 ? SH - 1 : SL0 + 1;
@@ -527,21 +530,29 @@ static FastBank fast_bank(const WaveletBank& bk) {
   return f;
 }
 
-template <int LA, int HA0>
-static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
+template <int LA, int HA0, bool WIN>
+static cudaError_t launch_analysis_fast_t(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
                                         const FastBank& fb, const LevelBands& th, cudaStream_t st,
                                         const ColRange& qcols) {
   constexpr int NY = 2 * FQY + LA - 1, NX = 2 * FQX + LA - 1, NYH = (NY + 1) / 2;
   constexpr int NYHP = ((NYH + 15) / 32) * 32 + 16;
   const size_t sm = (size_t)(2 * NX * NY + 4 * FQX * 2 * NYHP) * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_fast<LA, HA0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_fast<LA, HA0, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   int t0, nt;
   tile_span(qcols, Lx / 2, FQX, t0, nt);
   if (nt == 0) return cudaSuccess;
   dim3 grid((Ly / 2 + FQY - 1) / FQY, nt, Lz / 2);
-  k_wav_analysis_fast<LA, HA0><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, fb, th, t0);
+  k_wav_analysis_fast<LA, HA0, WIN><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, fb, th, t0);
   return cudaGetLastError();
+}
+
+template <int LA, int HA0>
+static cudaError_t launch_analysis_fast(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
+                                        const FastBank& fb, const LevelBands& th, cudaStream_t st,
+                                        const ColRange& qcols) {
+  return qcols.all(Lx / 2) ? launch_analysis_fast_t<LA, HA0, false>(in, Ly, Lx, Lz, shift, out, fb, th, st, qcols)
+                           : launch_analysis_fast_t<LA, HA0, true>(in, Ly, Lx, Lz, shift, out, fb, th, st, qcols);
 }
 
 template <int SL0, int SH>
