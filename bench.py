@@ -503,6 +503,43 @@ def batched_block(ctx, stream, work, reps=3):
                 np.mean(gains))}
 
 
+def strips_block(ctx, stream, dI, o, Uref, parts=(2, 4, 8), reps=3):
+    """The strip form on one GPU: the image's column strips computed one after
+    another (gbm3d_denoise_strip_device), each timed by CUDA events, and checked
+    against the whole-image result.  The slowest strip is the time per image
+    that N GPUs, one strip each, would take (the final gather aside); the strip
+    times' sum over the whole-image time is the halo overhead."""
+    import torch
+    from gbm3d_b200 import api
+    from gbm3d_b200 import distributed as D
+    out = {}
+    for n_parts in parts:
+        bounds = D.strip_bounds(SIZE, n_parts)
+        times, same = [], True
+        for lo, hi in bounds:
+            t = torch.empty((hi - lo) * SIZE, dtype=torch.float64, device=dI.device)
+
+            def call():
+                api.GBM3D_strip_device(dI.data_ptr(), SIZE, SIZE, SIGMA, lo, hi, t.data_ptr(), o, ctx=ctx)
+
+            call()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / reps)
+            same &= bool(np.array_equal(t.cpu().numpy().reshape((SIZE, hi - lo), order="F"), Uref[:, lo:hi]))
+        work = [api.strip_work(SIZE, SIZE, lo, hi, o)[0] for lo, hi in bounds]
+        out[str(n_parts)] = {"max_strip_ms": max(times), "sum_strip_ms": sum(times),
+                             "per_gpu_MPix_s": SIZE * SIZE / 1e6 / (max(times) / 1e3),
+                             "max_step1_reference_share": max(work), "bit_identical_to_whole": same}
+    return {"api": "gbm3d_denoise_strip_device, strips of equal width, one after another on one GPU",
+            "parts": out}
+
+
 def max_over_ranks(ms: float, dist, device) -> float:
     """The step time of the whole job: the slowest rank's (an all-reduce MAX of
     one value, on the device the backend needs: a GPU for NCCL, the CPU for gloo)."""
@@ -752,6 +789,9 @@ def run_ours(args):
         line["learned_pilot"] = learned_pilot_block(ctx)
     if rank == 0 and "tuned" in res and not args.tuned_opts:
         line["quality_by_size"] = quality_by_size(ctx, args.autotune and tuning)
+    if rank == 0 and world == 1 and o.get("form", "plain") in ("plain", "learned"):
+        line["strips"] = strips_block(ctx, stream, dI, o, Uref)
+        line["strips"]["whole_ms"] = ms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"], line["parity"] = cpu_baseline(o, args.cpu_size)
     if world > 1:
