@@ -86,6 +86,7 @@ _SIGS = {
     "gbm3d_strip_work": (C.c_int, [C.POINTER(gbm3d_opts), C.c_int, C.c_int, C.c_int, C.c_int, _P]),
     "gbm3d_ctx_enable_timing": (C.c_int, [_P, C.c_int]),
     "gbm3d_ctx_set_tc_wait": (C.c_int, [_P, C.c_longlong]),
+    "gbm3d_ctx_set_lanes": (C.c_int, [_P, C.c_int]),
     "gbm3d_ctx_tc_stats": (C.c_int, [_P, C.c_int, _P]),
     "gbm3d_stage_times": (C.c_int, [_P, _P, C.c_int]),
     "gbm3d_last_launch_count": (C.c_int, [_P]),
@@ -175,6 +176,10 @@ class Context:
 
     def enable_timing(self, on: bool = True) -> None:
         self.check(lib().gbm3d_ctx_enable_timing(self.h, 1 if on else 0))
+
+    def set_lanes(self, lanes: int = 1) -> None:
+        """Streams the batched form's mixed submission runs on at once (1..16)."""
+        self.check(lib().gbm3d_ctx_set_lanes(self.h, int(lanes)))
 
     def set_tc_wait(self, cycles: int = 0) -> None:
         """Limit (SM clocks) of each wait in the tensor-core matcher; 0 = about

@@ -59,6 +59,12 @@ struct gbm3d_ctx {
   long long tc_wait = 0;  // wait limit of the tensor-core matcher in SM clocks (0: about two seconds; < 0: probe)
   bool tc_stats = false;  // accumulate the tensor-core matcher's candidate histogram
   int* tc_hist = nullptr; // 33 buckets on the device
+  // batched form: items of one submission run on `lanes` streams at once, each
+  // lane with its own buffers (named with the lane's prefix `ns`)
+  int lanes = 1;
+  std::vector<cudaStream_t> lane_st;
+  std::vector<cudaEvent_t> lane_ev;  // [0] fork, [1 + l] lane l done
+  std::string ns;
 };
 
 namespace {
@@ -93,8 +99,9 @@ void report_flag(gbm3d_ctx* c, int flag) {
 }
 
 template <class T>
-T* buf(gbm3d_ctx* c, const char* name, size_t count) {
+T* buf(gbm3d_ctx* c, const char* cname, size_t count) {
   const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+  const std::string name = c->ns.empty() ? std::string(cname) : c->ns + cname;
   auto it = c->bufs.find(name);
   if (it != c->bufs.end() && it->second.second >= bytes) return reinterpret_cast<T*>(it->second.first);
   if (it != c->bufs.end()) {
@@ -102,7 +109,7 @@ T* buf(gbm3d_ctx* c, const char* name, size_t count) {
     c->bufs.erase(it);
   }
   void* p = nullptr;
-  ck(c, cudaMalloc(&p, bytes), name);
+  ck(c, cudaMalloc(&p, bytes), name.c_str());
   c->bufs[name] = {p, bytes};
   return reinterpret_cast<T*>(p);
 }
@@ -1127,6 +1134,11 @@ void gbm3d_ctx_destroy(gbm3d_ctx* c) {
   }
   if (c->sticky) cudaFree(c->sticky);
   if (c->tc_hist) cudaFree(c->tc_hist);
+  for (cudaStream_t s : c->lane_st) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (cudaEvent_t e : c->lane_ev) cudaEventDestroy(e);
   for (auto& kv : c->bufs) cudaFree(kv.second.first);
   for (auto& e : c->evpool) cudaEventDestroy(e);
   for (auto& e : c->kpool) cudaEventDestroy(e);
@@ -1134,6 +1146,12 @@ void gbm3d_ctx_destroy(gbm3d_ctx* c) {
   if (c->flag) cudaFree(c->flag);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
+}
+
+int gbm3d_ctx_set_lanes(gbm3d_ctx* c, int lanes) {
+  if (!c || lanes < 1 || lanes > 16) return GBM3D_ERR_ARG;
+  c->lanes = lanes;
+  return GBM3D_OK;
 }
 
 int gbm3d_ctx_set_stream(gbm3d_ctx* c, void* s) {
@@ -2102,12 +2120,78 @@ int gbm3d_denoise_mixed(gbm3d_ctx* c, const gbm3d_mixed_batch* b, const gbm3d_op
       key_add(key, b->video_frames);
       key_add(key, b->video_sigma);
     }
-    run_graph(c, key, use_graph != 0, [&] {
-      for (int k : og) pipeline(c, b->grey[k], b->grey_m[k], b->grey_n[k], b->grey_sigma[k], o, b->grey_out[k], nullptr);
-      for (int k : orgb)
+    // items (kind 0 grey, 1 colour, 2 video) in decreasing estimated work, each
+    // given to the lane with the least work so far (longest processing time
+    // first); a lane runs its items in that order on its own stream
+    struct Item {
+      int kind, k;
+      double work;
+    };
+    std::vector<Item> items;
+    for (int k : og) items.push_back({0, k, (double)b->grey_m[k] * b->grey_n[k]});
+    for (int k : orgb) items.push_back({1, k, 3.0 * b->rgb_m[k] * b->rgb_n[k]});
+    if (b->video) items.push_back({2, 0, 2.0 * b->video_m * b->video_n * b->video_frames});
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.work > y.work; });
+    // the learned pilot's parameters live in unprefixed buffers: one lane
+    const int L = std::max(1, std::min({c->lanes, (int)items.size(), o->form == 2 ? 1 : 16}));
+    key_add(key, L);
+    std::vector<int> lane(items.size(), 0);
+    {
+      std::vector<double> load(L, 0.0);
+      for (size_t t = 0; t < items.size(); ++t) {
+        const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        lane[t] = l;
+        load[l] += items[t].work;
+      }
+    }
+    while ((int)c->lane_st.size() < L) {
+      cudaStream_t st;
+      ck(c, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+      c->lane_st.push_back(st);
+    }
+    while ((int)c->lane_ev.size() < L + 1) {
+      cudaEvent_t e;
+      ck(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+      c->lane_ev.push_back(e);
+    }
+    auto run_item = [&](const Item& it) {
+      const int k = it.k;
+      if (it.kind == 0)
+        pipeline(c, b->grey[k], b->grey_m[k], b->grey_n[k], b->grey_sigma[k], o, b->grey_out[k], nullptr);
+      else if (it.kind == 1)
         pipeline_rgb(c, b->rgb + 3 * k, b->rgb_m[k], b->rgb_n[k], b->rgb_sigma[k], o, b->rgb_out + 3 * k);
-      if (b->video)
+      else
         pipeline_video(c, b->video, b->video_m, b->video_n, b->video_frames, b->video_sigma, ov, b->video_out);
+    };
+    run_graph(c, key, use_graph != 0, [&] {
+      if (L == 1) {
+        for (const Item& it : items) run_item(it);
+        return;
+      }
+      // fork: every lane waits for the work already on the context stream
+      cudaStream_t origin = c->st;
+      struct Restore {  // the context's stream and buffer names, also when an item throws
+        gbm3d_ctx* c;
+        cudaStream_t st;
+        ~Restore() {
+          c->st = st;
+          c->ns.clear();
+        }
+      } restore{c, origin};
+      ck(c, cudaEventRecord(c->lane_ev[0], origin), "cudaEventRecord");
+      for (int l = 0; l < L; ++l) ck(c, cudaStreamWaitEvent(c->lane_st[l], c->lane_ev[0], 0), "cudaStreamWaitEvent");
+      for (size_t t = 0; t < items.size(); ++t) {
+        c->st = c->lane_st[lane[t]];
+        c->ns = "lane" + std::to_string(lane[t]) + ".";
+        run_item(items[t]);
+      }
+      c->st = origin;
+      c->ns.clear();
+      // join: the context stream waits for every lane
+      for (int l = 0; l < L; ++l) {
+        ck(c, cudaEventRecord(c->lane_ev[1 + l], c->lane_st[l]), "cudaEventRecord");
+        ck(c, cudaStreamWaitEvent(origin, c->lane_ev[1 + l], 0), "cudaStreamWaitEvent");
+      }
     });
   });
 }

@@ -268,6 +268,15 @@ typedef struct gbm3d_mixed_batch {
 } gbm3d_mixed_batch;
 int gbm3d_denoise_mixed(gbm3d_ctx* ctx, const gbm3d_mixed_batch* batch, const gbm3d_opts* opts,
                         const gbm3d_opts* video_opts, int use_graph);
+/* Lanes of gbm3d_denoise_mixed (1..16, default 1).  The submission's items
+ * (images, colour images, the video) go to `lanes` streams, the largest first
+ * to the least-loaded lane.  Each lane has its own buffers, and the lanes run
+ * at once, inside one graph when use_graph is set, so small images' launches
+ * fill the GPU together.  Every output is the same as with one lane.  The
+ * learned-pilot form always runs on one lane.  Not in the reference: its
+ * parfor over work items (GBM3D_distributed.m:54,94) is the host-side
+ * counterpart. */
+int gbm3d_ctx_set_lanes(gbm3d_ctx* ctx, int lanes);
 
 /* Asynchronous form of gbm3d_denoise for a stream of images (U1 is not
  * returned): the call enqueues the host-to-device copy of I, the whole

@@ -90,10 +90,20 @@ def test_autotune_choice_runs_within_budget(gpu):
     assert abs(options.myPSNR(clean, U, 255) - (best["psnr"])) < 1e-9
 
 
-def test_mixed_batch_matches_single_entries(gpu):
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_mixed_batch_matches_single_entries(gpu, lanes):
     """Grey images, colour images and a video in one submission: eager, then
     captured, then replayed twice; every output equals its own single-image
-    entry's bit for bit."""
+    entry's bit for bit, on one lane and on three concurrent lanes."""
+    from gbm3d_b200 import api
+    api.context().set_lanes(lanes)
+    try:
+        _mixed_case()
+    finally:
+        api.context().set_lanes(1)
+
+
+def _mixed_case():
     import torch
     from gbm3d_b200 import api
     o = _dense()
