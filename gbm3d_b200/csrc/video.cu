@@ -43,17 +43,58 @@ __global__ void __launch_bounds__(128) k_match_video(VideoMatchArgs A) {
       win[e] = pad[(size_t)(i * D + r) + (size_t)(j * D + c) * A.P];
     }
     __syncthreads();
-    for (int cand = tid; cand < DD; cand += 128) {
-      const int a = cand % D, b = cand / D;
-      float acc = 0.f;
-      for (int r = 0; r < D; ++r)
-#pragma unroll 8
-        for (int c = 0; c < D; ++c) {
-          const float t = xr[r * D + c] - win[(a + r) + (b + c) * WD];
-          acc = fmaf(t, t, acc);
+    if constexpr (D == 32) {
+      // 1024 candidates, 8 per thread: lane a = candidate row, warp w the
+      // columns b = 8w .. 8w+7.  Per pixel (r, c) the reference value is one
+      // broadcast and the 8 candidates' window values slide along the row
+      // a + r in registers (one new shared load per c), so the loop runs at
+      // the FP32 issue rate instead of two shared loads per FMA.  Each
+      // candidate still accumulates in the order (r, then c).
+      constexpr int NB = 8;
+      const int a = tid & 31, b0 = (tid >> 5) * NB;
+      float acc[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) acc[q] = 0.f;
+      for (int r = 0; r < D; ++r) {
+        const float* wr = win + (a + r) + b0 * WD;  // row a + r of the window, from column b0
+        const float4* x4p = reinterpret_cast<const float4*>(xr + r * D);
+        float wv[NB];  // wv[j & 7] = window column b0 + j of this row
+#pragma unroll
+        for (int q = 0; q < NB - 1; ++q) wv[q] = wr[q * WD];
+#pragma unroll
+        for (int c4 = 0; c4 < D / 4; ++c4) {
+          const float4 x4 = x4p[c4];
+          const float xs[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int c = c4 * 4 + u;
+            wv[(c + NB - 1) & (NB - 1)] = wr[(c + NB - 1) * WD];
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+              const float t = xs[u] - wv[(c + q) & (NB - 1)];
+              acc[q] = fmaf(t, t, acc[q]);
+            }
+          }
         }
-      const uint32_t idx = (uint32_t)(a + b * D + f * DD);
-      keys[idx] = ((unsigned long long)__float_as_uint(acc) << 32) | idx;
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const uint32_t idx = (uint32_t)(a + (b0 + q) * D + f * DD);
+        keys[idx] = ((unsigned long long)__float_as_uint(acc[q]) << 32) | idx;
+      }
+    } else {
+      for (int cand = tid; cand < DD; cand += 128) {
+        const int a = cand % D, b = cand / D;
+        float acc = 0.f;
+        for (int r = 0; r < D; ++r)
+#pragma unroll 8
+          for (int c = 0; c < D; ++c) {
+            const float t = xr[r * D + c] - win[(a + r) + (b + c) * WD];
+            acc = fmaf(t, t, acc);
+          }
+        const uint32_t idx = (uint32_t)(a + b * D + f * DD);
+        keys[idx] = ((unsigned long long)__float_as_uint(acc) << 32) | idx;
+      }
     }
   }
   __syncthreads();
@@ -90,10 +131,12 @@ __global__ void __launch_bounds__(128) k_match_video(VideoMatchArgs A) {
 // of frame fr; contributions (reference y, x, slot k) in the reference's loop
 // order, block k of (y, x) starting at (a + y d - d/2, b + x d - d/2) of frame
 // f (skipped when the start is negative); each term fl(w * block) is added in
-// double (the reference's U and out.K are double arrays).
+// double (the reference's U and out.K are double arrays).  DT is the patch
+// size at compile time (the index decoding becomes shifts), 0 = A.d.
+template <int DT>
 __global__ void k_aggregate_video(VideoAggArgs A) {
   const size_t total = (size_t)A.m * A.n * A.F;
-  const int d = A.d, h = d / 2, K = A.K;
+  const int d = DT ? DT : A.d, h = d / 2, K = A.K;
   const size_t mn = (size_t)A.m * A.n;
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
     const int r = (int)(p % A.m), c = (int)((p / A.m) % A.n), fr = (int)(p / mn);
@@ -154,7 +197,12 @@ cudaError_t launch_match_video(int d, const VideoMatchArgs& A, cudaStream_t st) 
 }
 
 cudaError_t launch_aggregate_video(const VideoAggArgs& A, cudaStream_t st) {
-  k_aggregate_video<<<1184, 256, 0, st>>>(A);
+  switch (A.d) {
+    case 8: k_aggregate_video<8><<<1184, 256, 0, st>>>(A); break;
+    case 16: k_aggregate_video<16><<<1184, 256, 0, st>>>(A); break;
+    case 32: k_aggregate_video<32><<<1184, 256, 0, st>>>(A); break;
+    default: k_aggregate_video<0><<<1184, 256, 0, st>>>(A); break;
+  }
   return cudaGetLastError();
 }
 

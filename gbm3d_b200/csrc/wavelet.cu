@@ -173,6 +173,154 @@ __global__ void __launch_bounds__(256) k_wav_synthesis(const float* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// Dense banks: every spatial filter has the taps 0..R and the slot filters
+// the taps 0, 1 (sym4 x Haar, getWaveFilters3D('sym','db',4,1), VBM3D's bank:
+// R = 7).  These are the generic kernels' three passes with the tile shapes
+// and tap loops fixed at compile time, single wraps in place of the modulo
+// (the launcher checks the sizes that make one wrap enough), and in the
+// synthesis y-pass the two output parities of a coefficient pair computed by
+// one thread (the generic pass predicates off half the taps in alternate
+// lanes).  Every output is the same serial fmaf chain, over the same taps in
+// the same order, as in the generic kernels.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int wrap_once(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
+
+template <int R>
+__global__ void __launch_bounds__(256) k_wav_analysis_dense(const float* __restrict__ in, int Ly, int Lx, int Lz,
+                                                            int shift, float* __restrict__ out, WaveletBank bk,
+                                                            LevelBands th, int tx0) {
+  constexpr int NY = 2 * TQ + R;
+  extern __shared__ float sm[];
+  float* tz = sm;                // [2][NY(x)][NY(y)]
+  float* tx = sm + 2 * NY * NY;  // [4][TQ(qx)][NY(y)]
+  const int Oy = Ly >> 1, Ox = Lx >> 1, Oz = Lz >> 1;
+  const int ntx = (Ox + TQ - 1) / TQ, bx = blockIdx.y + tx0;
+  const int qy0 = blockIdx.x * TQ, qx0 = (bx >= ntx ? bx - ntx : bx) * TQ, qz = blockIdx.z;
+  const int y0 = 2 * qy0 - R - shift, x0 = 2 * qx0 - R - shift;
+  const size_t plane = (size_t)Ly * Lx;
+  // the slot taps k = 0, 1 read slots (2 qz - k - shift) mod Lz
+  const size_t zo0 = plane * (size_t)wrap_once(2 * qz - shift, Lz);
+  const size_t zo1 = plane * (size_t)wrap_once(2 * qz - 1 - shift, Lz);
+  float hz[2][2];
+#pragma unroll
+  for (int f = 0; f < 2; ++f) {
+    hz[f][0] = bk.z.a[f].h[0];
+    hz[f][1] = bk.z.a[f].h[1];
+  }
+  // load + z-pass (slot axis)
+  for (int e = threadIdx.x; e < NY * NY; e += 256) {
+    const int yy = e % NY, xx = e / NY;
+    const int y = wrap_once(y0 + yy, Ly), x = wrap_once(x0 + xx, Lx);
+    const float* col = in + y + (size_t)Ly * x;
+    const float v0 = col[zo0], v1 = col[zo1];
+#pragma unroll
+    for (int fz = 0; fz < 2; ++fz) tz[fz * NY * NY + e] = fmaf(hz[fz][1], v1, fmaf(hz[fz][0], v0, 0.f));
+  }
+  __syncthreads();
+  // x-pass
+  for (int e = threadIdx.x; e < 4 * TQ * NY; e += 256) {
+    const int yy = e % NY, qx = (e / NY) % TQ, comb = e / (NY * TQ);
+    const int fx = comb & 1, fz = comb >> 1;
+    const float* src = tz + fz * NY * NY + yy + (2 * qx + R) * NY;
+    float acc = 0.f;
+#pragma unroll
+    for (int u = 0; u <= R; ++u) acc = fmaf(fx ? bk.xy.a[1].h[u] : bk.xy.a[0].h[u], src[-u * NY], acc);
+    tx[(comb * TQ + qx) * NY + yy] = acc;
+  }
+  __syncthreads();
+  // y-pass + hard threshold + store
+  const size_t bsz = (size_t)Oy * Ox * Oz;
+  for (int e = threadIdx.x; e < 8 * TQ * TQ; e += 256) {
+    const int qy = e % TQ, qx = (e / TQ) % TQ, code = e / (TQ * TQ);
+    if (qy0 + qy >= Oy || qx0 + qx >= Ox) continue;
+    const int fy = code & 1, comb = code >> 1;
+    const float* src = tx + (comb * TQ + qx) * NY + 2 * qy + R;
+    float acc = 0.f;
+#pragma unroll
+    for (int u = 0; u <= R; ++u) acc = fmaf(fy ? bk.xy.a[1].h[u] : bk.xy.a[0].h[u], src[-u], acc);
+    if (code) acc = acc * (fabsf(acc) > th.tau[code] ? 1.f : 0.f);
+    out[code * bsz + (qy0 + qy) + (size_t)Oy * ((qx0 + qx) + (size_t)Ox * qz)] = acc;
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_wav_synthesis_dense(const float* __restrict__ bands,
+                                                             const float* __restrict__ approx, int Oy, int Ox,
+                                                             int Oz, SynthOut o, WaveletBank bk, int tx0) {
+  constexpr int NQ = (TP - 1 + R) / 2 + 1;
+  extern __shared__ float sm[];
+  float* B = sm;               // [8][NQ(qx)][NQ(qy)]
+  float* Y = B + 8 * NQ * NQ;  // [4][NQ(qx)][TP(py)]
+  float* X = Y + 4 * NQ * TP;  // [2][TP(px)][TP(py)]
+  const int Iy = Oy >> 1, Ix = Ox >> 1, Iz = Oz >> 1;
+  const int ntx = (Ox + TP - 1) / TP, bx = blockIdx.y + tx0;
+  const int py0 = blockIdx.x * TP, px0 = (bx >= ntx ? bx - ntx : bx) * TP, qz = blockIdx.z;
+  const int qy0 = py0 >> 1, qx0 = px0 >> 1;
+  const size_t bsz = (size_t)Iy * Ix * Iz;
+
+  for (int e = threadIdx.x; e < 8 * NQ * NQ; e += 256) {
+    const int qyl = e % NQ, qxl = (e / NQ) % NQ, code = e / (NQ * NQ);
+    const int qy = wrap_once(qy0 + qyl, Iy), qx = wrap_once(qx0 + qxl, Ix);
+    const float* src = code ? bands + code * bsz : approx;
+    B[e] = src[qy + (size_t)Iy * (qx + (size_t)Ix * qz)];
+  }
+  __syncthreads();
+  // y-pass: outputs py = 2j (even taps) and 2j + 1 (odd taps) of one thread,
+  // each summing fy = 0 then 1, taps in ascending order
+  for (int e = threadIdx.x; e < 4 * NQ * (TP / 2); e += 256) {
+    const int j = e % (TP / 2), qxl = (e / (TP / 2)) % NQ, comb = e / ((TP / 2) * NQ);
+    float ae = 0.f, ao = 0.f;
+#pragma unroll
+    for (int fy = 0; fy < 2; ++fy) {
+      const float* src = B + (fy + 2 * comb) * NQ * NQ + qxl * NQ + j;
+#pragma unroll
+      for (int u = 0; u <= R; ++u) {
+        const float h = fy ? bk.xy.s[1].h[u] : bk.xy.s[0].h[u];
+        if (u & 1) ao = fmaf(h, src[(u + 1) >> 1], ao);  // (2j + 1 + u) / 2
+        else ae = fmaf(h, src[u >> 1], ae);              // (2j + u) / 2
+      }
+    }
+    *reinterpret_cast<float2*>(Y + (comb * NQ + qxl) * TP + 2 * j) = make_float2(ae, ao);
+  }
+  __syncthreads();
+  // x-pass: combine fx for each fz (px is uniform across a warp)
+  for (int e = threadIdx.x; e < 2 * TP * TP; e += 256) {
+    const int py = e % TP, px = (e / TP) % TP, fz = e / (TP * TP);
+    float acc = 0.f;
+#pragma unroll
+    for (int fx = 0; fx < 2; ++fx) {
+      const float* src = Y + (fx + 2 * fz) * NQ * TP + py;
+#pragma unroll
+      for (int u = 0; u <= R; ++u) {
+        if ((px + u) & 1) continue;
+        acc = fmaf(fx ? bk.xy.s[1].h[u] : bk.xy.s[0].h[u], src[((px + u) >> 1) * TP], acc);
+      }
+    }
+    X[(fz * TP + px) * TP + py] = acc;
+  }
+  __syncthreads();
+  // z-pass: output pz = 2qz takes the slot tap 0 of both bands, pz = 2qz - 1 tap 1
+  for (int e = threadIdx.x; e < 2 * TP * TP; e += 256) {
+    const int py = e % TP, px = (e / TP) % TP, which = e / (TP * TP);
+    if (py0 + py >= Oy || px0 + px >= Ox) continue;
+    const int pz = wrap_once(2 * qz - which, Oz);
+    float acc = 0.f;
+#pragma unroll
+    for (int fz = 0; fz < 2; ++fz)
+      acc = fmaf(which ? bk.z.s[fz].h[1] : bk.z.s[fz].h[0], X[(fz * TP + px) * TP + py], acc);
+    const int oy = wrap_once(py0 + py - o.shift, Oy), ox = wrap_once(px0 + px - o.shift, Ox),
+              oz = wrap_once(pz - o.shift, Oz);
+    float* dst = o.out + oy + (size_t)Oy * (ox + (size_t)Ox * oz);
+    float v = o.first ? acc : *dst + acc;
+    if (o.last) {
+      v = v / o.cycles;
+      v = v > 0.f ? v : 0.f;
+    }
+    *dst = v;
+  }
+}
+
 // getBM3DAggWeights(3,1) (getBM3DAggWeights.m:11-19) and weight = 1/(D+eps)
 // (denoiseAndAggregateGPU.m:75), one warp per group.  Each of the three sums
 // is a fixed-order reduction: lane l adds the elements l, l+32, ... of the
@@ -672,6 +820,50 @@ static size_t synthesis_smem(int reach) {
   return (size_t)(8 * NQ * NQ + 4 * NQ * TP + 2 * TP * TP) * sizeof(float);
 }
 
+// R when every spatial filter has exactly the taps 0..R and every slot filter
+// the taps 0 and 1, else -1
+static int dense_reach(const WaveletBank& bk) {
+  const int R = bk.xy.a[0].n - 1;
+  auto dense = [](const Taps& t, int n) {
+    if (t.n != n) return false;
+    for (int u = 0; u < n; ++u)
+      if (t.k[u] != u) return false;
+    return true;
+  };
+  for (int f = 0; f < 2; ++f)
+    if (!dense(bk.xy.a[f], R + 1) || !dense(bk.xy.s[f], R + 1) || !dense(bk.z.a[f], 2) || !dense(bk.z.s[f], 2))
+      return -1;
+  return R;
+}
+
+// analysis (AN) or synthesis of a dense bank of reach R; the tile grids are
+// the generic kernels'
+template <bool AN, int R>
+static cudaError_t launch_dense(const float* in, const float* approx, int Ly, int Lx, int Lz, int shift, float* out,
+                                const SynthOut& o, const WaveletBank& bk, const LevelBands& th, cudaStream_t st,
+                                const ColRange& cols) {
+  if (AN) {
+    const size_t sm = analysis_smem(R);
+    cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_dense<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int t0, nt;
+    tile_span(cols, Lx / 2, TQ, t0, nt);
+    if (nt == 0) return cudaSuccess;
+    dim3 grid((Ly / 2 + TQ - 1) / TQ, nt, Lz / 2);
+    k_wav_analysis_dense<R><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, bk, th, t0);
+  } else {
+    const size_t sm = synthesis_smem(R);
+    cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_dense<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int t0, nt;
+    tile_span(cols, Lx, TP, t0, nt);
+    if (nt == 0) return cudaSuccess;
+    dim3 grid((Ly + TP - 1) / TP, nt, Lz / 2);
+    k_wav_synthesis_dense<R><<<grid, 256, sm, st>>>(in, approx, Ly, Lx, Lz, o, bk, t0);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shift, float* out,
                                 const WaveletBank& bk, const LevelBands& th, cudaStream_t st,
                                 const ColRange& qcols) {
@@ -682,6 +874,11 @@ cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shi
     if (kind == 1) return launch_analysis_fast<10, 4>(in, Ly, Lx, Lz, shift, out, fb, th, st, qcols);
     return launch_analysis_fast<2, 0>(in, Ly, Lx, Lz, shift, out, fb, th, st, qcols);
   }
+  // dense sym4 x Haar bank: one wrap of every index is enough when the level
+  // exceeds a tile plus the filter reach and the shift is below every size
+  if (dense_reach(bk) == 7 && shift >= 0 && Ly >= 2 * TQ + 7 + shift && Lx >= 2 * TQ + 7 + shift && Lz >= 2 &&
+      shift + 1 <= Lz)
+    return launch_dense<true, 7>(in, nullptr, Ly, Lx, Lz, shift, out, SynthOut{}, bk, th, st, qcols);
   const size_t sm = analysis_smem(bk.reach_a);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
@@ -703,6 +900,9 @@ cudaError_t launch_wav_synthesis(const float* bands, const float* approx, int Oy
     if (kind == 1) return launch_synthesis_fast<4, 10>(bands, approx, Oy, Ox, Oz, o, fb, st, cols);
     return launch_synthesis_fast<0, 2>(bands, approx, Oy, Ox, Oz, o, fb, st, cols);
   }
+  if (dense_reach(bk) == 7 && Oy >= 2 * TP + 8 && Ox >= 2 * TP + 8 && Oz >= 2 && o.shift >= 0 && o.shift < Oy &&
+      o.shift < Ox && o.shift < Oz)
+    return launch_dense<false, 7>(bands, approx, Oy, Ox, Oz, 0, nullptr, o, bk, LevelBands{}, st, cols);
   const size_t sm = synthesis_smem(bk.reach_s);
   cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;

@@ -31,6 +31,7 @@ CASES_MATCH = [
     (64, 64, 3, 16, 16, 3),
     (96, 64, 5, 32, 16, 4),
     (48, 56, 11, 8, 8, 5),
+    (64, 96, 3, 32, 16, 6),  # patch 32, 3-frame window: the batched configuration's video shape
 ]
 
 
@@ -45,7 +46,8 @@ def test_matchBlocksV_bit_identical(gpu, oracle, m, n, F, d, K, seed):
     assert np.all(np.asarray(S)[0] == d * d * F // 2 + d // 2 + 1)  # slot 1 is the reference (matchBlocksV.m:103)
 
 
-@pytest.mark.parametrize("m,n,F,d,K,seed", CASES_MATCH[:4])
+# the 320 x 288 case reaches the dense sym4 x Haar wavelet kernels at every level
+@pytest.mark.parametrize("m,n,F,d,K,seed", CASES_MATCH[:4] + [(320, 288, 3, 8, 16, 7)])
 def test_denoiseAndAggregateV_bit_identical(gpu, oracle, m, n, F, d, K, seed):
     """The stage alone, fed the oracle's match sets and volume."""
     _, I, s = _frames(m, n, F, 25.0, seed)
@@ -63,6 +65,8 @@ CASES_VBM3D = [
     (30, 44, 5, 3, 8, (0, 4), 6),     # not a multiple of d: mirror padding
     (64, 64, 7, 5, 16, (0, 8), 7),
     (40, 48, 6, 5, 8, (0, 2, 5), 8),  # three spins: the mean divides by 3
+    (80, 100, 4, 3, 32, (0, 16), 9),  # VBM3D's default patch 32 (register-tiled matcher), mirror padding
+    (192, 256, 4, 3, 32, (0, 16), 10),  # levels 1-2 of the wavelet on the dense sym4 x Haar kernels
 ]
 
 
