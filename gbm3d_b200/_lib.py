@@ -56,6 +56,7 @@ class gbm3d_mixed_batch(C.Structure):
         ("rgb_sigma", C.c_void_p), ("rgb_out", C.c_void_p),
         ("video", C.c_void_p), ("video_m", C.c_int), ("video_n", C.c_int), ("video_frames", C.c_int),
         ("video_sigma", C.c_double), ("video_out", C.c_void_p),
+        ("grey_opts", C.c_void_p), ("rgb_opts", C.c_void_p),
     ]
 
 

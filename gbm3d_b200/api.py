@@ -367,7 +367,7 @@ def GBM3D_rgb(I, sigma, opts: dict | None = None, ctx: Context | None = None):
 
 def GBM3D_mixed(grey=(), grey_sigma=(), rgb=(), rgb_sigma=(), video=None, video_sigma: float = 0.0,
                 opts: dict | None = None, vopts: dict | None = None, use_graph: bool = True,
-                ctx: Context | None = None, outputs=None):
+                ctx: Context | None = None, outputs=None, grey_opts=None, rgb_opts=None):
     """Batched form over a mixed submission (gbm3d_denoise_mixed): grey
     device images (torch float64 (n, m) tensors, i.e. column-major m x n),
     colour images as (R, G, B) triples of such tensors, and one video (a
@@ -375,8 +375,12 @@ def GBM3D_mixed(grey=(), grey_sigma=(), rgb=(), rgb_sigma=(), video=None, video_
     call; with use_graph the whole launch sequence is captured into one CUDA
     graph on the first call and replayed by later calls with the same
     geometry.  Grey and colour images use ``opts``, the video ``vopts``
-    (VBM3D.m's defaults).  Returns (grey outputs, colour output triples, video
-    output (frames - nF + 1, n, m) or None) once the work has finished."""
+    (VBM3D.m's defaults).  ``grey_opts`` / ``rgb_opts``, when given, hold one
+    option dict per image instead, each resolved at that image's size and
+    sigma (so {"profile": "tuned"} gives every image the autotuner's set for
+    its own size and noise class).  Returns (grey outputs, colour output
+    triples, video output (frames - nF + 1, n, m) or None) once the work has
+    finished."""
     import torch
     ctx = ctx or context()
     o = c_opts(_opt.resolve_opts(opts))
@@ -414,6 +418,20 @@ def GBM3D_mixed(grey=(), grey_sigma=(), rgb=(), rgb_sigma=(), video=None, video_
         b.video_out = v_out.data_ptr()
     if len(grey_sigma) != len(grey) or len(rgb_sigma) != len(rgb):
         raise GBM3DError(1, "one sigma per image")
+
+    def per_image(optlist, shapes, sigmas):
+        if optlist is None:
+            return None
+        if len(optlist) != len(shapes):
+            raise GBM3DError(1, "one option set per image")
+        a = (gbm3d_opts * max(len(optlist), 1))()
+        for k, (d, sh, sg) in enumerate(zip(optlist, shapes, sigmas)):
+            a[k] = c_opts(_opt.resolve_opts(d, shape=sh, sigma=sg))
+        keep.append(a)
+        return C.cast(a, C.c_void_p)
+
+    b.grey_opts = per_image(grey_opts, [(int(x.shape[1]), int(x.shape[0])) for x in grey], grey_sigma)
+    b.rgb_opts = per_image(rgb_opts, [(int(t[0].shape[1]), int(t[0].shape[0])) for t in rgb], rgb_sigma)
     torch.cuda.synchronize()
     ctx.check(lib().gbm3d_denoise_mixed(ctx.h, C.byref(b), C.byref(o), C.byref(cv) if cv is not None else None,
                                         1 if use_graph else 0))

@@ -2093,10 +2093,19 @@ int gbm3d_denoise_mixed(gbm3d_ctx* c, const gbm3d_mixed_batch* b, const gbm3d_op
     };
     std::stable_sort(og.begin(), og.end(), larger(b->grey_m, b->grey_n));
     std::stable_sort(orgb.begin(), orgb.end(), larger(b->rgb_m, b->rgb_n));
+    // each image's options: its own entry of grey_opts / rgb_opts, else opts
+    auto grey_o = [&](int k) { return b->grey_opts ? b->grey_opts + k : o; };
+    auto rgb_o = [&](int k) { return b->rgb_opts ? b->rgb_opts + k : o; };
+    bool learned = o->form == 2;
+    for (int k = 0; k < b->n_grey; ++k) learned |= grey_o(k)->form == 2;
+    for (int k = 0; k < b->n_rgb; ++k) learned |= rgb_o(k)->form == 2;
     std::string key("mixed");
     key_add(key, *o);
     if (b->video) key_add(key, *ov);
+    key_add(key, (int)(b->grey_opts != nullptr));
+    key_add(key, (int)(b->rgb_opts != nullptr));
     for (int k = 0; k < b->n_grey; ++k) {
+      if (b->grey_opts) key_add(key, b->grey_opts[k]);
       key_add(key, b->grey[k]);
       key_add(key, b->grey_out[k]);
       key_add(key, b->grey_m[k]);
@@ -2104,6 +2113,7 @@ int gbm3d_denoise_mixed(gbm3d_ctx* c, const gbm3d_mixed_batch* b, const gbm3d_op
       key_add(key, b->grey_sigma[k]);
     }
     for (int k = 0; k < b->n_rgb; ++k) {
+      if (b->rgb_opts) key_add(key, b->rgb_opts[k]);
       for (int q = 0; q < 3; ++q) {
         key_add(key, b->rgb[3 * k + q]);
         key_add(key, b->rgb_out[3 * k + q]);
@@ -2133,7 +2143,7 @@ int gbm3d_denoise_mixed(gbm3d_ctx* c, const gbm3d_mixed_batch* b, const gbm3d_op
     if (b->video) items.push_back({2, 0, 2.0 * b->video_m * b->video_n * b->video_frames});
     std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.work > y.work; });
     // the learned pilot's parameters live in unprefixed buffers: one lane
-    const int L = std::max(1, std::min({c->lanes, (int)items.size(), o->form == 2 ? 1 : 16}));
+    const int L = std::max(1, std::min({c->lanes, (int)items.size(), learned ? 1 : 16}));
     key_add(key, L);
     std::vector<int> lane(items.size(), 0);
     {
@@ -2157,9 +2167,9 @@ int gbm3d_denoise_mixed(gbm3d_ctx* c, const gbm3d_mixed_batch* b, const gbm3d_op
     auto run_item = [&](const Item& it) {
       const int k = it.k;
       if (it.kind == 0)
-        pipeline(c, b->grey[k], b->grey_m[k], b->grey_n[k], b->grey_sigma[k], o, b->grey_out[k], nullptr);
+        pipeline(c, b->grey[k], b->grey_m[k], b->grey_n[k], b->grey_sigma[k], grey_o(k), b->grey_out[k], nullptr);
       else if (it.kind == 1)
-        pipeline_rgb(c, b->rgb + 3 * k, b->rgb_m[k], b->rgb_n[k], b->rgb_sigma[k], o, b->rgb_out + 3 * k);
+        pipeline_rgb(c, b->rgb + 3 * k, b->rgb_m[k], b->rgb_n[k], b->rgb_sigma[k], rgb_o(k), b->rgb_out + 3 * k);
       else
         pipeline_video(c, b->video, b->video_m, b->video_n, b->video_frames, b->video_sigma, ov, b->video_out);
     };

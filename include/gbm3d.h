@@ -238,8 +238,9 @@ int gbm3d_denoise_batch(gbm3d_ctx* ctx, int nimg, const double* const* I, const 
 
 /* Mixed batch: grey images, colour images and one video in one submission
  * (device pointers, float64 column-major).  Grey images run the whole-image
- * pipeline of gbm3d_denoise_device with opts at their own sigma, colour images
- * the opponent-space pipeline of gbm3d_denoise_rgb_device with opts, and the
+ * pipeline of gbm3d_denoise_device with opts (or their own grey_opts entry) at
+ * their own sigma, colour images the opponent-space pipeline of
+ * gbm3d_denoise_rgb_device with opts (or their rgb_opts entry), and the
  * video the VBM3D pipeline of gbm3d_vbm3d_device with video_opts (frames on
  * the [0,1] scale).  Any part may be empty (count 0, video null).  With
  * use_graph the first call runs everything and captures the whole launch
@@ -265,6 +266,13 @@ typedef struct gbm3d_mixed_batch {
   int video_m, video_n, video_frames;
   double video_sigma;
   double* video_out;              /* video_m x video_n x (video_frames - videoFrames + 1) */
+  /* Per-image options: n_grey (n_rgb) structs, image k taking entry k, or
+   * null for the call's opts on every image of that kind.  A batch of uneven
+   * sizes and noise levels can so give each image the autotuner's set for its
+   * own size and sigma class.  Leave both null (zero-initialise the struct)
+   * when one option set serves the whole batch. */
+  const gbm3d_opts* grey_opts;
+  const gbm3d_opts* rgb_opts;
 } gbm3d_mixed_batch;
 int gbm3d_denoise_mixed(gbm3d_ctx* ctx, const gbm3d_mixed_batch* batch, const gbm3d_opts* opts,
                         const gbm3d_opts* video_opts, int use_graph);

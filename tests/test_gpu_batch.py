@@ -148,6 +148,50 @@ def _mixed_case():
     assert np.array_equal(g_out[0].cpu().numpy().reshape(-1).reshape(m, n, order="F"), grey_ref[0])
 
 
+def test_mixed_batch_per_image_options(gpu):
+    """Each image of a mixed submission with its own option set (grey_opts /
+    rgb_opts: strides, spins and cycle spins differing between images) gets
+    what its single-image entry gives with that set, bit for bit: eager, then
+    captured and replayed, on two lanes."""
+    import torch
+    from gbm3d_b200 import api
+    dev = torch.device("cuda", 0)
+
+    def col(a):
+        return torch.from_numpy(np.asfortranarray(a).ravel(order="F").copy()).to(dev)
+
+    sets = [_dense(), _dense(refStride=8, refStrideWie=4, matchSpins=[0], matchSpinsWie=[0, 2], cycleSpin=1),
+            _dense(refStride=6, refStrideWie=6, matchSpins=[0], matchSpinsWie=[0], cycleSpin=2)]
+    grey_sizes, grey_sig = [(96, 80), (64, 72), (120, 96)], [10.0, 30.0, 45.0]
+    noisy = [synth.noisy_image(m, n, s, seed=180 + k)[1] for k, ((m, n), s) in enumerate(zip(grey_sizes, grey_sig))]
+    grey = [col(x).view(n, m) for x, (m, n) in zip(noisy, grey_sizes)]
+    grey_ref = [api.GBM3D(x, s, o)[0] for x, s, o in zip(noisy, grey_sig, sets)]
+    rgb_sizes, rgb_sig = [(80, 64), (64, 96)], [20.0, 35.0]
+    rgb_sets = [sets[1], sets[2]]
+    rgb, rgb_ref = [], []
+    for k, ((m, n), s) in enumerate(zip(rgb_sizes, rgb_sig)):
+        planes = np.stack([synth.noisy_image(m, n, s, seed=190 + 3 * k + q)[1] for q in range(3)], axis=2)
+        rgb.append(tuple(col(planes[:, :, q]).view(n, m) for q in range(3)))
+        rgb_ref.append(api.GBM3D_rgb(planes, s, rgb_sets[k]))
+    api.context().set_lanes(2)
+    try:
+        for use_graph, calls in ((False, 1), (True, 2)):
+            for _ in range(calls):
+                g_out, c_out, _ = api.GBM3D_mixed(grey, grey_sig, rgb, rgb_sig, opts=_dense(), use_graph=use_graph,
+                                                  grey_opts=sets, rgb_opts=rgb_sets)
+                for k, (m, n) in enumerate(grey_sizes):
+                    got = g_out[k].cpu().numpy().reshape(-1).reshape(m, n, order="F")
+                    assert np.array_equal(got, grey_ref[k]), f"grey image {k} (graph={use_graph})"
+                for k, (m, n) in enumerate(rgb_sizes):
+                    for q in range(3):
+                        got = c_out[k][q].cpu().numpy().reshape(-1).reshape(m, n, order="F")
+                        assert np.array_equal(got, rgb_ref[k][:, :, q]), f"colour image {k} plane {q}"
+    finally:
+        api.context().set_lanes(1)
+    with pytest.raises(api.GBM3DError):
+        api.GBM3D_mixed(grey, grey_sig, opts=_dense(), grey_opts=sets[:2])
+
+
 def test_async_host_stream_matches_sync(gpu):
     """gbm3d_denoise_async over a stream of host images (sizes changing along
     the way) gives every image the synchronous entry's result bit for bit, and
