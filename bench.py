@@ -447,16 +447,27 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def batched_block(ctx, stream, work, reps=3):
+# How the batched block gives each image its option set (see batched_block).
+BATCH_RULE = "calibrated"
+BATCH_RULES = ("floor512", "calibrated", "calibrated_sigma_below", "uniform512")
+
+
+def batched_block(ctx, stream, work, reps=3, rule=None):
     """The batched form's mixed submission (64 grey images of uneven sizes
     and noise levels, 8 RGB 1024^2 images, a 32-frame 1280x720 video) through
     gbm3d_denoise_mixed: eager launches on one stream, and one captured CUDA
     graph per lane count (the items spread over 1, 2, 4 or 8 concurrent
     streams; the fastest count is the schedule kept), device time per
-    submission (CUDA events), MPix/s.  Grey and colour images use the
-    'tuned' profile's set of the smallest size class (the most conservative
-    one for a batch of uneven sizes), the video VBM3D.m's defaults with a
-    3-frame window."""
+    submission (CUDA events), MPix/s.  Each grey and colour image takes an
+    option set by ``rule`` (grey_opts / rgb_opts): 'calibrated' the 'tuned'
+    profile's set for its own size and sigma class (below the smallest
+    calibrated side, 512, the dense configuration, as the profile defines
+    it); 'calibrated_sigma_below' the same with the noise class rounded down;
+    'floor512' images below 512 take the 512 class; 'uniform512' every image
+    the 512 / sigma 25 set.  The video takes VBM3D.m's defaults with a
+    3-frame window.  The grey outputs are compared with the dense plain
+    configuration's (PSNR against the clean images)."""
+    rule = rule or BATCH_RULE
     import torch
     from gbm3d_b200 import api, options as _opt
     grey_pairs, gs, rgb, rs, frames, vs = work
@@ -464,6 +475,18 @@ def batched_block(ctx, stream, work, reps=3):
     dev = torch.device("cuda", ctx.device)
     o = _opt.resolve_opts({"profile": "tuned"}, shape=(512, 512), sigma=SIGMA) \
         if os.path.exists(_opt.TUNED_SETS) else opts()
+
+    def own_set(shape, sigma):
+        if not os.path.exists(_opt.TUNED_SETS):
+            return opts()
+        if rule == "uniform512":
+            return dict(o)
+        if rule == "floor512":
+            return _opt.tuned_opts(max(shape[0], 512), max(shape[1], 512), float(sigma))
+        return _opt.tuned_opts(shape[0], shape[1], float(sigma), sigma_below=rule == "calibrated_sigma_below")
+
+    g_sets = [own_set(x.shape, s) for x, s in zip(grey, gs)]
+    c_sets = [own_set(x.shape[:2], s) for x, s in zip(rgb, rs)]
 
     def col(x):
         return torch.from_numpy(np.asfortranarray(x).ravel(order="F").copy()).to(dev)
@@ -477,12 +500,13 @@ def batched_block(ctx, stream, work, reps=3):
 
     def timed(use_graph, lanes=1):
         ctx.set_lanes(lanes)
-        outs = api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, use_graph=use_graph, ctx=ctx)  # warm-up / capture
+        kw = dict(use_graph=use_graph, ctx=ctx, grey_opts=g_sets, rgb_opts=c_sets)
+        outs = api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, **kw)  # warm-up / capture
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
-            api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, use_graph=use_graph, ctx=ctx, outputs=outs)
+            api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, outputs=outs, **kw)
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps, ctx.launch_count(), outs
@@ -498,20 +522,39 @@ def batched_block(ctx, stream, work, reps=3):
     best = min(lanes_ms, key=lanes_ms.get)
     graph_ms, graph_launches, outs = timed(True, best)
     ctx.set_lanes(1)
-    gains = []
+    # the dense plain configuration on the same grey images (one eager call)
+    dense = opts() if WL == "dense" else _opt.resolve_opts(dict(_opt.setBM3Dopts("default"), **_opt.DENSE))
+    plain = api.GBM3D_mixed(dg, gs, opts=dense, use_graph=False, ctx=ctx)[0]
+    gains, vs_plain = [], []
     for k, (clean, x) in enumerate(grey_pairs):
         U = outs[0][k].cpu().numpy().reshape(-1).reshape(x.shape, order="F")
+        P = plain[k].cpu().numpy().reshape(-1).reshape(x.shape, order="F")
         gains.append(float(_opt.myPSNR(clean, U, 255) - _opt.myPSNR(clean, x, 255)))
+        vs_plain.append(float(_opt.myPSNR(clean, U, 255) - _opt.myPSNR(clean, P, 255)))
     return {"workload": "64 grey (200x300 .. 2048x1536, sigma 5-50) + 8 RGB 1024^2 (opponent colour, luma "
                         "matching) + 32-frame 1280x720 video (+-1 frame), one gbm3d_denoise_mixed submission",
-            "megapixels": mpix, "opts": {k: o.get(k, "plain") for k in (
-                "refStride", "refStrideWie", "matchSize", "matchSpins", "matchSpinsWie", "cycleSpin", "form")},
+            "megapixels": mpix, "rule": rule, "opts": {
+                "floor512": "per image: the 'tuned' set of its size (512 at least) and nearest sigma class",
+                "calibrated": "per image: the 'tuned' profile's set (size class not above its side, nearest "
+                              "sigma class; below 512 the dense configuration)",
+                "calibrated_sigma_below": "per image: the 'tuned' profile's set with the sigma class rounded down "
+                                          "(below 512 the dense configuration)",
+                "uniform512": "every image: the 'tuned' set of 512 x 512, sigma 25"}[rule],
+            "option_sets_used": sorted({json.dumps({k: g.get(k) for k in (
+                "refStride", "refStrideWie", "matchSpins", "matchSpinsWie", "cycleSpin")}, sort_keys=True)
+                for g in g_sets + c_sets}),
             "eager_ms": eager_ms, "graph_ms": graph_ms, "value": mpix / (min(eager_ms, graph_ms) / 1e3),
             "unit": "MPix/s", "eager_mpix_s": mpix / (eager_ms / 1e3), "graph_mpix_s": mpix / (graph_ms / 1e3),
             "launches_eager": eager_launches, "graph_launches_per_call": graph_launches,
             "lanes": best, "graph_ms_by_lanes": {str(k): v for k, v in lanes_ms.items()},
             "graph_equals_eager": same, "grey_psnr_gain_db_min": min(gains), "grey_psnr_gain_db_mean": float(
-                np.mean(gains))}
+                np.mean(gains)),
+            "grey_dpsnr_vs_plain_db": {"min": min(vs_plain), "mean": float(np.mean(vs_plain)),
+                                       "images_below_minus_0.05": int(sum(v < -0.05 for v in vs_plain)),
+                                       "below_minus_0.05": [[int(x.shape[0]), int(x.shape[1]), round(float(s), 2),
+                                                             round(v, 4)] for x, s, v in zip(grey, gs, vs_plain)
+                                                            if v < -0.05],
+                                       "plain": "dense configuration (stride 3, spins [0 4] + [0 4], 2 cycle spins)"}}
 
 
 def strips_block(ctx, stream, dI, o, Uref, parts=(2, 4, 8), reps=3):

@@ -186,10 +186,13 @@ __global__ void __launch_bounds__(256) k_wav_synthesis(const float* __restrict__
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int wrap_once(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
-template <int R>
+// T: coefficients per axis of a CTA's output tile (16: a 22 KB staging area,
+// eight CTAs per SM, where the 32 of the generic kernel allows two).
+template <int R, int T>
 __global__ void __launch_bounds__(256) k_wav_analysis_dense(const float* __restrict__ in, int Ly, int Lx, int Lz,
                                                             int shift, float* __restrict__ out, WaveletBank bk,
                                                             LevelBands th, int tx0) {
+  constexpr int TQ = T;
   constexpr int NY = 2 * TQ + R;
   extern __shared__ float sm[];
   float* tz = sm;                // [2][NY(x)][NY(y)]
@@ -836,21 +839,24 @@ static int dense_reach(const WaveletBank& bk) {
   return R;
 }
 
-// analysis (AN) or synthesis of a dense bank of reach R; the tile grids are
-// the generic kernels'
+// analysis (AN) or synthesis of a dense bank of reach R; the synthesis tile
+// grid is the generic kernel's, the analysis tiles DENSE_TQ coefficients wide
+constexpr int DENSE_TQ = 16;
 template <bool AN, int R>
 static cudaError_t launch_dense(const float* in, const float* approx, int Ly, int Lx, int Lz, int shift, float* out,
                                 const SynthOut& o, const WaveletBank& bk, const LevelBands& th, cudaStream_t st,
                                 const ColRange& cols) {
   if (AN) {
-    const size_t sm = analysis_smem(R);
-    cudaError_t e = cudaFuncSetAttribute(k_wav_analysis_dense<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    constexpr int T = DENSE_TQ, NY = 2 * T + R;
+    const size_t sm = (size_t)(2 * NY * NY + 4 * T * NY) * sizeof(float);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_wav_analysis_dense<R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     int t0, nt;
-    tile_span(cols, Lx / 2, TQ, t0, nt);
+    tile_span(cols, Lx / 2, T, t0, nt);
     if (nt == 0) return cudaSuccess;
-    dim3 grid((Ly / 2 + TQ - 1) / TQ, nt, Lz / 2);
-    k_wav_analysis_dense<R><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, bk, th, t0);
+    dim3 grid((Ly / 2 + T - 1) / T, nt, Lz / 2);
+    k_wav_analysis_dense<R, T><<<grid, 256, sm, st>>>(in, Ly, Lx, Lz, shift, out, bk, th, t0);
   } else {
     const size_t sm = synthesis_smem(R);
     cudaError_t e = cudaFuncSetAttribute(k_wav_synthesis_dense<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -876,8 +882,8 @@ cudaError_t launch_wav_analysis(const float* in, int Ly, int Lx, int Lz, int shi
   }
   // dense sym4 x Haar bank: one wrap of every index is enough when the level
   // exceeds a tile plus the filter reach and the shift is below every size
-  if (dense_reach(bk) == 7 && shift >= 0 && Ly >= 2 * TQ + 7 + shift && Lx >= 2 * TQ + 7 + shift && Lz >= 2 &&
-      shift + 1 <= Lz)
+  if (dense_reach(bk) == 7 && shift >= 0 && Ly >= 2 * DENSE_TQ + 7 + shift && Lx >= 2 * DENSE_TQ + 7 + shift &&
+      Lz >= 2 && shift + 1 <= Lz)
     return launch_dense<true, 7>(in, nullptr, Ly, Lx, Lz, shift, out, SynthOut{}, bk, th, st, qcols);
   const size_t sm = analysis_smem(bk.reach_a);
   cudaError_t e = cudaFuncSetAttribute(k_wav_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

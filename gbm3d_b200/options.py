@@ -76,10 +76,12 @@ DENSE = dict(blockSize=8, blockSizeWie=8, matchSize=32, numMax=16, numMin=16, re
              matchSpins=[0, 4], matchSpinsWie=[0, 4], cycleSpin=2, form="plain")
 
 
-def tuned_opts(m: int, n: int, sigma: float, table: dict | None = None) -> dict:
+def tuned_opts(m: int, n: int, sigma: float, table: dict | None = None, sigma_below: bool = False) -> dict:
     """Options of the 'tuned' profile for an m x n image at noise level sigma:
     the autotuner's set for the largest calibrated size class not above
-    min(m, n) and the calibrated sigma nearest in log scale
+    min(m, n) and the calibrated sigma nearest in log scale (with
+    ``sigma_below``, the largest calibrated sigma not above sigma, the
+    smallest one below them all: lower noise classes hold denser sets)
     (gbm3d_b200/tuned_sets.json, written by ``python -m gbm3d_b200.autotune
     --classes``).  Each set stayed within 0.05 dB (less a 0.02 dB margin) of
     the dense configuration on its calibration images; below the smallest
@@ -97,7 +99,11 @@ def tuned_opts(m: int, n: int, sigma: float, table: dict | None = None) -> dict:
     size = fit[-1]
     rows = [c for c in table["classes"] if c["size"] == size]
     sg = max(float(sigma), 1e-6)
-    row = min(rows, key=lambda c: (abs(np.log(c["sigma"] / sg)), c["sigma"]))
+    if sigma_below:
+        below = [c for c in rows if c["sigma"] <= sg]
+        row = max(below, key=lambda c: c["sigma"]) if below else min(rows, key=lambda c: c["sigma"])
+    else:
+        row = min(rows, key=lambda c: (abs(np.log(c["sigma"] / sg)), c["sigma"]))
     o.update(row["opts"])
     return o
 
