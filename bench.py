@@ -452,6 +452,20 @@ BATCH_RULE = "calibrated"
 BATCH_RULES = ("floor512", "calibrated", "calibrated_sigma_below", "uniform512")
 
 
+def batch_set(rule, shape, sigma, uniform):
+    """The option set the batched block gives an image of ``shape`` (m, n) at
+    ``sigma`` under ``rule`` (one of BATCH_RULES); ``uniform`` is the 512 /
+    sigma 25 set of the 'uniform512' rule."""
+    from gbm3d_b200 import options as _opt
+    if rule == "uniform512":
+        return dict(uniform)
+    if rule == "floor512":
+        return _opt.tuned_opts(max(shape[0], 512), max(shape[1], 512), float(sigma))
+    if rule in ("calibrated", "calibrated_sigma_below"):
+        return _opt.tuned_opts(shape[0], shape[1], float(sigma), sigma_below=rule == "calibrated_sigma_below")
+    raise ValueError(f"unknown batch rule {rule!r}")
+
+
 def batched_block(ctx, stream, work, reps=3, rule=None):
     """The batched form's mixed submission (64 grey images of uneven sizes
     and noise levels, 8 RGB 1024^2 images, a 32-frame 1280x720 video) through
@@ -477,13 +491,7 @@ def batched_block(ctx, stream, work, reps=3, rule=None):
         if os.path.exists(_opt.TUNED_SETS) else opts()
 
     def own_set(shape, sigma):
-        if not os.path.exists(_opt.TUNED_SETS):
-            return opts()
-        if rule == "uniform512":
-            return dict(o)
-        if rule == "floor512":
-            return _opt.tuned_opts(max(shape[0], 512), max(shape[1], 512), float(sigma))
-        return _opt.tuned_opts(shape[0], shape[1], float(sigma), sigma_below=rule == "calibrated_sigma_below")
+        return batch_set(rule, shape, sigma, o) if os.path.exists(_opt.TUNED_SETS) else opts()
 
     g_sets = [own_set(x.shape, s) for x, s in zip(grey, gs)]
     c_sets = [own_set(x.shape[:2], s) for x, s in zip(rgb, rs)]

@@ -196,3 +196,33 @@ def test_tuned_profile_lookup():
     assert (o["refStride"], o["refStrideWie"], o["cycleSpin"], o["matchSpins"]) == (3, 3, 2, [0, 4])
     with pytest.raises(ValueError):
         options.resolve_opts({"profile": "tuned"})
+    # sigma class rounded down: 40 -> 25 (nearest would be 50), 24 -> 10, below every class -> the smallest
+    o = options.tuned_opts(4096, 4096, 40.0, table, sigma_below=True)
+    assert (o["refStride"], o["refStrideWie"]) == (8, 6)
+    o = options.tuned_opts(600, 700, 24.0, table, sigma_below=True)
+    assert (o["refStride"], o["refStrideWie"]) == (6, 4)
+    o = options.tuned_opts(600, 700, 5.0, table, sigma_below=True)
+    assert (o["refStride"], o["refStrideWie"]) == (6, 4)
+    o = options.tuned_opts(4096, 4096, 20.0, table, sigma_below=True)  # only 25 and 50 at 2048: the smallest
+    assert (o["refStride"], o["refStrideWie"]) == (8, 6)
+
+
+def test_bench_batch_rules():
+    """The batched block's per-image option rules on the calibrated table:
+    'calibrated' is the 'tuned' profile itself (dense below 512), 'floor512'
+    lifts small images into the 512 class, 'uniform512' gives every image the
+    512 / sigma 25 set."""
+    import bench
+    from gbm3d_b200 import options
+    assert bench.BATCH_RULE in bench.BATCH_RULES
+    uniform = options.tuned_opts(512, 512, 25.0)
+    small, big = (300, 400), (1500, 1200)
+    sets = {r: (bench.batch_set(r, small, 40.0, uniform), bench.batch_set(r, big, 40.0, uniform))
+            for r in bench.BATCH_RULES}
+    assert sets["calibrated"][0]["refStride"] == 3 and sets["calibrated"][0]["cycleSpin"] == 2  # dense below 512
+    assert sets["calibrated"][1] == options.tuned_opts(1024, 1024, 50.0)  # 40 is nearer 50 than 25 in log scale
+    assert sets["calibrated_sigma_below"][1] == options.tuned_opts(1024, 1024, 25.0)
+    assert sets["floor512"][0] == options.tuned_opts(512, 512, 40.0)
+    assert sets["uniform512"] == (uniform, uniform)
+    with pytest.raises(ValueError):
+        bench.batch_set("nearest", small, 25.0, uniform)
