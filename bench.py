@@ -345,7 +345,7 @@ def cpu_baseline(o_chosen=None, size: int = 512):
     return base, parity
 
 
-def quality_by_size(ctx, fresh=None, sizes=(512, 1024, 2048, 4096)):
+def quality_by_size(ctx, fresh=None, sizes=(256, 512, 1024, 2048, 4096)):
     """PSNR of the 'tuned' profile's set against the dense plain configuration
     on seeded images of each size class (seeds not used in calibration), sigma
     25.  With a fresh autotune result, that one set is checked at every size."""
@@ -475,8 +475,8 @@ def batched_block(ctx, stream, work, reps=3, rule=None):
     submission (CUDA events), MPix/s.  Each grey and colour image takes an
     option set by ``rule`` (grey_opts / rgb_opts): 'calibrated' the 'tuned'
     profile's set for its own size and sigma class (below the smallest
-    calibrated side, 512, the dense configuration, as the profile defines
-    it); 'calibrated_sigma_below' the same with the noise class rounded down;
+    calibrated side the dense configuration, as the profile defines it);
+    'calibrated_sigma_below' the same with the noise class rounded down;
     'floor512' images below 512 take the 512 class; 'uniform512' every image
     the 512 / sigma 25 set.  The video takes VBM3D.m's defaults with a
     3-frame window.  The grey outputs are compared with the dense plain
@@ -544,9 +544,9 @@ def batched_block(ctx, stream, work, reps=3, rule=None):
             "megapixels": mpix, "rule": rule, "opts": {
                 "floor512": "per image: the 'tuned' set of its size (512 at least) and nearest sigma class",
                 "calibrated": "per image: the 'tuned' profile's set (size class not above its side, nearest "
-                              "sigma class; below 512 the dense configuration)",
+                              "sigma class; below the smallest class the dense configuration)",
                 "calibrated_sigma_below": "per image: the 'tuned' profile's set with the sigma class rounded down "
-                                          "(below 512 the dense configuration)",
+                                          "(below the smallest class the dense configuration)",
                 "uniform512": "every image: the 'tuned' set of 512 x 512, sigma 25"}[rule],
             "option_sets_used": sorted({json.dumps({k: g.get(k) for k in (
                 "refStride", "refStrideWie", "matchSpins", "matchSpinsWie", "cycleSpin")}, sort_keys=True)

@@ -182,15 +182,21 @@ def _tensor_ok(o) -> bool:
 # Calibration of the size classes: (side, sigma) -> seeds.  Small images hold
 # fewer patches, so their PSNR moves more from image to image: they are
 # calibrated on more images.
-CLASS_SIZES = (512, 1024, 2048, 4096)
+CLASS_SIZES = (256, 512, 1024, 2048, 4096)
 CLASS_SIGMAS = (10.0, 25.0, 50.0)
-CLASS_SEEDS = {512: (4242, 4243, 4244, 4245), 1024: (4242, 4243), 2048: (4242,), 4096: (4242,)}
+CLASS_SEEDS = {256: tuple(range(4242, 4250)), 512: (4242, 4243, 4244, 4245), 1024: (4242, 4243), 2048: (4242,),
+               4096: (4242,)}
 
 
-def tune_classes(sizes=CLASS_SIZES, sigmas=CLASS_SIGMAS, ctx=None, log=None) -> dict:
+def tune_classes(sizes=CLASS_SIZES, sigmas=CLASS_SIGMAS, ctx=None, log=None, table=None) -> dict:
     """The tuned option set of every (size class, sigma class): the table
-    options.tuned_opts() reads (gbm3d_b200/tuned_sets.json)."""
-    table = {"budget_db": 0.05, "margin_db": 0.02, "baseline": dict(BASELINE), "classes": []}
+    options.tuned_opts() reads (gbm3d_b200/tuned_sets.json).  With ``table``,
+    the classes of ``sizes`` are calibrated anew into a copy of it and its
+    other classes are kept."""
+    if table is None:
+        table = {"budget_db": 0.05, "margin_db": 0.02, "baseline": dict(BASELINE), "classes": []}
+    else:
+        table = dict(table, classes=[c for c in table["classes"] if c["size"] not in sizes])
     for size in sizes:
         for sigma in sigmas:
             t = tune(size, sigma, ctx=ctx, log=log, seeds=CLASS_SEEDS.get(size, (4242,)))
@@ -202,6 +208,7 @@ def tune_classes(sizes=CLASS_SIZES, sigmas=CLASS_SIGMAS, ctx=None, log=None) -> 
                 "seconds": t["seconds"]})
             if log:
                 log(json.dumps(table["classes"][-1]))
+    table["classes"].sort(key=lambda c: (c["size"], c["sigma"]))
     return table
 
 
@@ -236,13 +243,20 @@ def main():
     ap.add_argument("--classes", action="store_true",
                     help="calibrate every size and sigma class and write the table (default "
                          "gbm3d_b200/tuned_sets.json, or --out)")
+    ap.add_argument("--sizes", default=None,
+                    help="with --classes: comma-separated size classes to calibrate, merged into the existing table")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
     from . import build
     build.build()
     if a.classes:
         out = a.out or options.TUNED_SETS
-        table = tune_classes(log=print)
+        if a.sizes:
+            with open(options.TUNED_SETS) as f:
+                old = json.load(f)
+            table = tune_classes(sizes=tuple(int(v) for v in a.sizes.split(",")), log=print, table=old)
+        else:
+            table = tune_classes(log=print)
         with open(out, "w") as f:
             json.dump(table, f, indent=1)
         print(out)

@@ -209,17 +209,18 @@ def test_tuned_profile_lookup():
 
 def test_bench_batch_rules():
     """The batched block's per-image option rules on the calibrated table:
-    'calibrated' is the 'tuned' profile itself (dense below 512), 'floor512'
+    'calibrated' is the 'tuned' profile itself (dense below the smallest
+    calibrated class), 'floor512'
     lifts small images into the 512 class, 'uniform512' gives every image the
     512 / sigma 25 set."""
     import bench
     from gbm3d_b200 import options
     assert bench.BATCH_RULE in bench.BATCH_RULES
     uniform = options.tuned_opts(512, 512, 25.0)
-    small, big = (300, 400), (1500, 1200)
+    small, big = (200, 240), (1500, 1200)  # small: below every calibrated size class
     sets = {r: (bench.batch_set(r, small, 40.0, uniform), bench.batch_set(r, big, 40.0, uniform))
             for r in bench.BATCH_RULES}
-    assert sets["calibrated"][0]["refStride"] == 3 and sets["calibrated"][0]["cycleSpin"] == 2  # dense below 512
+    assert sets["calibrated"][0]["refStride"] == 3 and sets["calibrated"][0]["cycleSpin"] == 2  # dense
     assert sets["calibrated"][1] == options.tuned_opts(1024, 1024, 50.0)  # 40 is nearer 50 than 25 in log scale
     assert sets["calibrated_sigma_below"][1] == options.tuned_opts(1024, 1024, 25.0)
     assert sets["floor512"][0] == options.tuned_opts(512, 512, 40.0)
