@@ -334,6 +334,9 @@ def cpu_baseline(o_chosen=None, size: int = 512):
         dtc = time.perf_counter() - t0
         Uc64, _ = O.GBM3D(noisy, SIGMA, o_chosen, prec=64)
         parity["chosen"] = compare(api.GBM3D(noisy, SIGMA, o_chosen)[0], Uc32, Uc64)
+        parity["chosen"]["note"] = (f"the {SIZE}x{SIZE} chosen set on this {size}x{size} parity sample checks "
+                                    "bit-identity only: at this size the 'tuned' profile applies its own size "
+                                    "class's set (see quality_by_size), so the PSNR here is not a quality figure")
         # the same restatement run with the chosen form's options: the CPU
         # figure at the GPU's algorithmic settings, beside the dense one
         base["chosen_form_options"] = {"value": size * size / 1e6 / dtc, "unit": "MPix/s", "seconds": dtc,

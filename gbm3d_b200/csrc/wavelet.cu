@@ -221,29 +221,40 @@ __global__ void __launch_bounds__(256) k_wav_analysis_dense(const float* __restr
     for (int fz = 0; fz < 2; ++fz) tz[fz * NY * NY + e] = fmaf(hz[fz][1], v1, fmaf(hz[fz][0], v0, 0.f));
   }
   __syncthreads();
-  // x-pass
-  for (int e = threadIdx.x; e < 4 * TQ * NY; e += 256) {
-    const int yy = e % NY, qx = (e / NY) % TQ, comb = e / (NY * TQ);
-    const int fx = comb & 1, fz = comb >> 1;
-    const float* src = tz + fz * NY * NY + yy + (2 * qx + R) * NY;
-    float acc = 0.f;
+  // x-pass: the four (fx, fz) combinations as an unrolled outer loop, so
+  // each one's taps are compile-time indices into the bank
 #pragma unroll
-    for (int u = 0; u <= R; ++u) acc = fmaf(fx ? bk.xy.a[1].h[u] : bk.xy.a[0].h[u], src[-u * NY], acc);
-    tx[(comb * TQ + qx) * NY + yy] = acc;
+  for (int comb = 0; comb < 4; ++comb) {
+    const Taps& t = bk.xy.a[comb & 1];
+    const float* tzc = tz + (comb >> 1) * NY * NY + R * NY;
+    for (int e = threadIdx.x; e < TQ * NY; e += 256) {
+      const int yy = e % NY, qx = e / NY;
+      const float* src = tzc + yy + 2 * qx * NY;
+      float acc = 0.f;
+#pragma unroll
+      for (int u = 0; u <= R; ++u) acc = fmaf(t.h[u], src[-u * NY], acc);
+      tx[(comb * TQ + qx) * NY + yy] = acc;
+    }
   }
   __syncthreads();
-  // y-pass + hard threshold + store
+  // y-pass + hard threshold + store: a thread's coefficient (qy, qx) in all
+  // eight bands
   const size_t bsz = (size_t)Oy * Ox * Oz;
-  for (int e = threadIdx.x; e < 8 * TQ * TQ; e += 256) {
-    const int qy = e % TQ, qx = (e / TQ) % TQ, code = e / (TQ * TQ);
+  for (int e = threadIdx.x; e < TQ * TQ; e += 256) {
+    const int qy = e % TQ, qx = e / TQ;
     if (qy0 + qy >= Oy || qx0 + qx >= Ox) continue;
-    const int fy = code & 1, comb = code >> 1;
-    const float* src = tx + (comb * TQ + qx) * NY + 2 * qy + R;
-    float acc = 0.f;
+    const float* src0 = tx + qx * NY + 2 * qy + R;
+    float* dst = out + (qy0 + qy) + (size_t)Oy * ((qx0 + qx) + (size_t)Ox * qz);
 #pragma unroll
-    for (int u = 0; u <= R; ++u) acc = fmaf(fy ? bk.xy.a[1].h[u] : bk.xy.a[0].h[u], src[-u], acc);
-    if (code) acc = acc * (fabsf(acc) > th.tau[code] ? 1.f : 0.f);
-    out[code * bsz + (qy0 + qy) + (size_t)Oy * ((qx0 + qx) + (size_t)Ox * qz)] = acc;
+    for (int code = 0; code < 8; ++code) {
+      const Taps& t = bk.xy.a[code & 1];
+      const float* src = src0 + (code >> 1) * TQ * NY;
+      float acc = 0.f;
+#pragma unroll
+      for (int u = 0; u <= R; ++u) acc = fmaf(t.h[u], src[-u], acc);
+      if (code) acc = acc * (fabsf(acc) > th.tau[code] ? 1.f : 0.f);
+      dst[code * bsz] = acc;
+    }
   }
 }
 
