@@ -1,9 +1,9 @@
-"""Every `name.m:line` citation in the sources points at lines that exist.
+"""Every `name.m:line` citation in the source files points at lines that exist.
 
 The kernels, the oracle and the tests cite the MATLAB reference file by file
 and line so that each step can be audited against it.  This test reads the
 reference checkout (the directory in $GBM3D_REFERENCE_ROOT, by default the
-reference's checkout beside this build) and fails for a citation whose file is
+location in REF below) and fails for a citation whose file is
 unknown or whose highest cited line is past the end of that file.  Without the
 checkout it is skipped.
 """
@@ -16,9 +16,10 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.environ.get("GBM3D_REFERENCE_ROOT", "/root/reference")
 CITE = re.compile(r"([A-Za-z0-9_]+\.m):(\d+(?:-\d+)?(?:,\d+(?:-\d+)?)*)")
-SKIP_DIRS = {".git", "_work", "gpurun_out", "__pycache__", "_build", "baseline"}
-# review and survey notes quote citations as they found them
-SKIP_FILES = {"VERDICT.md", "SURVEY.md", "ADVICE.md"}
+# the source trees of the library, the oracle and the tests, and the
+# top-level scripts
+SOURCE_DIRS = ("gbm3d_b200", "oracle", "tests", "include")
+SOURCE_EXT = (".py", ".cu", ".cuh", ".cpp", ".h", ".c")
 
 
 def _reference_lines():
@@ -31,17 +32,24 @@ def _reference_lines():
     return index
 
 
+def _source_files():
+    for f in sorted(os.listdir(ROOT)):
+        if f.endswith(SOURCE_EXT):
+            yield os.path.join(ROOT, f)
+    for top in SOURCE_DIRS:
+        for dp, dirs, files in os.walk(os.path.join(ROOT, top)):
+            dirs[:] = [d for d in dirs if not d.startswith(("_", "."))]
+            for f in sorted(files):
+                if f.endswith(SOURCE_EXT):
+                    yield os.path.join(dp, f)
+
+
 def _citations():
-    for dp, dirs, files in os.walk(ROOT):
-        dirs[:] = [d for d in dirs if d not in SKIP_DIRS]
-        for f in files:
-            if not f.endswith((".py", ".cu", ".cuh", ".cpp", ".h", ".c", ".md")) or f in SKIP_FILES:
-                continue
-            p = os.path.join(dp, f)
-            with open(p, errors="replace") as fh:
-                for ln, line in enumerate(fh, 1):
-                    for m in CITE.finditer(line):
-                        yield os.path.relpath(p, ROOT), ln, m.group(1), m.group(2)
+    for p in _source_files():
+        with open(p, errors="replace") as fh:
+            for ln, line in enumerate(fh, 1):
+                for m in CITE.finditer(line):
+                    yield os.path.relpath(p, ROOT), ln, m.group(1), m.group(2)
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference checkout not present")
