@@ -849,7 +849,7 @@ def run_ours(args):
             "roofline": roof,
             "roofline_all": work}
     if rank == 0 and getattr(args, "mixed_work", None) is not None:
-        line["batched"] = batched_block(ctx, stream, args.mixed_work)
+        line["batched"] = batched_block(ctx, stream, args.mixed_work, rule=args.batch_rule)
     if rank == 0 and have_pilot and args.form == "auto":
         line["learned_pilot"] = learned_pilot_block(ctx)
     if rank == 0 and "tuned" in res and not args.tuned_opts:
@@ -882,6 +882,8 @@ def main():
                     help="the form timed for `value` (auto: the fastest within 0.05 dB of plain); "
                          "the plain path is timed beside it")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched form's mixed submission")
+    ap.add_argument("--batch-rule", default=BATCH_RULE, choices=BATCH_RULES,
+                    help="how the batched submission's images get their option sets")
     ap.add_argument("--autotune", action="store_true",
                     help="run the autotuner at this size instead of reading the calibrated 'tuned' profile")
     ap.add_argument("--tuned-opts", default=None,
