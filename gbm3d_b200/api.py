@@ -365,6 +365,20 @@ def GBM3D_rgb(I, sigma, opts: dict | None = None, ctx: Context | None = None):
     return np.stack([u.cpu().numpy().reshape(m, n, order="F") for u in outs], axis=2)
 
 
+def mixed_option_sets(opts, grey_opts, rgb_opts, n_grey: int, n_rgb: int):
+    """(call-level options, per-grey-image option list or None, per-colour-
+    image option list or None) of a mixed submission.  The 'tuned' profile
+    depends on each image's size and sigma, so ``opts`` of that profile
+    becomes every image's own entry (resolved per image) unless per-image
+    lists are given; the call-level set is then the dense configuration,
+    which no image uses."""
+    if isinstance(opts, dict) and opts.get("profile") == "tuned":
+        grey_opts = [opts] * n_grey if grey_opts is None else grey_opts
+        rgb_opts = [opts] * n_rgb if rgb_opts is None else rgb_opts
+        opts = dict(_opt.setBM3Dopts("default"), **_opt.DENSE)
+    return opts, grey_opts, rgb_opts
+
+
 def GBM3D_mixed(grey=(), grey_sigma=(), rgb=(), rgb_sigma=(), video=None, video_sigma: float = 0.0,
                 opts: dict | None = None, vopts: dict | None = None, use_graph: bool = True,
                 ctx: Context | None = None, outputs=None, grey_opts=None, rgb_opts=None):
@@ -378,11 +392,13 @@ def GBM3D_mixed(grey=(), grey_sigma=(), rgb=(), rgb_sigma=(), video=None, video_
     (VBM3D.m's defaults).  ``grey_opts`` / ``rgb_opts``, when given, hold one
     option dict per image instead, each resolved at that image's size and
     sigma (so {"profile": "tuned"} gives every image the autotuner's set for
-    its own size and noise class).  Returns (grey outputs, colour output
-    triples, video output (frames - nF + 1, n, m) or None) once the work has
-    finished."""
+    its own size and noise class; ``opts`` of the 'tuned' profile does the
+    same for every image without a list of its own).  Returns (grey outputs,
+    colour output triples, video output (frames - nF + 1, n, m) or None) once
+    the work has finished."""
     import torch
     ctx = ctx or context()
+    opts, grey_opts, rgb_opts = mixed_option_sets(opts, grey_opts, rgb_opts, len(grey), len(rgb))
     o = c_opts(_opt.resolve_opts(opts))
     cv = c_video_opts(vopts) if video is not None else None
     grey, rgb = list(grey), [tuple(t) for t in rgb]

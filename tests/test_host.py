@@ -227,3 +227,19 @@ def test_bench_batch_rules():
     assert sets["uniform512"] == (uniform, uniform)
     with pytest.raises(ValueError):
         bench.batch_set("nearest", small, 25.0, uniform)
+
+
+def test_mixed_option_sets():
+    """A mixed submission with opts of the 'tuned' profile gives every image
+    its own entry (resolved at its size and sigma by the binding); explicit
+    per-image lists win, and other profiles stay call-level."""
+    from gbm3d_b200 import api, options
+    tuned = {"profile": "tuned"}
+    o, g, c = api.mixed_option_sets(tuned, None, None, 3, 2)
+    assert g == [tuned] * 3 and c == [tuned] * 2
+    assert options.resolve_opts(o)["refStride"] == 3  # the dense configuration, used by no image
+    own = [{"profile": "fast"}] * 3
+    o, g, c = api.mixed_option_sets(tuned, own, None, 3, 1)
+    assert g is own and c == [tuned]
+    o, g, c = api.mixed_option_sets({"profile": "default"}, None, None, 3, 2)
+    assert o == {"profile": "default"} and g is None and c is None
