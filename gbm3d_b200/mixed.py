@@ -5,10 +5,12 @@ luma-driven matching) and a 32-frame 1280 x 720 synthetic video (ellipses
 translating 0-3 px per frame) with a +-1-frame temporal window, denoised by
 gbm3d_denoise_mixed as eager launches and as one captured CUDA graph.
 
-    python -m gbm3d_b200.mixed [--scale 1.0] [--reps 3] [--opts JSON] [--tune]
+    python -m gbm3d_b200.mixed [--scale 1.0] [--reps 3] [--opts JSON] [--tune] [--per-image]
 
 Grey and colour images use the dense configuration with the JSON overrides
-(or, with --tune, the autotuner's choice on its calibration image); the video
+(or, with --tune, the autotuner's choice on its calibration image, or, with
+--per-image, the 'tuned' profile's set for each image's own size and sigma
+class, as the bench's batched block gives them); the video
 uses VBM3D.m's defaults with a 3-frame window.  --scale shrinks every image
 side (a quick run).  Prints one JSON line: megapixels in the batch, device
 time per submission (CUDA events on the library stream), MPix/s eager and
@@ -72,6 +74,8 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--opts", default="{}", help="JSON overrides of the dense configuration")
     ap.add_argument("--tune", action="store_true", help="use the autotuner's choice for the images")
+    ap.add_argument("--per-image", action="store_true",
+                    help="each image the 'tuned' profile's set for its own size and sigma class")
     a = ap.parse_args()
 
     grey_pairs, gs, rgb, rs, frames, vs = workload(a.scale)  # before any CUDA work (spawned pool)
@@ -105,12 +109,15 @@ def main():
             + frames.shape[0] * frames.shape[1] * (frames.shape[2] - 2)) / 1e6
 
     def timed(use_graph):
-        outs = api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, use_graph=use_graph, ctx=ctx)  # warm-up / capture
+        kw = dict(use_graph=use_graph, ctx=ctx)
+        if a.per_image:
+            kw.update(grey_opts=[{"profile": "tuned"}] * len(dg), rgb_opts=[{"profile": "tuned"}] * len(dr))
+        outs = api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, **kw)  # warm-up / capture
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(a.reps):
-            api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, use_graph=use_graph, ctx=ctx, outputs=outs)
+            api.GBM3D_mixed(dg, gs, dr, rs, dv, vs, o, vo, outputs=outs, **kw)
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / a.reps, ctx.launch_count(), outs
@@ -125,8 +132,9 @@ def main():
         psnr.append(round(float(options.myPSNR(clean, U, 255) - options.myPSNR(clean, x, 255)), 3))
     print(json.dumps({"workload": "64 grey (200x300 .. 2048x1536, sigma 5-50) + 8 RGB 1024^2 + 32-frame 1280x720 "
                                   "video, +-1 frame", "scale": a.scale, "megapixels": mpix,
-                      "opts": {k: o[k] for k in ("refStride", "refStrideWie", "matchSize", "matchSpins",
-                                                 "matchSpinsWie", "cycleSpin", "form")},
+                      "opts": "per image: the 'tuned' profile" if a.per_image else {
+                          k: o[k] for k in ("refStride", "refStrideWie", "matchSize", "matchSpins",
+                                            "matchSpinsWie", "cycleSpin", "form")},
                       "eager_ms": eager_ms, "graph_ms": graph_ms, "eager_mpix_s": mpix / (eager_ms / 1e3),
                       "graph_mpix_s": mpix / (graph_ms / 1e3), "graph_launches_per_call": graph_launches,
                       "graph_equals_eager": same,
