@@ -119,9 +119,10 @@ def make_global(name, m, n, sigma, seed):
     print(name, S.shape)
 
 
-def make_video(name, m, n, frames, sigma, seed):
-    """VBM3D (nF = 3, patch 8, group 16, sym4 x Haar, tauMode 2, spins [0 4])
-    on frames scaled to [0,1], and the stages of its first window."""
+def make_video(name, m, n, frames, sigma, seed, d=8):
+    """VBM3D (nF = 3, patch d (8, or VBM3D.m's default 32), group 16, sym4 x
+    Haar, tauMode 2, spins [0 d/2]) on frames scaled to [0,1], and the stages
+    of its first window."""
     clean, noisy = synth.video(m, n, frames, sigma, seed=seed)
     I, s = noisy / 255.0, sigma / 255.0
     fac = dict(a_lo_xy=F.SYM4_LO, a_hi_xy=F.SYM4_HI, s_lo_xy=F.SYM4_LO, s_hi_xy=F.SYM4_HI,
@@ -129,9 +130,9 @@ def make_video(name, m, n, frames, sigma, seed):
                s_lo_z=options.haar_factors()["a_lo_z"], s_hi_z=options.haar_factors()["a_hi_z"])
     P, P2 = banks(fac)
     tau_unit = options.getTau(3, 2)
-    Y = F.vbm3d(I, s, 8, 16, 3, 2, tau_unit, [0, 4], 3, P, P2)
-    S, Vol = F.match_blocks_video(I[:, :, :3], 8, 16)
-    U, W = F.denoise_video(Vol, S, s * tau_unit, P, P2, 8, 3, 3, 2)
+    Y = F.vbm3d(I, s, d, 16, 3, 2, tau_unit, [0, d // 2], 3, P, P2)
+    S, Vol = F.match_blocks_video(I[:, :, :3], d, 16)
+    U, W = F.denoise_video(Vol, S, s * tau_unit, P, P2, d, 3, 3, 2)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), clean=clean, noisy=noisy, sigma=sigma, Y=Y, S=S,
                         Vol=Vol, U=U, W=W)
     print(name, Y.shape)
@@ -163,9 +164,12 @@ if __name__ == "__main__":
         make("tuned8x7_fabio_96x80_s25", 96, 80, 25.0, 41, "default", "bior", TUNED8X7, image=fabio_crop)
     if "video_32x40x4_s25" in only:
         make_video("video_32x40x4_s25", 32, 40, 4, 25.0, 23)
+    if "video_64x96x4_d32_s25" in only:
+        make_video("video_64x96x4_d32_s25", 64, 96, 4, 25.0, 24, d=32)
     if only:
         sys.exit(0)
     make_global("global_64x64_s25", 64, 64, 25.0, 21)
     make_global("global_48x64_s01", 48, 64, 0.1, 22)
     make_video("video_32x40x4_s25", 32, 40, 4, 25.0, 23)
+    make_video("video_64x96x4_d32_s25", 64, 96, 4, 25.0, 24, d=32)
     check_sym4_data()

@@ -228,3 +228,16 @@ def test_video_oracle_matches_golden(oracle):
     assert max_abs(U, g["U"]) <= 1e-12 and max_abs(W, g["W"]) <= 1e-12
     Y = oracle.VBM3D(I, s, prec=64)
     assert max_abs(Y, g["Y"]) <= 1e-6  # the reference's Y and nn are single
+
+
+def test_video_oracle_matches_golden_patch32(oracle):
+    """The same at VBM3D.m's default patch 32 (nF = 3, spins [0 16]): the
+    configuration of the batched submission's video."""
+    g = _load(os.path.join(os.path.dirname(__file__), "golden", "video_64x96x4_d32_s25.npz"))
+    I, s = g["noisy"] / 255.0, float(g["sigma"]) / 255.0
+    S, Vol = oracle.matchBlocksV(I[:, :, :3], 32, 16, prec=64)
+    assert np.array_equal(S, g["S"]) and max_abs(Vol, g["Vol"]) == 0
+    U, W = oracle.denoiseAndAggregateV(Vol, S, 32, 3, s * options.getTau(3, 2), 3, 2, prec=64)
+    assert max_abs(U, g["U"]) <= 1e-12 and max_abs(W, g["W"]) <= 1e-12
+    Y = oracle.VBM3D(I, s, d=32, spins=(0, 16), prec=64)
+    assert max_abs(Y, g["Y"]) <= 1e-6
